@@ -1,0 +1,351 @@
+#!/usr/bin/env python
+"""Benchmark: FP64 Gauss-Radau N-body propagation throughput (object-years/s) on B200.
+
+Workload (default): the plain N-body configuration -- 10,000 seeded main-belt states
+propagated 365.25 days under the Sun, eight planets and the Moon read from a seeded
+synthetic SPK type-2 ephemeris (degree-13 Chebyshev records).  One step = one propagation
+of the whole population.  ``value`` is device-resident throughput (inputs already in HBM,
+one kernel launch per step, CUDA-event timed, L2 flushed between steps); ``e2e`` is the
+same through the public C ABI with pinned host buffers (host->device and device->host
+copies inside the timed region).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl kete_b200|reference]
+
+With N > 1 (torchrun) every rank propagates its own population (weak scaling, no data
+exchange); the time is the maximum over ranks.  ``--impl reference`` times the CPU
+restatement of kete's path (the oracle) on all host cores on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Radau object-years/s at ≤1e-9 AU vs CPU ref: batched+adjoint vs plain on B200"
+UNIT = "object-years/s"
+EPOCH = 2460000.5
+SPAN = 365.25
+
+# algorithmic FP64 flops (add/sub/mul = 1, fma = 2, div = 1, sqrt = 1) of the kernel's
+# arithmetic, derived term by term from the force model and the Radau step for the
+# PLANETS force list with 14-coefficient Chebyshev records.
+FLOPS_PER_EVAL = 2867      # 11 Chebyshev records (223 each) + 10 bodies + GR/J2 terms
+FLOPS_PER_ITER = 7 * FLOPS_PER_EVAL + 1201  # 7 node evaluations + predictor/g/b/test
+FLOPS_PER_STEP = 120       # state update + step-size control
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def workload(n, seed=21):
+    from kete_b200 import synthetic
+
+    pos, vel = synthetic.main_belt(n, seed=seed)
+    jd0 = np.full(n, EPOCH)
+    jd1 = np.full(n, EPOCH + SPAN)
+    return pos, vel, jd0, jd1
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu_index = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu_index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def reduce_max(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def cpu_baseline(pos, vel, jd0, jd1, spk_bytes, threads=0):
+    """Time the oracle (CPU restatement of kete's path) on all host cores."""
+    from oracle import oracle as O
+
+    O.spk_reset()
+    O.spk_load_bytes(spk_bytes)
+    cores = threads or os.cpu_count()
+    t = time.perf_counter()
+    op, ov, st, ns, ne = O.propagate_n_body(pos, vel, jd0, jd1, threads=cores)
+    dt = time.perf_counter() - t
+    return op, st, dt, cores
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    from kete_b200 import synthetic
+
+    pos, vel, jd0, jd1 = workload(args.n)
+    with tempfile.TemporaryDirectory() as td:
+        spk = synthetic.write_synthetic_spk(os.path.join(td, "syn.bsp"))
+        spk_bytes = open(spk, "rb").read()
+    for _ in range(args.warmup):
+        cpu_baseline(pos[:, :200], vel[:, :200], jd0[:200], jd1[:200], spk_bytes)
+    times = []
+    cores = os.cpu_count()
+    for _ in range(args.steps):
+        _, st, dt, cores = cpu_baseline(pos, vel, jd0, jd1, spk_bytes)
+        times.append(dt)
+    total = float(np.sum(times))
+    value = args.n * SPAN / 365.25 * args.steps / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": f"plain N-body Radau, {args.n} main-belt states x {SPAN} d, "
+                   "Sun+8 planets+Moon from a synthetic SPK type-2 file", "n_objects": args.n},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"full workload ({args.n} objects) per step; the reference "
+                                   "Rust/rayon path cannot be built (no Rust toolchain), so the "
+                                   "C restatement of kete's FP64 code runs under OpenMP"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_gpu(args, world, rank, local):
+    import torch
+
+    import kete_b200
+    from kete_b200 import _lib, build, synthetic
+
+    build.build()
+    torch.cuda.set_device(local)
+    kete_b200.init(local)
+    td = tempfile.mkdtemp(prefix="kete_b200_bench_")
+    spk = synthetic.write_synthetic_spk(os.path.join(td, "syn.bsp"))
+    spk_bytes = open(spk, "rb").read()
+    kete_b200.spice.kernel_reload([spk])
+
+    n = args.n
+    pos, vel, jd0, jd1 = workload(n, seed=21 + rank)
+    dev = torch.device("cuda", local)
+    d = {k: torch.from_numpy(np.ascontiguousarray(v)).to(dev)
+         for k, v in dict(pos=pos, vel=vel, jd0=jd0, jd1=jd1).items()}
+    mode = args.mode
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def step():
+        return kete_b200.propagate_n_body_arrays(d["pos"], d["vel"], d["jd0"], d["jd1"],
+                                                 mode=mode)
+
+    # counts for the flop model (deterministic: same inputs every step)
+    _, _, st_d, det = kete_b200.propagate_n_body_arrays(d["pos"], d["vel"], d["jd0"], d["jd1"],
+                                                        mode=mode, with_details=True)
+    cnt = det["counters"].to(torch.int64).sum(dim=1).cpu().numpy()
+    steps_total, iters_total, exact_total = (int(x) for x in cnt)
+    flops = iters_total * FLOPS_PER_ITER + exact_total * FLOPS_PER_EVAL + steps_total * FLOPS_PER_STEP
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream(dev)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    with ClockSampler(local) as clk:
+        barrier(world)
+        torch.cuda.synchronize()
+        for k in range(args.steps):
+            flush.zero_()  # write > L2 (126 MB) between steps, outside the timed pair
+            evs[k][0].record(stream)
+            out = step()
+            evs[k][1].record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+    ms = [a.elapsed_time(b) for a, b in evs]
+    t_total = reduce_max(float(np.sum(ms)) * 1e-3, world)
+    ms_step = 1e3 * t_total / args.steps
+    obj_years = n * SPAN / 365.25
+    value = world * obj_years * args.steps / t_total
+
+    # end to end through the C ABI with pinned host buffers
+    hp = {k: torch.from_numpy(np.ascontiguousarray(v)).pin_memory()
+          for k, v in dict(pos=pos, vel=vel, jd0=jd0, jd1=jd1).items()}
+    hnp = {k: v.numpy() for k, v in hp.items()}
+    kete_b200.propagate_n_body_arrays(hnp["pos"], hnp["vel"], hnp["jd0"], hnp["jd1"], mode=mode)
+    e2e_t = []
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        op_h, ov_h, st_h = kete_b200.propagate_n_body_arrays(hnp["pos"], hnp["vel"], hnp["jd0"],
+                                                             hnp["jd1"], mode=mode)
+        e2e_t.append(time.perf_counter() - t)
+    e2e_total = reduce_max(float(np.sum(e2e_t)), world)
+    e2e_value = world * obj_years * args.steps / e2e_total
+    h2d = 8 * n * 8
+    d2h = 6 * n * 8 + 4 * n
+
+    if rank != 0:
+        return
+    peaks = measured_peaks()
+    tflops_probe = ctypes_probe(_lib)
+    achieved = flops / (ms_step * 1e-3) / 1e12
+    roof = {"bound": "fp64", "achieved": achieved, "peak": tflops_probe, "unit": "TFLOP/s",
+            "frac": achieved / tflops_probe if tflops_probe else None, "traffic": None,
+            "peak_source": "measured DFMA probe (kete_b200_fp64_probe) in this run",
+            "flops_per_launch": flops,
+            "hbm_bytes_algorithmic": int(n * (8 * 8 + 6 * 8 + 4))}
+
+    # CPU baseline (oracle on all host cores) on the full workload, and a parity check
+    op, st_cpu, cpu_dt, cores = cpu_baseline(pos, vel, jd0, jd1, spk_bytes)
+    err = np.linalg.norm(op_h - op, axis=0)
+    ok = (st_h == 0) & (st_cpu == 0)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"plain N-body Radau, {n} main-belt states x {SPAN} d per GPU, "
+                   "Sun+8 planets+Moon from a synthetic SPK type-2 file (14-coef records)",
+                   "n_objects_per_gpu": n, "span_days": SPAN, "mode": mode,
+                   "l2": "flushed (256 MB write) between timed steps",
+                   "parallelism": f"replicas x{world} (objects independent)"},
+        "object_steps_per_s": world * steps_total * args.steps / t_total,
+        "corrector_iterations_per_step": iters_total / max(steps_total, 1),
+        "roofline": roof,
+        "cpu_baseline": {"value": obj_years / cpu_dt, "unit": UNIT, "cores": cores,
+                         "kind": "port",
+                         "sample": f"the full {n}-object workload once, oracle (C restatement "
+                                   "of kete's FP64 path) with OpenMP on all host cores"},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": args.steps,
+        "clocks": clk.summary(),
+        "parity": {"max_err_au": float(err[ok].max()) if ok.any() else None,
+                   "status_match": bool((st_h == st_cpu).all()), "tolerance_au": 1e-9},
+        "mem_peaks_hbm_gbs": peaks.get("hbm_gbs"),
+    }
+    print(json.dumps(line), flush=True)
+
+
+def ctypes_probe(_lib):
+    import ctypes
+
+    L = _lib.lib()
+    L.kete_b200_fp64_probe.argtypes = [ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p]
+    out = ctypes.c_double()
+    ms = ctypes.c_float()
+    _lib.check(L.kete_b200_fp64_probe(20000, ctypes.byref(out), ctypes.byref(ms)))
+    return out.value
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="kete_b200", choices=["kete_b200", "reference"])
+    ap.add_argument("--n", type=int, default=10_000)
+    ap.add_argument("--mode", type=int, default=0)
+    args = ap.parse_args()
+    world, rank, local = dist_setup() if args.impl == "kete_b200" else (
+        int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0)
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+    else:
+        run_gpu(args, world, rank, local)
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

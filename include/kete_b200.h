@@ -1,0 +1,127 @@
+/*
+ * kete_b200.h -- C ABI of the B200-native kete orbit-propagation hot path.
+ *
+ * Plain pointers and sizes only.  Arrays of vectors are structure-of-arrays FP64:
+ * a "3 x n" array holds all x components, then all y, then all z.  Every entry point
+ * returns 0 on success or a negative KETE_B200_E_* code, with a message available from
+ * kete_b200_last_error() (per calling thread).  Per-object failures never abort a call:
+ * they are reported in status[i] with the codes below, which mirror
+ * kete_core::errors::Error (src/kete_core/src/errors.rs:14-32), and the object's outputs
+ * are NaN -- the behaviour of the reference's suppress_errors=True path
+ * (src/kete/rust/propagation.rs:113-143).
+ *
+ * `on_device`: 0 = the array arguments are host pointers (the call copies them to the
+ * GPU and back, and returns when the results are in host memory); 1 = they are device
+ * pointers on the current device (the call only enqueues work on `stream`).
+ * `stream` is a cudaStream_t (NULL = the legacy default stream).
+ *
+ * Frames: KETE_B200_FRAME_EQUATORIAL (J2000) and KETE_B200_FRAME_ECLIPTIC (J2000 ecliptic
+ * with the DE obliquity, src/kete_core/src/frames/definitions.rs:135).
+ */
+#ifndef KETE_B200_H
+#define KETE_B200_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* per-object status codes */
+#define KETE_B200_OK 0
+#define KETE_B200_CONVERGENCE 1
+#define KETE_B200_VALUE_ERROR 2
+#define KETE_B200_DAF_LIMITS 3
+#define KETE_B200_UNKNOWN_FRAME 4
+#define KETE_B200_IO_ERROR 5
+#define KETE_B200_IMPACT 6
+#define KETE_B200_TIMEOUT 7
+
+/* call return codes */
+#define KETE_B200_E_ARGUMENT (-1)
+#define KETE_B200_E_CUDA (-2)
+#define KETE_B200_E_NO_EPHEMERIS (-3)
+#define KETE_B200_E_IO (-4)
+#define KETE_B200_E_UNSUPPORTED (-5)
+
+#define KETE_B200_FRAME_EQUATORIAL 1
+#define KETE_B200_FRAME_ECLIPTIC 2
+
+/* propagate_n_body modes */
+#define KETE_B200_MODE_AUTO 0
+#define KETE_B200_MODE_THREAD 1  /* one object per thread, one launch per call */
+#define KETE_B200_MODE_NODES 2   /* eight lanes per object: the 7 Gauss-Radau nodes in parallel */
+
+/* Library version (major*10000 + minor*100 + patch). */
+int kete_b200_version(void);
+
+/* Select the CUDA device for this thread and prepare it (tables, constant memory).
+ * Replaces nothing in the reference (kete has no device); called once per process. */
+int kete_b200_init(int device);
+
+/* Message of the last failed call on this thread ("" if none). */
+const char* kete_b200_last_error(void);
+
+/* --- ephemeris --------------------------------------------------------------------------
+ * SpkCollection::load_file (src/kete_core/src/spice/spk.rs:307-329): parse a DAF/SPK file
+ * and make its type-2 segments resident on the current device.  Segments of other types
+ * are skipped and counted (kete_b200_spk_skipped). */
+int kete_b200_spk_load_file(const char* path);
+/* Same from an in-memory copy of the file (DafFile::from_buffer, spice/daf.rs:148-203). */
+int kete_b200_spk_load_buffer(const uint8_t* bytes, int64_t n_bytes);
+/* SpkCollection::reset (spk.rs:332-334). */
+int kete_b200_spk_reset(void);
+/* Number of segments skipped because their type is not 2. */
+int kete_b200_spk_skipped(void);
+/* loaded_objects(false) (spk.rs:186-205): writes up to `max` NAIF ids; returns the count. */
+int kete_b200_spk_loaded_ids(int64_t* ids, int max);
+/* Batched SpkCollection::try_get_state (spk.rs:87-96): state of NAIF `id` at each of the
+ * n epochs `jd` relative to `center`, in `frame`.  out6 is 6 x n (pos, vel). */
+int kete_b200_spk_get_states(int64_t n, int64_t id, const double* jd, int64_t center,
+                             int frame, double* out6, int32_t* status, int on_device,
+                             void* stream);
+
+/* --- propagation ------------------------------------------------------------------------
+ * propagate_two_body (src/kete_core/src/propagation/kepler.rs:306-322) for n Sun-centred
+ * states, object i from jd0[i] to jd1[i].  With observer_pos (3 doubles, same frame) each
+ * result is moved back by the light time to the observer, as the PyO3 binding does
+ * (src/kete/rust/kepler.rs:89-102); out_jd then holds the delayed epochs.  out_jd may be
+ * NULL. */
+int kete_b200_propagate_two_body(int64_t n, const double* pos, const double* vel,
+                                 const double* jd0, const double* jd1,
+                                 const double* observer_pos, double* out_pos, double* out_vel,
+                                 double* out_jd, int32_t* status, int on_device, void* stream);
+
+/* propagate_n_body_spk (src/kete_core/src/propagation/mod.rs:70-118) for n states that
+ * share `frame` and `center` (NAIF id), object i from jd0[i] to jd1[i], under the Sun,
+ * planets and Moon of the loaded SPK (plus the five large asteroids when
+ * include_asteroids != 0, mod.rs:82-88).
+ *   nongrav: NULL or 10 x n rows (kind, p1..p9): kind 0 none; kind 1 JPL comet
+ *            (a1 a2 a3 alpha r0 m n k dt, propagation/nongrav.rs:28-48); kind 2 dust
+ *            (beta, nongrav.rs:57-60).
+ *   impact_id / impact_jd: NAIF id and epoch of the body hit when status is
+ *            KETE_B200_IMPACT (acceleration.rs:147-158).  May be NULL.
+ *   min_dist: closest distance (AU) to any non-Sun perturber at an accepted step. May be NULL.
+ *   counters: NULL or 3 x n int32 (accepted steps, corrector iterations, exact evaluations).
+ *   mode: KETE_B200_MODE_*. */
+int kete_b200_propagate_n_body(int64_t n, const double* pos, const double* vel,
+                               const double* jd0, const double* jd1, int frame, int64_t center,
+                               int include_asteroids, const double* nongrav, double* out_pos,
+                               double* out_vel, int32_t* status, int32_t* impact_id,
+                               double* impact_jd, double* min_dist, int32_t* counters, int mode,
+                               int on_device, void* stream);
+
+/* RadauIntegrator::integrate with central_accel (propagation/mod.rs:35-46,126-138): the
+ * integrator alone, for checking it against kete's closed-form two-body result. */
+int kete_b200_radau_central(int64_t n, const double* pos, const double* vel, const double* t0,
+                            const double* t1, double* out_pos, double* out_vel,
+                            int32_t* status, int on_device, void* stream);
+
+/* --- diagnostics (no counterpart in the reference) ------------------------------------
+ * FP64 pipe throughput of the current device, measured with independent DFMA chains
+ * (the FP64 roofline denominator).  Synchronous; ms may be NULL. */
+int kete_b200_fp64_probe(int64_t iters, double* tflops, float* ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,32 @@
+"""kete_b200 -- kete's orbit-propagation hot path, B200-native.
+
+Drop-in GPU versions of kete's ``propagate_two_body``, ``propagate_n_body``,
+``fov_state_check``, ``hg_apparent_mag`` and ``NeatmParams.evaluate``, computed in FP64
+by hand-written sm_100a CUDA kernels in ``libketeb200.so`` (C ABI: include/kete_b200.h).
+"""
+from . import spice
+from ._lib import KeteB200Error, init
+from .propagation import (
+    NonGravModel,
+    propagate_n_body,
+    propagate_n_body_arrays,
+    propagate_two_body,
+    propagate_two_body_arrays,
+    radau_central_arrays,
+)
+from .state import Frames, SimultaneousStates, State
+
+__all__ = [
+    "spice",
+    "init",
+    "KeteB200Error",
+    "NonGravModel",
+    "propagate_n_body",
+    "propagate_n_body_arrays",
+    "propagate_two_body",
+    "propagate_two_body_arrays",
+    "radau_central_arrays",
+    "Frames",
+    "SimultaneousStates",
+    "State",
+]

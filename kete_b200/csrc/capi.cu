@@ -1,0 +1,632 @@
+// capi.cpp -- the extern "C" boundary: DAF/SPK ingest, device residency of the ephemeris,
+// argument checking, host<->device staging and kernel dispatch.
+//
+// The ephemeris side restates DafFile::from_buffer / try_load_segments
+// (src/kete_core/src/spice/daf.rs:148-262), SpkSegment / SpkSegmentType2 construction
+// (spice/spk_segments.rs:105-135,379-397) and SpkCollection::load_file (spice/spk.rs:307-329).
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/kete_b200.h"
+#include "common.cuh"
+#include "ephem.cuh"
+#include "internal.h"
+
+namespace kb {
+
+static thread_local std::string g_last_error;
+
+int set_error(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+int cuda_check(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return 0;
+    return set_error(KETE_B200_E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// ------------------------------------------------------------------------------------------
+// GravParams table (src/kete_core/src/constants/gravity.rs:43-148): PLANETS = first 10.
+// ------------------------------------------------------------------------------------------
+struct GravEntry {
+    int64_t id;
+    double mass_ratio, radius;
+    int kind;
+};
+static const GravEntry MASSES[15] = {
+    {10, 1.0, 0.004654758765894654, FK_SUN},
+    {1, 1.66012082548908e-07, 1.63139354095098e-05, FK_PLAIN},
+    {2, 2.44783828779694e-06, 4.04537843465442e-05, FK_PLAIN},
+    {399, 3.00348961546514e-06, 4.33036684926559e-05, FK_EARTH},
+    {301, 3.69430335010988e-08, 1.16138016662292e-05, FK_PLAIN},
+    {4, 3.22715608291416e-07, 2.27021279387769e-05, FK_PLAIN},
+    {5, 0.0009547919099414246, 0.00047789450254521576, FK_JUPITER},
+    {6, 0.00028588567002459455, 0.0004028666966848747, FK_PLAIN},
+    {7, 4.36624961322212e-05, 0.0001708513622580592, FK_PLAIN},
+    {8, 5.15138377265457e-05, 0.0001655371154958558, FK_PLAIN},
+    {20000001, 4.7191659919436e-10, 6.276827e-6, FK_PLAIN},
+    {20000002, 1.0259143964958e-10, 3.415824e-6, FK_PLAIN},
+    {20000004, 1.3026452498655e-10, 3.512082e-6, FK_PLAIN},
+    {20000010, 4.3953391300849e-11, 2.894426e-6, FK_PLAIN},
+    {20000704, 1.911e-11, 2.219283e-6, FK_PLAIN},
+};
+constexpr int N_PLANETS = 10;
+constexpr int N_MASSES = 15;
+
+// ------------------------------------------------------------------------------------------
+// host copy of the loaded SPK segments (type 2 only), in load order
+// ------------------------------------------------------------------------------------------
+struct HostSeg {
+    int64_t obj_id, center_id;
+    int frame_code;
+    double jd_start, jd_end;  // JD
+    double start_s;           // jd_to_spice_jd(jd_start)
+    double intlen;
+    int64_t n_coef, rsize, n_rec;
+    std::vector<double> data;  // the DAF array
+};
+
+struct DevState {
+    int version = -1;       // ephemeris version resident on this device
+    bool tables = false;
+    double* pool = nullptr;
+    size_t pool_cap = 0;
+    // grow-only staging buffers for host-pointer calls
+    std::vector<std::pair<void*, size_t>> bufs;
+};
+
+static std::mutex g_mu;
+static std::vector<HostSeg> g_segs;
+static int g_version = 0;
+static int g_skipped = 0;
+static std::map<int, DevState> g_dev;
+static EphemConst g_eph;  // host image of the constant table (pool pointer set per device)
+static std::vector<double> g_pool_host;
+static std::map<int64_t, int> g_slot_of;  // naif id -> slot
+
+static double spice_jds_to_jd(double s) { return s / 86400.0 + 2451545.0; }
+static double jd_to_spice_jd(double jd) { return (jd - 2451545.0) * 86400.0; }
+
+static int32_t rd_i32(const uint8_t* p, bool le) {
+    uint32_t v;
+    if (le)
+        v = (uint32_t)p[0] | ((uint32_t)p[1] << 8) | ((uint32_t)p[2] << 16) | ((uint32_t)p[3] << 24);
+    else
+        v = (uint32_t)p[3] | ((uint32_t)p[2] << 8) | ((uint32_t)p[1] << 16) | ((uint32_t)p[0] << 24);
+    return (int32_t)v;
+}
+static double rd_f64(const uint8_t* p, bool le) {
+    uint8_t b[8];
+    for (int i = 0; i < 8; ++i) b[i] = le ? p[i] : p[7 - i];
+    double d;
+    std::memcpy(&d, b, 8);
+    return d;
+}
+
+static int parse_daf(const uint8_t* buf, int64_t n, std::vector<HostSeg>& out, int& skipped) {
+    if (n < 1024) return set_error(KETE_B200_E_IO, "DAF file shorter than one record");
+    if (std::strncmp((const char*)buf, "DAF/", 4) != 0 && std::strncmp((const char*)buf, "NAIF", 4) != 0)
+        return set_error(KETE_B200_E_IO, "not a DAF file");
+    char kind[4] = {0};
+    for (int i = 0; i < 3; ++i) kind[i] = (char)toupper(buf[4 + i]);
+    if (std::strncmp(kind, "SPK", 3) != 0) return set_error(KETE_B200_E_IO, "DAF file is not an SPK");
+    bool le;
+    if (std::strncmp((const char*)buf + 88, "LTL-IEEE", 8) == 0)
+        le = true;
+    else if (std::strncmp((const char*)buf + 88, "BIG-IEEE", 8) == 0)
+        le = false;
+    else
+        return set_error(KETE_B200_E_IO, "Expected little or big endian in DAF file, found neither");
+    const int nd = rd_i32(buf + 8, le), ni = rd_i32(buf + 12, le);
+    if (nd != 2 || ni != 6) return set_error(KETE_B200_E_IO, "SPK File incorrectly Formatted.");
+    const int summary_size = nd + (ni + 1) / 2;
+    int next = rd_i32(buf + 76, le);
+    int guard = 0;
+    while (next != 0) {
+        if (++guard > 100000) return set_error(KETE_B200_E_IO, "DAF summary chain does not end");
+        const int64_t off = 1024LL * (next - 1);
+        if (off < 0 || off + 1024 > n) return set_error(KETE_B200_E_IO, "DAF summary record outside the file");
+        const uint8_t* rec = buf + off;
+        next = (int)rd_f64(rec, le);
+        const int n_sum = (int)rd_f64(rec + 16, le);
+        if (n_sum < 0 || 24 + (int64_t)n_sum * summary_size * 8 > 1024)
+            return set_error(KETE_B200_E_IO, "DAF summary record corrupt");
+        for (int k = 0; k < n_sum; ++k) {
+            const uint8_t* s = rec + 24 + (int64_t)k * summary_size * 8;
+            const double f0 = rd_f64(s, le), f1 = rd_f64(s + 8, le);
+            int32_t iv[6];
+            for (int q = 0; q < 6; ++q) iv[q] = rd_i32(s + 16 + 4 * q, le);
+            const int64_t a0 = iv[4], a1 = iv[5];
+            const int64_t nf = a1 - a0 + 1;
+            if (a0 < 1 || nf <= 4 || 8 * (a0 - 1) + 8 * nf > n)
+                return set_error(KETE_B200_E_IO, "SPK array outside the file");
+            if (iv[3] != 2) {
+                ++skipped;
+                continue;
+            }
+            HostSeg seg;
+            seg.obj_id = iv[0];
+            seg.center_id = iv[1];
+            seg.frame_code = iv[2];
+            seg.jd_start = spice_jds_to_jd(f0);
+            seg.jd_end = spice_jds_to_jd(f1);
+            seg.start_s = jd_to_spice_jd(seg.jd_start);
+            seg.data.resize((size_t)nf);
+            for (int64_t q = 0; q < nf; ++q) seg.data[q] = rd_f64(buf + 8 * (a0 - 1) + 8 * q, le);
+            seg.rsize = (int64_t)seg.data[nf - 2];
+            seg.intlen = seg.data[nf - 3];
+            seg.n_coef = (seg.rsize - 2) / 3;
+            if (seg.rsize < 5 || 3 * seg.n_coef + 2 != seg.rsize)
+                return set_error(KETE_B200_E_IO,
+                                 "File incorrectly formatted, found number of Chebyshev coefficients "
+                                 "doesn't match expected");
+            seg.n_rec = (nf - 4) / seg.rsize;
+            if (seg.n_rec < 1 || !(seg.intlen > 0.0))
+                return set_error(KETE_B200_E_IO, "type-2 segment without records");
+            out.push_back(std::move(seg));
+        }
+    }
+    return 0;
+}
+
+// Build the slot / segment / force tables and the device record pool from g_segs.
+static int rebuild_tables() {
+    std::memset(&g_eph, 0, sizeof g_eph);
+    g_pool_host.clear();
+    g_slot_of.clear();
+    // slots in order of first appearance; segments grouped per body, load order kept
+    std::vector<int64_t> ids;
+    for (const auto& s : g_segs)
+        if (!g_slot_of.count(s.obj_id)) {
+            g_slot_of[s.obj_id] = (int)ids.size();
+            ids.push_back(s.obj_id);
+        }
+    if ((int)ids.size() > MAX_SLOT) return set_error(KETE_B200_E_UNSUPPORTED, "too many SPK bodies for the device table");
+    if ((int)g_segs.size() > MAX_SEG) return set_error(KETE_B200_E_UNSUPPORTED, "too many SPK segments for the device table");
+    int nseg = 0;
+    for (size_t si = 0; si < ids.size(); ++si) {
+        Slot& sl = g_eph.slot[si];
+        sl.naif_id = (int32_t)ids[si];
+        sl.first = nseg;
+        sl.count = 0;
+        sl.center_id = -1;
+        for (const auto& s : g_segs) {
+            if (s.obj_id != ids[si]) continue;
+            if (s.frame_code != 1)
+                return set_error(KETE_B200_E_UNSUPPORTED,
+                                 "SPK segment for body " + std::to_string(s.obj_id) +
+                                     " is not in the J2000 equatorial frame (code 1)");
+            if (sl.count == 0) sl.center_id = (int32_t)s.center_id;
+            else if (sl.center_id != s.center_id)
+                return set_error(KETE_B200_E_UNSUPPORTED, "body with segments about different centres");
+            SegDesc& d = g_eph.seg[nseg];
+            d.jd_start = s.jd_start;
+            d.jd_end = s.jd_end;
+            d.start_s = s.start_s;
+            d.intlen = s.intlen;
+            d.n_coef = (int32_t)s.n_coef;
+            d.n_pad = (int32_t)((s.n_coef + 1) & ~1LL);
+            d.n_rec = (int32_t)s.n_rec;
+            d.rsize = 4 + 3 * d.n_pad;
+            d.offset = (int64_t)g_pool_host.size();
+            for (int64_t r = 0; r < s.n_rec; ++r) {
+                const double* rec = s.data.data() + r * s.rsize;
+                const double mid = rec[0], rad = rec[1];
+                g_pool_host.push_back(mid);
+                g_pool_host.push_back(rad);
+                g_pool_host.push_back(1.0 / rad);
+                g_pool_host.push_back(86400.0 / rad / AU_KM);  // spk_segments.rs:366
+                for (int c = 0; c < 3; ++c) {
+                    for (int64_t q = 0; q < s.n_coef; ++q) g_pool_host.push_back(rec[2 + c * s.n_coef + q]);
+                    for (int64_t q = s.n_coef; q < d.n_pad; ++q) g_pool_host.push_back(0.0);
+                }
+            }
+            ++sl.count;
+            ++nseg;
+        }
+    }
+    for (size_t si = 0; si < ids.size(); ++si) {
+        Slot& sl = g_eph.slot[si];
+        sl.parent_slot = -1;
+        if (sl.center_id != 0) {
+            auto it = g_slot_of.find(sl.center_id);
+            sl.parent_slot = it == g_slot_of.end() ? -2 : it->second;  // -2: centre not loaded
+        }
+    }
+    g_eph.n_seg = nseg;
+    g_eph.n_slot = (int32_t)ids.size();
+    // force plan (PLANETS / MASSES).  A body is usable when its chain reaches the
+    // barycentre within one intermediate centre.
+    auto usable = [&](int64_t id) -> int {
+        auto it = g_slot_of.find(id);
+        if (it == g_slot_of.end()) return -1;
+        const Slot& sl = g_eph.slot[it->second];
+        if (sl.parent_slot == -1) return it->second;
+        if (sl.parent_slot < 0) return -1;
+        if (g_eph.slot[sl.parent_slot].parent_slot != -1) return -1;
+        return it->second;
+    };
+    int nf = 0;
+    bool planets_ok = true, all_ok = true;
+    for (int b = 0; b < N_MASSES; ++b) {
+        const int slot = usable(MASSES[b].id);
+        if (slot < 0) {
+            if (b < N_PLANETS) planets_ok = false;
+            all_ok = false;
+            continue;
+        }
+        if (!all_ok && b >= N_PLANETS) continue;
+        ForceEntry& f = g_eph.force[nf++];
+        f.mass = MASSES[b].mass_ratio == 1.0 ? GMS : MASSES[b].mass_ratio * GMS;
+        f.radius = MASSES[b].radius;
+        f.slot = slot;
+        f.kind = MASSES[b].kind;
+        f.naif_id = (int32_t)MASSES[b].id;
+    }
+    g_eph.n_force_planets = planets_ok ? N_PLANETS : 0;
+    g_eph.n_force_all = (planets_ok && all_ok) ? N_MASSES : 0;
+    g_eph.sun_slot = g_slot_of.count(10) ? g_slot_of[10] : -1;
+    g_eph.loaded = 1;
+    ++g_version;
+    return 0;
+}
+
+static int ensure_tables(DevState& ds) {
+    if (ds.tables) return 0;
+    Tables t;
+    std::memset(&t, 0, sizeof t);
+    t.rot_c = std::cos(0.40909280422232897);
+    t.rot_s = std::sin(0.40909280422232897);
+    const double sp[8] = {0.0, 0.05626256053692215, 0.18024069173689236, 0.3526247171131696,
+                          0.5471536263305554, 0.7342101772154105, 0.8853209468390958,
+                          0.9775206135612875};
+    for (int i = 0; i < 8; ++i) t.spacing[i] = sp[i];
+    for (int i = 0; i < 7; ++i) {
+        t.w[i] = 1.0 / (double)((i + 2) * (i + 3));
+        t.u[i] = 1.0 / (double)(i + 2);
+    }
+    for (int i = 0; i < 7; ++i)
+        for (int j = 0; j < 7; ++j) t.c[i][j] = i == j ? 1.0 : 0.0;
+    for (int idx = 0; idx < 7; ++idx) {
+        if (idx > 0) t.c[idx][0] = -sp[idx] * t.c[idx - 1][0];
+        for (int idy = 1; idy < idx; ++idy)
+            t.c[idx][idy] = t.c[idx - 1][idy - 1] - sp[idx] * t.c[idx - 1][idy];
+    }
+    auto powi_h = [](double x, int n) {  // LLVM powi expansion, as on the device
+        double res = 1.0, sq = x;
+        bool have = false;
+        for (int v = n; v; v >>= 1) {
+            if (v & 1) {
+                res = have ? res * sq : sq;
+                have = true;
+            }
+            if (v >> 1) sq = sq * sq;
+        }
+        return res;
+    };
+    for (int j = 1; j < 8; ++j) {
+        for (int k = 0; k < 7; ++k) {
+            t.w_pow[j][k] = powi_h(sp[j], 1 + k) * t.w[k];
+            t.u_pow[j][k] = powi_h(sp[j], 1 + k) * t.u[k];
+        }
+        t.frac2[j] = powi_h(sp[j], 2);
+        t.inv_frac[j] = 1.0 / sp[j];
+        for (int z = 1; z < j; ++z) t.inv_diff[j][z] = 1.0 / (sp[j] - sp[z]);
+    }
+    int rc = upload_tables(t);
+    if (rc) return rc;
+    ds.tables = true;
+    return 0;
+}
+
+static int current_device(int& dev) { return cuda_check(cudaGetDevice(&dev), "cudaGetDevice"); }
+
+// Make the latest ephemeris resident on the current device.
+static int ensure_device(DevState*& out) {
+    int dev;
+    int rc = current_device(dev);
+    if (rc) return rc;
+    DevState& ds = g_dev[dev];
+    if ((rc = ensure_tables(ds))) return rc;
+    if (ds.version != g_version) {
+        const size_t bytes = g_pool_host.size() * sizeof(double);
+        if (bytes > ds.pool_cap) {
+            if (ds.pool) cudaFree(ds.pool);
+            ds.pool = nullptr;
+            ds.pool_cap = 0;
+            if ((rc = cuda_check(cudaMalloc(&ds.pool, bytes), "cudaMalloc ephemeris pool"))) return rc;
+            ds.pool_cap = bytes;
+        }
+        if (bytes && (rc = cuda_check(cudaMemcpy(ds.pool, g_pool_host.data(), bytes, cudaMemcpyHostToDevice),
+                                      "upload ephemeris pool")))
+            return rc;
+        EphemConst e = g_eph;
+        e.pool = ds.pool;
+        if ((rc = upload_ephem(e))) return rc;
+        ds.version = g_version;
+    }
+    out = &ds;
+    return 0;
+}
+
+// grow-only staging buffer `k` of at least `bytes`
+static int staging(DevState& ds, size_t k, size_t bytes, void** p) {
+    if (ds.bufs.size() <= k) ds.bufs.resize(k + 1, {nullptr, 0});
+    auto& b = ds.bufs[k];
+    if (b.second < bytes) {
+        if (b.first) cudaFree(b.first);
+        b.first = nullptr;
+        b.second = 0;
+        const size_t want = bytes < 256 ? 256 : bytes;
+        int rc = cuda_check(cudaMalloc(&b.first, want), "cudaMalloc staging buffer");
+        if (rc) return rc;
+        b.second = want;
+    }
+    *p = b.first;
+    return 0;
+}
+
+// chain of slots from `center` up to the barycentre (empty for centre 0)
+static int center_chain(int64_t center, CenterChain& ch) {
+    ch.len = 0;
+    int64_t c = center;
+    while (c != 0) {
+        auto it = g_slot_of.find(c);
+        if (it == g_slot_of.end() || ch.len >= 3)
+            return set_error(KETE_B200_E_NO_EPHEMERIS,
+                             "SPK files are missing information to be able to map from obj " +
+                                 std::to_string(center) + " to obj 0");
+        ch.slot[ch.len++] = it->second;
+        c = g_eph.slot[it->second].center_id;
+    }
+    return 0;
+}
+
+static int check_frame(int frame) {
+    if (frame != FRAME_EQUATORIAL && frame != FRAME_ECLIPTIC)
+        return set_error(KETE_B200_E_UNSUPPORTED, "frame must be equatorial (1) or ecliptic (2)");
+    return 0;
+}
+
+// Host-pointer staging helper: copy in, run, copy out.
+struct Stager {
+    DevState& ds;
+    cudaStream_t st;
+    int on_device;
+    size_t slot = 0;
+    int rc = 0;
+    std::vector<std::tuple<void*, const void*, size_t>> outs;  // host dst, dev src, bytes
+    template <class T>
+    T* in(const T* host, size_t count) {
+        if (!host || rc) return const_cast<T*>(host);
+        if (on_device) return const_cast<T*>(host);
+        void* d;
+        if ((rc = staging(ds, slot++, count * sizeof(T), &d))) return nullptr;
+        rc = cuda_check(cudaMemcpyAsync(d, host, count * sizeof(T), cudaMemcpyHostToDevice, st), "copy inputs to device");
+        return (T*)d;
+    }
+    template <class T>
+    T* out(T* host, size_t count) {
+        if (!host || rc) return host;
+        if (on_device) return host;
+        void* d;
+        if ((rc = staging(ds, slot++, count * sizeof(T), &d))) return nullptr;
+        outs.emplace_back((void*)host, d, count * sizeof(T));
+        return (T*)d;
+    }
+    int finish() {
+        if (rc) return rc;
+        for (auto& o : outs)
+            if ((rc = cuda_check(cudaMemcpyAsync(std::get<0>(o), std::get<1>(o), std::get<2>(o),
+                                                 cudaMemcpyDeviceToHost, st),
+                                 "copy results to host")))
+                return rc;
+        if (!on_device) rc = cuda_check(cudaStreamSynchronize(st), "stream synchronize");
+        return rc;
+    }
+};
+
+}  // namespace kb
+
+using namespace kb;
+
+extern "C" {
+
+int kete_b200_version(void) { return 100; }
+
+const char* kete_b200_last_error(void) { return g_last_error.c_str(); }
+
+int kete_b200_init(int device) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    int rc = cuda_check(cudaSetDevice(device), "cudaSetDevice");
+    if (rc) return rc;
+    DevState* ds;
+    return ensure_device(ds);
+}
+
+int kete_b200_spk_load_buffer(const uint8_t* bytes, int64_t n_bytes) {
+    if (!bytes || n_bytes <= 0) return set_error(KETE_B200_E_ARGUMENT, "empty SPK buffer");
+    std::lock_guard<std::mutex> lk(g_mu);
+    std::vector<HostSeg> segs;
+    int skipped = 0;
+    int rc = parse_daf(bytes, n_bytes, segs, skipped);
+    if (rc) return rc;
+    for (auto& s : segs) g_segs.push_back(std::move(s));
+    g_skipped += skipped;
+    return rebuild_tables();
+}
+
+int kete_b200_spk_load_file(const char* path) {
+    if (!path) return set_error(KETE_B200_E_ARGUMENT, "null path");
+    std::ifstream f(path, std::ios::binary);
+    if (!f) return set_error(KETE_B200_E_IO, std::string("cannot open ") + path);
+    std::vector<uint8_t> buf((std::istreambuf_iterator<char>(f)), std::istreambuf_iterator<char>());
+    return kete_b200_spk_load_buffer(buf.data(), (int64_t)buf.size());
+}
+
+int kete_b200_spk_reset(void) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_segs.clear();
+    g_skipped = 0;
+    g_slot_of.clear();
+    std::memset(&g_eph, 0, sizeof g_eph);
+    g_pool_host.clear();
+    ++g_version;
+    return 0;
+}
+
+int kete_b200_spk_skipped(void) { return g_skipped; }
+
+int kete_b200_spk_loaded_ids(int64_t* ids, int max) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    int k = 0;
+    for (int s = 0; s < g_eph.n_slot; ++s) {
+        if (ids && k < max) ids[k] = g_eph.slot[s].naif_id;
+        ++k;
+    }
+    return k;
+}
+
+int kete_b200_spk_get_states(int64_t n, int64_t id, const double* jd, int64_t center, int frame,
+                             double* out6, int32_t* status, int on_device, void* stream) {
+    if (n < 0 || (n > 0 && (!jd || !out6 || !status))) return set_error(KETE_B200_E_ARGUMENT, "null array");
+    std::lock_guard<std::mutex> lk(g_mu);
+    int rc = check_frame(frame);
+    if (rc) return rc;
+    auto it = g_slot_of.find(id);
+    if (it == g_slot_of.end())
+        return set_error(KETE_B200_E_NO_EPHEMERIS,
+                         "Object (" + std::to_string(id) + ") does not have an SPK record");
+    CenterChain ch;
+    if ((rc = center_chain(center, ch))) return rc;
+    DevState* ds;
+    if ((rc = ensure_device(ds))) return rc;
+    if (n == 0) return 0;
+    cudaStream_t st = (cudaStream_t)stream;
+    std::vector<int32_t> slots((size_t)n, it->second);
+    Stager S{*ds, st, 0};
+    int32_t* d_slot = S.in(slots.data(), (size_t)n);
+    S.on_device = on_device;
+    const double* d_jd = S.in(jd, (size_t)n);
+    double* d_out = S.out(out6, (size_t)n * 6);
+    int32_t* d_st = S.out(status, (size_t)n);
+    if (S.rc) return S.rc;
+    if ((rc = launch_spk_states(n, d_slot, d_jd, ch, frame, d_out, d_st, st))) return rc;
+    rc = S.finish();
+    if (!rc && on_device) rc = cuda_check(cudaStreamSynchronize(st), "stream synchronize");
+    return rc;
+}
+
+int kete_b200_propagate_two_body(int64_t n, const double* pos, const double* vel,
+                                 const double* jd0, const double* jd1, const double* observer_pos,
+                                 double* out_pos, double* out_vel, double* out_jd, int32_t* status,
+                                 int on_device, void* stream) {
+    if (n < 0 || (n > 0 && (!pos || !vel || !jd0 || !jd1 || !out_pos || !out_vel || !status)))
+        return set_error(KETE_B200_E_ARGUMENT, "null array");
+    std::lock_guard<std::mutex> lk(g_mu);
+    DevState* ds;
+    int rc = ensure_device(ds);
+    if (rc) return rc;
+    if (n == 0) return 0;
+    cudaStream_t st = (cudaStream_t)stream;
+    Stager S{*ds, st, on_device};
+    const double* d_pos = S.in(pos, 3 * (size_t)n);
+    const double* d_vel = S.in(vel, 3 * (size_t)n);
+    const double* d_jd0 = S.in(jd0, (size_t)n);
+    const double* d_jd1 = S.in(jd1, (size_t)n);
+    const double* d_obs = S.in(observer_pos, 3);
+    double* d_op = S.out(out_pos, 3 * (size_t)n);
+    double* d_ov = S.out(out_vel, 3 * (size_t)n);
+    double* d_oj = S.out(out_jd, (size_t)n);
+    int32_t* d_st = S.out(status, (size_t)n);
+    if (S.rc) return S.rc;
+    if ((rc = launch_two_body(n, d_pos, d_vel, d_jd0, d_jd1, d_obs, d_op, d_ov, d_oj, d_st, st)))
+        return rc;
+    return S.finish();
+}
+
+int kete_b200_propagate_n_body(int64_t n, const double* pos, const double* vel, const double* jd0,
+                               const double* jd1, int frame, int64_t center, int include_asteroids,
+                               const double* nongrav, double* out_pos, double* out_vel,
+                               int32_t* status, int32_t* impact_id, double* impact_jd,
+                               double* min_dist, int32_t* counters, int mode, int on_device,
+                               void* stream) {
+    if (n < 0 || (n > 0 && (!pos || !vel || !jd0 || !jd1 || !out_pos || !out_vel || !status)))
+        return set_error(KETE_B200_E_ARGUMENT, "null array");
+    std::lock_guard<std::mutex> lk(g_mu);
+    int rc = check_frame(frame);
+    if (rc) return rc;
+    if (!g_eph.loaded) return set_error(KETE_B200_E_NO_EPHEMERIS, "no SPK loaded");
+    const int n_force = include_asteroids ? g_eph.n_force_all : g_eph.n_force_planets;
+    if (n_force == 0)
+        return set_error(KETE_B200_E_NO_EPHEMERIS,
+                         include_asteroids ? "loaded SPKs lack a perturbing asteroid or planet"
+                                           : "loaded SPKs lack a planet, the Sun or the Moon");
+    NBodyArgs a;
+    std::memset(&a, 0, sizeof a);
+    if ((rc = center_chain(center, a.chain))) return rc;
+    DevState* ds;
+    if ((rc = ensure_device(ds))) return rc;
+    if (n == 0) return 0;
+    cudaStream_t st = (cudaStream_t)stream;
+    Stager S{*ds, st, on_device};
+    a.n = n;
+    a.pos = S.in(pos, 3 * (size_t)n);
+    a.vel = S.in(vel, 3 * (size_t)n);
+    a.jd0 = S.in(jd0, (size_t)n);
+    a.jd1 = S.in(jd1, (size_t)n);
+    a.nongrav = S.in(nongrav, 10 * (size_t)n);
+    a.frame = frame;
+    a.n_force = n_force;
+    a.out_pos = S.out(out_pos, 3 * (size_t)n);
+    a.out_vel = S.out(out_vel, 3 * (size_t)n);
+    a.status = S.out(status, (size_t)n);
+    a.impact_id = S.out(impact_id, (size_t)n);
+    a.impact_jd = S.out(impact_jd, (size_t)n);
+    a.min_dist = S.out(min_dist, (size_t)n);
+    a.counters = S.out(counters, 3 * (size_t)n);
+    a.max_loops = 1 << 20;
+    if (S.rc) return S.rc;
+    (void)mode;
+    if ((rc = launch_nbody_thread(a, 128, st))) return rc;
+    return S.finish();
+}
+
+int kete_b200_radau_central(int64_t n, const double* pos, const double* vel, const double* t0,
+                            const double* t1, double* out_pos, double* out_vel, int32_t* status,
+                            int on_device, void* stream) {
+    if (n < 0 || (n > 0 && (!pos || !vel || !t0 || !t1 || !out_pos || !out_vel || !status)))
+        return set_error(KETE_B200_E_ARGUMENT, "null array");
+    std::lock_guard<std::mutex> lk(g_mu);
+    DevState* ds;
+    int rc = ensure_device(ds);
+    if (rc) return rc;
+    if (n == 0) return 0;
+    cudaStream_t st = (cudaStream_t)stream;
+    Stager S{*ds, st, on_device};
+    const double* d_p = S.in(pos, 3 * (size_t)n);
+    const double* d_v = S.in(vel, 3 * (size_t)n);
+    const double* d_t0 = S.in(t0, (size_t)n);
+    const double* d_t1 = S.in(t1, (size_t)n);
+    double* d_op = S.out(out_pos, 3 * (size_t)n);
+    double* d_ov = S.out(out_vel, 3 * (size_t)n);
+    int32_t* d_st = S.out(status, (size_t)n);
+    if (S.rc) return S.rc;
+    if ((rc = launch_radau_central(n, d_p, d_v, d_t0, d_t1, d_op, d_ov, d_st, st))) return rc;
+    return S.finish();
+}
+
+int kete_b200_fp64_probe(int64_t iters, double* tflops, float* ms) {
+    if (iters <= 0 || !tflops) return set_error(KETE_B200_E_ARGUMENT, "bad probe arguments");
+    std::lock_guard<std::mutex> lk(g_mu);
+    return fp64_probe(iters, tflops, ms);
+}
+
+}  // extern "C"

@@ -1,0 +1,212 @@
+// forces.cuh -- accelerations used by the Radau integrators.
+//
+// SpkForce restates spk_accel (kete_core/propagation/acceleration.rs:121-168) with
+// GravParams::add_acceleration, j2_correction and apply_gr_correction
+// (kete_core/constants/gravity.rs:171-253) and NonGravModel::add_acceleration
+// (kete_core/propagation/nongrav.rs:114-157).  Bodies are summed in the reference's
+// order (Sun, Mercury, Venus, Earth, Moon, Mars, Jupiter, Saturn, Uranus, Neptune).  A
+// body whose SPK centre is not the barycentre (Earth and Moon, centred on the Earth-Moon
+// barycentre) reuses the centre state evaluated for the previous body when it is the same
+// centre, so a force evaluation costs 11 Chebyshev records instead of the reference's 12.
+#pragma once
+#include "common.cuh"
+#include "ephem.cuh"
+#include "kepler.cuh"
+
+namespace kb {
+
+// Device constants.  Only kernels.cu includes the device headers, so these are defined
+// once; the host uploads them with upload_tables / upload_ephem.
+__constant__ Tables c_tab;
+__constant__ EphemConst c_eph;
+
+__device__ __forceinline__ void eq_to_ecl(const double v[3], double o[3]) {
+    const double c = c_tab.rot_c, s = c_tab.rot_s;
+    const double y = c * v[1] + s * v[2];
+    const double z = -s * v[1] + c * v[2];
+    o[0] = v[0];
+    o[1] = y;
+    o[2] = z;
+}
+__device__ __forceinline__ void ecl_to_eq(const double v[3], double o[3]) {
+    const double c = c_tab.rot_c, s = c_tab.rot_s;
+    const double y = c * v[1] - s * v[2];
+    const double z = s * v[1] + c * v[2];
+    o[0] = v[0];
+    o[1] = y;
+    o[2] = z;
+}
+
+__device__ __forceinline__ void j2_correction(const double rp[3], double radius, double j2,
+                                              double mass, double o[3]) {
+    const double r = norm3(rp[0], rp[1], rp[2]);
+    const double zr = rp[2] / r;
+    const double z_squared = 5.0 * (zr * zr);
+    const double rr = radius / r;
+    const double coef = 1.5 * j2 * mass * (rr * rr) * powi<-3>(r);
+    o[0] = rp[0] * coef * (z_squared - 1.0);
+    o[1] = rp[1] * coef * (z_squared - 1.0);
+    o[2] = rp[2] * coef * (z_squared - 3.0);
+}
+
+__device__ __forceinline__ void apply_gr(double acc[3], const double rp[3], const double rv[3],
+                                         double mass, double r) {
+    const double r_v = 4.0 * (rp[0] * rv[0] + rp[1] * rv[1] + rp[2] * rv[2]);
+    const double rel_v2 = rv[0] * rv[0] + rv[1] * rv[1] + rv[2] * rv[2];
+    const double gr_const = mass * C_AU_PER_DAY_INV_SQUARED * powi<-3>(r);
+    const double c = 4. * mass / r - rel_v2;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) acc[i] += gr_const * (c * rp[i] + r_v * rv[i]);
+}
+
+// Per-object non-gravitational model row: kind (0 none, 1 JPL comet, 2 dust) then
+// a1 a2 a3 alpha r0 m n k dt (JPL) or beta (dust).  Stored column-major (10 x n).
+struct NonGrav {
+    const double* __restrict__ base;
+    int64_t stride;
+    int kind;
+    __device__ __forceinline__ double p(int k) const { return __ldg(base + (int64_t)k * stride); }
+};
+
+__device__ __noinline__ void nongrav_add(const NonGrav& ng, double acc[3], const double pos_in[3],
+                                         const double vel[3]) {
+    if (ng.kind == 2) {
+        const double beta = ng.p(1);
+        const double n = norm3(pos_in[0], pos_in[1], pos_in[2]);
+        const double pn[3] = {pos_in[0] / n, pos_in[1] / n, pos_in[2] / n};
+        const double r_dot = pn[0] * vel[0] + pn[1] * vel[1] + pn[2] * vel[2];
+        const double norm2_inv =
+            1.0 / (pos_in[0] * pos_in[0] + pos_in[1] * pos_in[1] + pos_in[2] * pos_in[2]);
+        const double scaling = GMS * beta * norm2_inv;
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+            acc[i] += scaling * ((1.0 - r_dot * C_AU_PER_DAY_INV_SQUARED) * pn[i] -
+                                 vel[i] * C_AU_PER_DAY_INV_SQUARED);
+        return;
+    }
+    const double a1 = ng.p(1), a2 = ng.p(2), a3 = ng.p(3), alpha = ng.p(4), r_0 = ng.p(5);
+    const double m = ng.p(6), nn = ng.p(7), k = ng.p(8), dt = ng.p(9);
+    double pos[3] = {pos_in[0], pos_in[1], pos_in[2]};
+    const double pnorm = norm3(pos[0], pos[1], pos[2]);
+    const double pn[3] = {pos[0] / pnorm, pos[1] / pnorm, pos[2] / pnorm};
+    const double vdp = vel[0] * pn[0] + vel[1] * pn[1] + vel[2] * pn[2];
+    double tv[3] = {vel[0] - pn[0] * vdp, vel[1] - pn[1] * vdp, vel[2] - pn[2] * vdp};
+    const double tn = norm3(tv[0], tv[1], tv[2]);
+    const double t_vec[3] = {tv[0] / tn, tv[1] / tn, tv[2] / tn};
+    double nv[3] = {t_vec[1] * pn[2] - t_vec[2] * pn[1], t_vec[2] * pn[0] - t_vec[0] * pn[2],
+                    t_vec[0] * pn[1] - t_vec[1] * pn[0]};
+    const double nnrm = norm3(nv[0], nv[1], nv[2]);
+    const double n_vec[3] = {nv[0] / nnrm, nv[1] / nnrm, nv[2] / nnrm};
+    if (dt != 0.0) {
+        double p2[3] = {pos[0], pos[1], pos[2]}, v2[3] = {vel[0], vel[1], vel[2]};
+        if (analytic_2_body(-dt, p2, v2) == ST_OK) {
+            pos[0] = p2[0];
+            pos[1] = p2[1];
+            pos[2] = p2[2];
+        }
+    }
+    const double rr0 = norm3(pos[0], pos[1], pos[2]) / r_0;
+    const double scale = alpha * pow(rr0, -m) * pow(1.0 + pow(rr0, nn), -k);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) acc[i] += pn[i] * (scale * a1);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) acc[i] += t_vec[i] * (scale * a2);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) acc[i] += n_vec[i] * (scale * a3);
+}
+
+// Acceleration from the SPK perturbers.  exact=true marks the evaluations at the
+// integrator's accepted states: only those check for impacts (r <= body radius) and
+// update the closest-approach record.
+struct SpkForce {
+    int n_force;
+    NonGrav ng;
+    // outputs of exact evaluations
+    mutable int32_t impact_id;
+    mutable double min_dist;  // smallest distance to a non-Sun body seen at exact evals
+    mutable int32_t min_id;
+
+    template <bool EXACT>
+    __device__ __forceinline__ int eval(double t, const double x[3], const double v[3],
+                                        double out[3]) const {
+        double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
+        int cache_slot = -1;
+        double cp[3] = {0.0, 0.0, 0.0}, cv[3] = {0.0, 0.0, 0.0};
+        for (int b = 0; b < n_force; ++b) {
+            const ForceEntry fe = c_eph.force[b];
+            const int slot = fe.slot;
+            double bp[3], bv[3];
+            if (eph_raw(c_eph, slot, t, bp, bv) != ST_OK) return ST_DAF_LIMITS;
+            const int parent = c_eph.slot[slot].parent_slot;
+            if (parent >= 0) {
+                if (parent != cache_slot) {
+                    if (eph_raw(c_eph, parent, t, cp, cv) != ST_OK) return ST_DAF_LIMITS;
+                    cache_slot = parent;
+                }
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    bp[i] += cp[i];
+                    bv[i] += cv[i];
+                }
+            }
+            const double rp[3] = {x[0] - bp[0], x[1] - bp[1], x[2] - bp[2]};
+            const double rv[3] = {v[0] - bv[0], v[1] - bv[1], v[2] - bv[2]};
+            const double r = norm3(rp[0], rp[1], rp[2]);
+            if (EXACT) {
+                if (r <= fe.radius) {
+                    impact_id = fe.naif_id;
+                    return ST_IMPACT;
+                }
+                if (fe.kind != FK_SUN && r < min_dist) {
+                    min_dist = r;
+                    min_id = fe.naif_id;
+                }
+            }
+            const double mass = fe.mass;
+            const double kk = mass * powi<-3>(r);
+            double acc[3] = {acc0 - rp[0] * kk, acc1 - rp[1] * kk, acc2 - rp[2] * kk};
+            if (fe.kind == FK_SUN || fe.kind == FK_JUPITER) {
+                apply_gr(acc, rp, rv, mass, r);
+                double re[3], j2[3], j2q[3];
+                eq_to_ecl(rp, re);
+                j2_correction(re, fe.radius, fe.kind == FK_JUPITER ? JUPITER_J2 : SUN_J2, mass, j2);
+                ecl_to_eq(j2, j2q);
+                acc[0] += j2q[0];
+                acc[1] += j2q[1];
+                acc[2] += j2q[2];
+                if (fe.kind == FK_SUN && ng.kind != 0) nongrav_add(ng, acc, rp, rv);
+            } else if (fe.kind == FK_EARTH) {
+                double j2[3];
+                j2_correction(rp, fe.radius, EARTH_J2, mass, j2);
+                acc[0] += j2[0];
+                acc[1] += j2[1];
+                acc[2] += j2[2];
+            }
+            acc0 = acc[0];
+            acc1 = acc[1];
+            acc2 = acc[2];
+        }
+        out[0] = acc0;
+        out[1] = acc1;
+        out[2] = acc2;
+        return ST_OK;
+    }
+};
+
+// central_accel (acceleration.rs:66-80): the Sun at the origin only.
+struct CentralForce {
+    mutable int32_t impact_id;
+    mutable double min_dist;
+    mutable int32_t min_id;
+    template <bool EXACT>
+    __device__ __forceinline__ int eval(double, const double x[3], const double[3],
+                                        double out[3]) const {
+        const double k = powi<-3>(norm3(x[0], x[1], x[2]));
+        out[0] = -x[0] * k * GMS;
+        out[1] = -x[1] * k * GMS;
+        out[2] = -x[2] * k * GMS;
+        return ST_OK;
+    }
+};
+
+}  // namespace kb

@@ -1,0 +1,60 @@
+// internal.h -- host-side declarations shared by the C-ABI layer and the kernel TU.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+namespace kb {
+
+struct Tables;
+struct EphemConst;
+
+// set the thread's last error message; returns `code`
+int set_error(int code, const std::string& msg);
+int cuda_check(cudaError_t e, const char* what);
+
+// kernels.cu
+int upload_tables(const Tables& t);
+int upload_ephem(const EphemConst& e);
+
+struct CenterChain {
+    int len = 0;
+    int slot[3] = {-1, -1, -1};
+};
+
+struct NBodyArgs {
+    int64_t n;
+    const double* pos;  // 3 x n
+    const double* vel;
+    const double* jd0;
+    const double* jd1;
+    const double* nongrav;  // 10 x n or null
+    int frame;
+    CenterChain chain;
+    int n_force;
+    double* out_pos;
+    double* out_vel;
+    int32_t* status;
+    int32_t* impact_id;   // may be null
+    double* impact_jd;    // may be null
+    double* min_dist;     // may be null
+    int32_t* counters;    // 3 x n (steps, iterations, exact evals) or null
+    int max_loops;
+};
+
+int launch_two_body(int64_t n, const double* pos, const double* vel, const double* jd0,
+                    const double* jd1, const double* obs, double* out_pos, double* out_vel,
+                    double* out_jd, int32_t* status, cudaStream_t stream);
+int launch_nbody_thread(const NBodyArgs& a, int block, cudaStream_t stream);
+int launch_radau_central(int64_t n, const double* pos, const double* vel, const double* t0,
+                         const double* t1, double* out_pos, double* out_vel, int32_t* status,
+                         cudaStream_t stream);
+int launch_spk_states(int64_t n, const int32_t* slot, const double* jd,
+                      const CenterChain& center_chain, int frame, double* out6, int32_t* status,
+                      cudaStream_t stream);
+
+int fp64_probe(int64_t iters, double* tflops, float* ms_out);
+
+}  // namespace kb

@@ -1,0 +1,304 @@
+// kernels.cu -- propagation kernels (two-body, N-body Radau, ephemeris queries) and their
+// host launchers.  All device constants (Radau tables, ephemeris tables) live in this
+// translation unit.
+#include <cstdio>
+
+#include "common.cuh"
+#include "ephem.cuh"
+#include "forces.cuh"
+#include "internal.h"
+#include "kepler.cuh"
+#include "radau.cuh"
+
+namespace kb {
+
+int upload_tables(const Tables& t) {
+    return cuda_check(cudaMemcpyToSymbol(c_tab, &t, sizeof(Tables)), "upload Radau tables");
+}
+int upload_ephem(const EphemConst& e) {
+    return cuda_check(cudaMemcpyToSymbol(c_eph, &e, sizeof(EphemConst)), "upload ephemeris table");
+}
+
+// -------------------------------------------------------------------------------------------
+// two-body (kete_core/propagation/kepler.rs:306-322 with the light-delay second pass of the
+// PyO3 binding, src/kete/rust/kepler.rs:89-102).  One thread per object, SoA FP64.
+// -------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) two_body_kernel(
+    int64_t n, const double* __restrict__ pos, const double* __restrict__ vel,
+    const double* __restrict__ jd0, const double* __restrict__ jd1,
+    const double* __restrict__ obs, double* __restrict__ out_pos, double* __restrict__ out_vel,
+    double* __restrict__ out_jd, int32_t* __restrict__ status) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double p[3] = {pos[i], pos[n + i], pos[2 * n + i]};
+    double v[3] = {vel[i], vel[n + i], vel[2 * n + i]};
+    const double t0 = jd0[i], t1 = jd1[i];
+    double tj = t1;
+    int rc = analytic_2_body(t1 - t0, p, v);
+    if (rc == ST_OK && obs != nullptr) {
+        const double o0 = obs[0], o1 = obs[1], o2 = obs[2];
+        const double delay = -norm3(p[0] - o0, p[1] - o1, p[2] - o2) / C_AU_PER_DAY;
+        const double t2 = tj + delay;
+        rc = analytic_2_body(t2 - tj, p, v);
+        tj = t2;
+    }
+    if (rc != ST_OK) {
+        p[0] = p[1] = p[2] = v[0] = v[1] = v[2] = __longlong_as_double(0x7ff8000000000000LL);
+        tj = t1;
+    }
+    out_pos[i] = p[0];
+    out_pos[n + i] = p[1];
+    out_pos[2 * n + i] = p[2];
+    out_vel[i] = v[0];
+    out_vel[n + i] = v[1];
+    out_vel[2 * n + i] = v[2];
+    if (out_jd) out_jd[i] = tj;
+    status[i] = rc;
+}
+
+int launch_two_body(int64_t n, const double* pos, const double* vel, const double* jd0,
+                    const double* jd1, const double* obs, double* out_pos, double* out_vel,
+                    double* out_jd, int32_t* status, cudaStream_t stream) {
+    if (n <= 0) return 0;
+    const int block = 128;
+    const int64_t grid = (n + block - 1) / block;
+    two_body_kernel<<<(unsigned)grid, block, 0, stream>>>(n, pos, vel, jd0, jd1, obs, out_pos,
+                                                          out_vel, out_jd, status);
+    return cuda_check(cudaGetLastError(), "two_body_kernel launch");
+}
+
+// -------------------------------------------------------------------------------------------
+// centre / frame changes around the integration (kete_core/propagation/mod.rs:76-80,
+// 107-116 with SpkCollection::try_change_center, spk.rs:99-126, and State::try_change_center,
+// state.rs:242-281): the SPK states are expressed in the object's frame before they are
+// added, then the sum is rotated into the integration frame (equatorial).
+// -------------------------------------------------------------------------------------------
+__device__ __forceinline__ int to_ssb_equatorial(double t, int frame, const CenterChain& ch,
+                                                 double p[3], double v[3]) {
+    for (int k = 0; k < ch.len; ++k) {
+        double sp[3], sv[3];
+        if (eph_raw(c_eph, ch.slot[k], t, sp, sv) != ST_OK) return ST_DAF_LIMITS;
+        if (frame == FRAME_ECLIPTIC) {
+            double q[3];
+            eq_to_ecl(sp, q);
+            sp[0] = q[0]; sp[1] = q[1]; sp[2] = q[2];
+            eq_to_ecl(sv, q);
+            sv[0] = q[0]; sv[1] = q[1]; sv[2] = q[2];
+        }
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            p[i] += sp[i];
+            v[i] += sv[i];
+        }
+    }
+    if (frame == FRAME_ECLIPTIC) {
+        double q[3];
+        ecl_to_eq(p, q);
+        p[0] = q[0]; p[1] = q[1]; p[2] = q[2];
+        ecl_to_eq(v, q);
+        v[0] = q[0]; v[1] = q[1]; v[2] = q[2];
+    }
+    return ST_OK;
+}
+
+__device__ __forceinline__ int from_ssb_equatorial(double t, int frame, const CenterChain& ch,
+                                                   double p[3], double v[3]) {
+    for (int k = ch.len - 1; k >= 0; --k) {
+        double sp[3], sv[3];
+        if (eph_raw(c_eph, ch.slot[k], t, sp, sv) != ST_OK) return ST_DAF_LIMITS;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            p[i] += -sp[i];
+            v[i] += -sv[i];
+        }
+    }
+    if (frame == FRAME_ECLIPTIC) {
+        double q[3];
+        eq_to_ecl(p, q);
+        p[0] = q[0]; p[1] = q[1]; p[2] = q[2];
+        eq_to_ecl(v, q);
+        v[0] = q[0]; v[1] = q[1]; v[2] = q[2];
+    }
+    return ST_OK;
+}
+
+// -------------------------------------------------------------------------------------------
+// N-body Radau, one object per thread (the plain form of propagate_n_body_spk,
+// kete_core/propagation/mod.rs:70-118).
+// -------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) nbody_thread_kernel(NBodyArgs a) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const int64_t n = a.n;
+    RadauObj s;
+    s.t = a.jd0[i];
+    const double tf = a.jd1[i];
+    s.x[0] = a.pos[i]; s.x[1] = a.pos[n + i]; s.x[2] = a.pos[2 * n + i];
+    s.v[0] = a.vel[i]; s.v[1] = a.vel[n + i]; s.v[2] = a.vel[2 * n + i];
+    SpkForce F;
+    F.n_force = a.n_force;
+    F.ng.base = a.nongrav ? a.nongrav + i : nullptr;
+    F.ng.stride = n;
+    F.ng.kind = a.nongrav ? (int)a.nongrav[i] : 0;
+    F.impact_id = 0;
+    F.min_dist = 1e300;
+    F.min_id = 0;
+    RadauCounters cnt;
+    int rc = ST_OK;
+    bool finite = isfinite(s.x[0]) && isfinite(s.x[1]) && isfinite(s.x[2]) && isfinite(s.v[0]) &&
+                  isfinite(s.v[1]) && isfinite(s.v[2]) && isfinite(s.t);
+    if (!finite) rc = ST_VALUE_ERROR;
+    if (rc == ST_OK) rc = to_ssb_equatorial(s.t, a.frame, a.chain, s.x, s.v);
+    if (rc == ST_OK) rc = radau_integrate(s, tf, F, cnt, a.max_loops);
+    if (rc == ST_OK) rc = from_ssb_equatorial(tf, a.frame, a.chain, s.x, s.v);
+    if (rc != ST_OK) {
+        const double nan = __longlong_as_double(0x7ff8000000000000LL);
+        s.x[0] = s.x[1] = s.x[2] = s.v[0] = s.v[1] = s.v[2] = nan;
+    }
+    a.out_pos[i] = s.x[0]; a.out_pos[n + i] = s.x[1]; a.out_pos[2 * n + i] = s.x[2];
+    a.out_vel[i] = s.v[0]; a.out_vel[n + i] = s.v[1]; a.out_vel[2 * n + i] = s.v[2];
+    a.status[i] = rc;
+    if (a.impact_id) a.impact_id[i] = rc == ST_IMPACT ? F.impact_id : 0;
+    if (a.impact_jd) a.impact_jd[i] = rc == ST_IMPACT ? s.t : 0.0;
+    if (a.min_dist) a.min_dist[i] = F.min_dist;
+    if (a.counters) {
+        a.counters[i] = cnt.steps;
+        a.counters[n + i] = cnt.iterations;
+        a.counters[2 * n + i] = cnt.exact;
+    }
+}
+
+int launch_nbody_thread(const NBodyArgs& a, int block, cudaStream_t stream) {
+    if (a.n <= 0) return 0;
+    if (block <= 0) block = 128;
+    const int64_t grid = (a.n + block - 1) / block;
+    nbody_thread_kernel<<<(unsigned)grid, block, 0, stream>>>(a);
+    return cuda_check(cudaGetLastError(), "nbody_thread_kernel launch");
+}
+
+// -------------------------------------------------------------------------------------------
+// Radau with the central force only (propagate_two_body_radau / propagation_central,
+// kete_core/propagation/mod.rs:35-46,126-138): checks the integrator in isolation.
+// -------------------------------------------------------------------------------------------
+__global__ void radau_central_kernel(int64_t n, const double* pos, const double* vel,
+                                     const double* t0, const double* t1, double* out_pos,
+                                     double* out_vel, int32_t* status) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    RadauObj s;
+    s.t = t0[i];
+    s.x[0] = pos[i]; s.x[1] = pos[n + i]; s.x[2] = pos[2 * n + i];
+    s.v[0] = vel[i]; s.v[1] = vel[n + i]; s.v[2] = vel[2 * n + i];
+    CentralForce F;
+    RadauCounters cnt;
+    int rc = radau_integrate(s, t1[i], F, cnt, 1 << 20);
+    out_pos[i] = s.x[0]; out_pos[n + i] = s.x[1]; out_pos[2 * n + i] = s.x[2];
+    out_vel[i] = s.v[0]; out_vel[n + i] = s.v[1]; out_vel[2 * n + i] = s.v[2];
+    status[i] = rc;
+}
+
+int launch_radau_central(int64_t n, const double* pos, const double* vel, const double* t0,
+                         const double* t1, double* out_pos, double* out_vel, int32_t* status,
+                         cudaStream_t stream) {
+    if (n <= 0) return 0;
+    const int block = 128;
+    radau_central_kernel<<<(unsigned)((n + block - 1) / block), block, 0, stream>>>(
+        n, pos, vel, t0, t1, out_pos, out_vel, status);
+    return cuda_check(cudaGetLastError(), "radau_central_kernel launch");
+}
+
+// -------------------------------------------------------------------------------------------
+// batched SpkCollection::try_get_state (spk.rs:87-96): state of body `slot` (chained to the
+// barycentre) minus the centre chain, in `frame`.
+// -------------------------------------------------------------------------------------------
+__global__ void spk_states_kernel(int64_t n, const int32_t* slot, const double* jd,
+                                  CenterChain center_chain, int frame, double* out6,
+                                  int32_t* status) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double t = jd[i];
+    double p[3] = {0, 0, 0}, v[3] = {0, 0, 0};
+    int rc = ST_OK;
+    // the body's own chain: raw(body) + raw(parent) ...
+    int s = slot[i];
+    for (int k = 0; k < 3 && s >= 0 && rc == ST_OK; ++k) {
+        double sp[3], sv[3];
+        rc = eph_raw(c_eph, s, t, sp, sv);
+        for (int q = 0; q < 3; ++q) {
+            p[q] += sp[q];
+            v[q] += sv[q];
+        }
+        s = c_eph.slot[s].parent_slot;
+    }
+    if (s < -1 || s >= 0) rc = ST_DAF_LIMITS;  // centre chain not complete
+    if (rc == ST_OK) rc = from_ssb_equatorial(t, frame, center_chain, p, v);
+    for (int q = 0; q < 3; ++q) {
+        out6[q * n + i] = p[q];
+        out6[(3 + q) * n + i] = v[q];
+    }
+    status[i] = rc;
+}
+
+int launch_spk_states(int64_t n, const int32_t* slot, const double* jd,
+                      const CenterChain& center_chain, int frame, double* out6, int32_t* status,
+                      cudaStream_t stream) {
+    if (n <= 0) return 0;
+    const int block = 128;
+    spk_states_kernel<<<(unsigned)((n + block - 1) / block), block, 0, stream>>>(
+        n, slot, jd, center_chain, frame, out6, status);
+    return cuda_check(cudaGetLastError(), "spk_states_kernel launch");
+}
+
+}  // namespace kb
+
+namespace kb {
+
+// -------------------------------------------------------------------------------------------
+// FP64 pipe probe: independent DFMA chains, for the roofline denominator.  Each thread
+// runs 16 independent accumulators for `iters` iterations (2 flops per FMA).
+// -------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) dfma_probe_kernel(int64_t iters, double seed, double* out) {
+    double a[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) a[k] = seed + threadIdx.x * 1e-9 + k * 1e-7;
+    const double m = 0.999999999, c = 1e-9;
+    for (int64_t i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int k = 0; k < 16; ++k) a[k] = fma(a[k], m, c);
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) s += a[k];
+    if (s == 12345.678) out[0] = s;  // practically never true; keeps the chains live
+}
+
+int fp64_probe(int64_t iters, double* tflops, float* ms_out) {
+    int dev = 0, sms = 0;
+    int rc = cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    if (rc) return rc;
+    if ((rc = cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attr")))
+        return rc;
+    double* d_out = nullptr;
+    if ((rc = cuda_check(cudaMalloc(&d_out, sizeof(double)), "cudaMalloc probe"))) return rc;
+    const int block = 256, grid = sms * 8;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    dfma_probe_kernel<<<grid, block>>>(iters / 10, 1.0, d_out);  // warm-up
+    cudaEventRecord(e0);
+    dfma_probe_kernel<<<grid, block>>>(iters, 1.0, d_out);
+    cudaEventRecord(e1);
+    rc = cuda_check(cudaEventSynchronize(e1), "probe synchronize");
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(d_out);
+    if (rc) return rc;
+    const double flops = 2.0 * 16.0 * (double)iters * (double)grid * (double)block;
+    *tflops = flops / (ms * 1e-3) / 1e12;
+    if (ms_out) *ms_out = ms;
+    return 0;
+}
+
+}  // namespace kb

@@ -1,0 +1,218 @@
+"""kete's propagation entry points on the GPU.
+
+``propagate_two_body`` and ``propagate_n_body`` keep the signatures, argument meaning and
+error behaviour of kete's PyO3 functions (src/kete/rust/kepler.rs:68-108 and
+src/kete/rust/propagation.rs:70-151); the per-object rayon loop becomes one batched call
+into libketeb200.so.  The ``*_arrays`` functions are the batched forms on SoA arrays
+(numpy on the host or torch tensors already on the GPU).
+"""
+from __future__ import annotations
+
+import sys
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from .state import Frames, State, pack
+
+GMS = 0.00029591220828411956
+
+
+@dataclass(frozen=True)
+class NonGravModel:
+    """Non-gravitational force model (kete_core/propagation/nongrav.rs:12-61)."""
+
+    row: tuple
+
+    @staticmethod
+    def new_comet(a1=0.0, a2=0.0, a3=0.0, alpha=0.1112620426, r_0=2.808, m=2.15, n=5.093,
+                  k=4.6142, dt=0.0) -> "NonGravModel":
+        """JPL comet model, defaults as src/kete/rust/nongrav.rs:106-130."""
+        return NonGravModel((1.0, a1, a2, a3, alpha, r_0, m, n, k, dt))
+
+    @staticmethod
+    def new_asteroid(a1, a2, a3, alpha=1.0, r_0=1.0, m=2.0, n=1.0, k=0.0, dt=0.0):
+        """JPL model with g(r) = 1/r^2 defaults (src/kete/rust/nongrav.rs:132-157)."""
+        return NonGravModel((1.0, a1, a2, a3, alpha, r_0, m, n, k, dt))
+
+    @staticmethod
+    def new_dust(beta: float) -> "NonGravModel":
+        """Radiation pressure + Poynting-Robertson model (nongrav.rs:91-94)."""
+        return NonGravModel((2.0, beta, 0, 0, 0, 0, 0, 0, 0, 0))
+
+
+def _status_error(code: int, what: str):
+    return ValueError(f"{what}: {_lib.STATUS_NAMES.get(int(code), code)}")
+
+
+# ------------------------------------------------------------------------------------------
+# array forms
+# ------------------------------------------------------------------------------------------
+def _alloc_like(template, shape, dtype):
+    if _lib._is_torch_cuda(template):
+        import torch
+
+        tdt = {np.float64: torch.float64, np.int32: torch.int32}[dtype]
+        return torch.empty(shape, dtype=tdt, device=template.device)
+    return np.empty(shape, dtype=dtype)
+
+
+def propagate_two_body_arrays(pos, vel, jd0, jd1, observer_pos=None):
+    """Two-body propagation of n Sun-centred states (SoA (3, n) arrays), object i from
+    jd0[i] to jd1[i].  Returns (pos, vel, jd, status)."""
+    n = int(pos.shape[1])
+    _lib.init()
+    out_p = _alloc_like(pos, (3, n), np.float64)
+    out_v = _alloc_like(pos, (3, n), np.float64)
+    out_j = _alloc_like(pos, (n,), np.float64)
+    st = _alloc_like(pos, (n,), np.int32)
+    a = _lib.Args()
+    args = [a.ptr(pos), a.ptr(vel), a.ptr(jd0), a.ptr(jd1), a.ptr(observer_pos), a.ptr(out_p),
+            a.ptr(out_v), a.ptr(out_j), a.ptr(st, np.int32)]
+    _lib.check(_lib.lib().kete_b200_propagate_two_body(n, *args, a.on_device, a.stream))
+    return out_p, out_v, out_j, st
+
+
+def propagate_n_body_arrays(pos, vel, jd0, jd1, frame=Frames.Ecliptic, center=10,
+                            include_asteroids=False, nongrav=None, mode=_lib.MODE_AUTO,
+                            with_details=False):
+    """N-body Radau propagation of n states sharing ``frame`` and ``center``.
+
+    pos/vel: (3, n); jd0/jd1: (n,); nongrav: None or (10, n) rows.  Returns
+    (pos, vel, status) and, with ``with_details``, a dict with impact_id, impact_jd,
+    min_dist and counters (3, n: accepted steps, corrector iterations, exact evals)."""
+    n = int(pos.shape[1])
+    _lib.init()
+    out_p = _alloc_like(pos, (3, n), np.float64)
+    out_v = _alloc_like(pos, (3, n), np.float64)
+    st = _alloc_like(pos, (n,), np.int32)
+    det = None
+    if with_details:
+        det = dict(impact_id=_alloc_like(pos, (n,), np.int32),
+                   impact_jd=_alloc_like(pos, (n,), np.float64),
+                   min_dist=_alloc_like(pos, (n,), np.float64),
+                   counters=_alloc_like(pos, (3, n), np.int32))
+    a = _lib.Args()
+    args = [a.ptr(pos), a.ptr(vel), a.ptr(jd0), a.ptr(jd1)]
+    ng = a.ptr(nongrav)
+    outs = [a.ptr(out_p), a.ptr(out_v), a.ptr(st, np.int32)]
+    if det:
+        extra = [a.ptr(det["impact_id"], np.int32), a.ptr(det["impact_jd"]),
+                 a.ptr(det["min_dist"]), a.ptr(det["counters"], np.int32)]
+    else:
+        extra = [None, None, None, None]
+    _lib.check(_lib.lib().kete_b200_propagate_n_body(
+        n, *args, int(frame), int(center), int(bool(include_asteroids)), ng, *outs, *extra,
+        int(mode), a.on_device, a.stream))
+    if with_details:
+        return out_p, out_v, st, det
+    return out_p, out_v, st
+
+
+def radau_central_arrays(pos, vel, t0, t1):
+    """RadauIntegrator with the Sun-only force (kete_core/propagation/mod.rs:126-138)."""
+    n = int(pos.shape[1])
+    _lib.init()
+    out_p = _alloc_like(pos, (3, n), np.float64)
+    out_v = _alloc_like(pos, (3, n), np.float64)
+    st = _alloc_like(pos, (n,), np.int32)
+    a = _lib.Args()
+    args = [a.ptr(pos), a.ptr(vel), a.ptr(t0), a.ptr(t1), a.ptr(out_p), a.ptr(out_v),
+            a.ptr(st, np.int32)]
+    _lib.check(_lib.lib().kete_b200_radau_central(n, *args, a.on_device, a.stream))
+    return out_p, out_v, st
+
+
+# ------------------------------------------------------------------------------------------
+# kete-compatible State API
+# ------------------------------------------------------------------------------------------
+def _jd(jd) -> float:
+    return float(getattr(jd, "jd", jd))
+
+
+def propagate_two_body(states, jd, observer_pos=None):
+    """kete.propagate_two_body (src/kete/rust/kepler.rs:68-108).
+
+    States are moved to the Sun-centred frame they came in, propagated to ``jd`` (with
+    the light delay to ``observer_pos`` when given) and returned with their original
+    centre.  Failures give NaN states, as in the reference."""
+    jd = _jd(jd)
+    states = list(states)
+    if not states:
+        return []
+    from . import spice
+
+    out = [None] * len(states)
+    groups = {}
+    for i, s in enumerate(states):
+        groups.setdefault((int(s.frame), int(s.center_id)), []).append(i)
+    for (frame, center), idx in groups.items():
+        sub = [states[i] for i in idx]
+        pos, vel, jd0 = pack(sub)
+        ok = np.ones(len(sub), dtype=bool)
+        if center != 10:
+            shift0 = spice._center_shift(center, 10, jd0, frame)
+            ok &= shift0["ok"]
+            pos = pos - shift0["pos"]
+            vel = vel - shift0["vel"]
+        jd1 = np.full(len(sub), jd)
+        obs = None if observer_pos is None else np.asarray(observer_pos, dtype=np.float64).reshape(3).copy()
+        p, v, ojd, st = propagate_two_body_arrays(pos, vel, jd0, jd1, obs)
+        if center != 10:
+            shift1 = spice._center_shift(center, 10, ojd, frame)
+            ok &= shift1["ok"]
+            p = p + shift1["pos"]
+            v = v + shift1["vel"]
+        for k, i in enumerate(idx):
+            s = states[i]
+            if st[k] != 0 or not ok[k]:
+                out[i] = State.new_nan(s.desig, jd, s.frame, s.center_id)
+            else:
+                out[i] = State(s.desig, float(ojd[k]), p[:, k], v[:, k], s.frame, s.center_id)
+    return out
+
+
+def propagate_n_body(states, jd, include_asteroids=False, non_gravs=None, suppress_errors=True,
+                     suppress_impact_errors=False):
+    """kete.propagate_n_body (src/kete/rust/propagation.rs:70-151)."""
+    jd = _jd(jd)
+    states = list(states)
+    if non_gravs is None:
+        non_gravs = [None] * len(states)
+    non_gravs = list(non_gravs)
+    if len(non_gravs) != len(states):
+        raise ValueError("non_gravs must be the same length as states.")
+    out = [None] * len(states)
+    groups = {}
+    for i, s in enumerate(states):
+        if not s.is_finite:
+            if not suppress_errors:
+                raise ValueError("Input state contains NaNs.")
+            out[i] = State.new_nan(s.desig, jd, s.frame, s.center_id)
+            continue
+        groups.setdefault((int(s.frame), int(s.center_id)), []).append(i)
+    for (frame, center), idx in groups.items():
+        sub = [states[i] for i in idx]
+        pos, vel, jd0 = pack(sub)
+        ng = None
+        if any(non_gravs[i] is not None for i in idx):
+            ng = np.zeros((10, len(sub)))
+            for k, i in enumerate(idx):
+                if non_gravs[i] is not None:
+                    ng[:, k] = non_gravs[i].row
+        jd1 = np.full(len(sub), jd)
+        p, v, st, det = propagate_n_body_arrays(pos, vel, jd0, jd1, frame, center,
+                                                include_asteroids, ng, with_details=True)
+        for k, i in enumerate(idx):
+            s = states[i]
+            if st[k] == 0:
+                out[i] = State(s.desig, jd, p[:, k], v[:, k], s.frame, s.center_id)
+                continue
+            if not suppress_errors:
+                raise _status_error(st[k], f"propagation of {s.desig!r} failed")
+            if st[k] == _lib.IMPACT and not suppress_impact_errors:
+                print(f"Impact detected between ({s.desig!r}) <-> ({int(det['impact_id'][k])}) "
+                      f"at time {float(det['impact_jd'][k])}", file=sys.stderr)
+            out[i] = State.new_nan(s.desig, jd, s.frame, s.center_id)
+    return out

@@ -1,0 +1,54 @@
+"""Host-side logic that needs no GPU: State handling, synthetic inputs, argument checks."""
+import numpy as np
+import pytest
+
+
+def test_state_defaults():
+    from kete_b200 import Frames, State
+
+    s = State("a", 2460000.5, [1, 2, 3], [0.1, 0.2, 0.3])
+    assert s.frame == Frames.Ecliptic and s.center_id == 10 and s.is_finite
+    n = State.new_nan("b", 1.0)
+    assert not n.is_finite
+
+
+def test_frames_roundtrip():
+    from kete_b200.state import ecliptic_to_equatorial, equatorial_to_ecliptic
+
+    v = np.array([0.3, -1.2, 0.4])
+    np.testing.assert_allclose(equatorial_to_ecliptic(ecliptic_to_equatorial(v)), v, atol=1e-15)
+
+
+def test_population_matches_oracle_elements(oracle):
+    """The vectorised element conversion used for inputs agrees with the oracle's
+    restatement of CometElements::to_pos_vel."""
+    from kete_b200 import synthetic
+
+    rng = np.random.default_rng(3)
+    for _ in range(20):
+        a, e, i = rng.uniform(0.8, 3.3), rng.uniform(0, 0.6), rng.uniform(0, 0.5)
+        lan, argp, m = rng.uniform(0, 2 * np.pi, 3)
+        q = a * (1 - e)
+        tp = 2460000.5 - m / (a**-1.5 * synthetic.GMS_SQRT)
+        p, v = synthetic.elements_to_state(2460000.5, e, i, lan, tp, argp, q)
+        rc, po, vo = oracle.elements_to_state(2460000.5, e, i, lan, tp, argp, q)
+        assert rc == 0
+        np.testing.assert_allclose(p, po, atol=1e-11)
+        np.testing.assert_allclose(v, vo, atol=1e-13)
+
+
+def test_mixed_population_shape():
+    from kete_b200 import synthetic
+
+    pos, vel, ng = synthetic.mixed(1000, seed=1)
+    assert pos.shape == (3, 1000) and ng.shape == (10, 1000)
+    frac = (ng[0] == 1).mean()
+    assert 0.02 < frac < 0.09
+
+
+def test_host_arrays_must_be_float64():
+    from kete_b200 import _lib
+
+    a = _lib.Args()
+    with pytest.raises(TypeError):
+        a.ptr(np.zeros(3, dtype=np.float32))
