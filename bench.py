@@ -309,7 +309,11 @@ def run_gpu(args, world, rank, local):
         "gpu_launches": args.steps,
         "clocks": clk.summary(),
         "parity": {"max_err_au": float(err[ok].max()) if ok.any() else None,
-                   "status_match": bool((st_h == st_cpu).all()), "tolerance_au": 1e-9},
+                   "status_match": bool((st_h == st_cpu).all()),
+                   "status_mismatches": int((st_h != st_cpu).sum()),
+                   "gpu_status_counts": np.bincount(st_h, minlength=8).tolist(),
+                   "cpu_status_counts": np.bincount(st_cpu, minlength=8).tolist(),
+                   "tolerance_au": 1e-9},
         "mem_peaks_hbm_gbs": peaks.get("hbm_gbs"),
     }
     print(json.dumps(line), flush=True)

@@ -109,8 +109,10 @@ class Args:
         if self.device is True:
             raise ValueError("mixing host and device arrays in one call")
         self.device = False
-        if not (isinstance(a, np.ndarray) and a.dtype == dtype and a.flags.c_contiguous):
-            raise TypeError("host arrays must be C-contiguous numpy arrays of " + str(dtype))
+        if not isinstance(a, np.ndarray) or a.dtype != dtype:
+            raise TypeError("host arrays must be numpy arrays of " + np.dtype(dtype).name)
+        if not a.flags.c_contiguous:
+            a = np.ascontiguousarray(a)  # inputs only: outputs are allocated contiguous
         self.keep.append(a)
         return a.ctypes.data
 

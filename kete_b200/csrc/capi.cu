@@ -594,8 +594,13 @@ int kete_b200_propagate_n_body(int64_t n, const double* pos, const double* vel, 
     a.counters = S.out(counters, 3 * (size_t)n);
     a.max_loops = 1 << 20;
     if (S.rc) return S.rc;
-    (void)mode;
-    if ((rc = launch_nbody_thread(a, 128, st))) return rc;
+    if (mode == KETE_B200_MODE_THREAD) {
+        if ((rc = launch_nbody_thread(a, 128, st))) return rc;
+    } else if (mode == KETE_B200_MODE_NODES || mode == KETE_B200_MODE_AUTO) {
+        if ((rc = launch_nbody_nodes(a, 128, 0, st))) return rc;
+    } else {
+        return set_error(KETE_B200_E_ARGUMENT, "unknown propagation mode");
+    }
     return S.finish();
 }
 

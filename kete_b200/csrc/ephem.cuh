@@ -46,6 +46,12 @@ struct ForceEntry {
     int32_t slot, kind, naif_id, pad_;
 };
 
+// Chain of SPK slots from a state's centre up to the barycentre (empty for centre 0).
+struct CenterChain {
+    int len = 0;
+    int slot[3] = {-1, -1, -1};
+};
+
 struct EphemConst {
     int32_t n_seg, n_slot;
     int32_t n_force_planets, n_force_all;  // PLANETS (10) and MASSES (15) lengths
@@ -127,7 +133,9 @@ __device__ __forceinline__ int eph_raw(const EphemConst& E, int slot, double jd,
     for (int q = 0; q < s.count; ++q) {
         const SegDesc& d = E.seg[s.first + q];
         if (jd >= d.jd_start && jd <= d.jd_end) {
-            const double jds = (jd - 2451545.0) * 86400.0;
+            // jd_to_spice_jd (spice/mod.rs:31-34), rounded as the reference rounds it: an
+            // explicit multiply so the compiler cannot fuse it into the subtraction below
+            const double jds = __dmul_rn(jd - 2451545.0, 86400.0);
             double fidx = floor((jds - d.start_s) / d.intlen);
             int idx = fidx < 0.0 ? 0 : (fidx >= (double)d.n_rec ? d.n_rec - 1 : (int)fidx);
             const double* rec = E.pool + d.offset + (int64_t)idx * d.rsize;

@@ -68,8 +68,12 @@ struct NonGrav {
     __device__ __forceinline__ double p(int k) const { return __ldg(base + (int64_t)k * stride); }
 };
 
-__device__ __noinline__ void nongrav_add(const NonGrav& ng, double acc[3], const double pos_in[3],
-                                         const double vel[3]) {
+// Returns the non-gravitational acceleration (added by the caller), so that no array of the
+// caller has its address taken by this out-of-line function.
+__device__ __noinline__ double3 nongrav_accel(const NonGrav ng, const double3 rp, const double3 rv) {
+    const double pos_in[3] = {rp.x, rp.y, rp.z};
+    const double vel[3] = {rv.x, rv.y, rv.z};
+    double acc[3] = {0.0, 0.0, 0.0};
     if (ng.kind == 2) {
         const double beta = ng.p(1);
         const double n = norm3(pos_in[0], pos_in[1], pos_in[2]);
@@ -82,7 +86,7 @@ __device__ __noinline__ void nongrav_add(const NonGrav& ng, double acc[3], const
         for (int i = 0; i < 3; ++i)
             acc[i] += scaling * ((1.0 - r_dot * C_AU_PER_DAY_INV_SQUARED) * pn[i] -
                                  vel[i] * C_AU_PER_DAY_INV_SQUARED);
-        return;
+        return make_double3(acc[0], acc[1], acc[2]);
     }
     const double a1 = ng.p(1), a2 = ng.p(2), a3 = ng.p(3), alpha = ng.p(4), r_0 = ng.p(5);
     const double m = ng.p(6), nn = ng.p(7), k = ng.p(8), dt = ng.p(9);
@@ -113,6 +117,62 @@ __device__ __noinline__ void nongrav_add(const NonGrav& ng, double acc[3], const
     for (int i = 0; i < 3; ++i) acc[i] += t_vec[i] * (scale * a2);
 #pragma unroll
     for (int i = 0; i < 3; ++i) acc[i] += n_vec[i] * (scale * a3);
+    return make_double3(acc[0], acc[1], acc[2]);
+}
+
+// -------------------------------------------------------------------------------------------
+// centre / frame changes around the integration (kete_core/propagation/mod.rs:76-80,
+// 107-116 with SpkCollection::try_change_center, spk.rs:99-126, and State::try_change_center,
+// state.rs:242-281): the SPK states are expressed in the object's frame before they are
+// added, then the sum is rotated into the integration frame (equatorial).
+// -------------------------------------------------------------------------------------------
+__device__ __forceinline__ int to_ssb_equatorial(double t, int frame, const CenterChain& ch,
+                                                 double p[3], double v[3]) {
+    for (int k = 0; k < ch.len; ++k) {
+        double sp[3], sv[3];
+        if (eph_raw(c_eph, ch.slot[k], t, sp, sv) != ST_OK) return ST_DAF_LIMITS;
+        if (frame == FRAME_ECLIPTIC) {
+            double q[3];
+            eq_to_ecl(sp, q);
+            sp[0] = q[0]; sp[1] = q[1]; sp[2] = q[2];
+            eq_to_ecl(sv, q);
+            sv[0] = q[0]; sv[1] = q[1]; sv[2] = q[2];
+        }
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            p[i] += sp[i];
+            v[i] += sv[i];
+        }
+    }
+    if (frame == FRAME_ECLIPTIC) {
+        double q[3];
+        ecl_to_eq(p, q);
+        p[0] = q[0]; p[1] = q[1]; p[2] = q[2];
+        ecl_to_eq(v, q);
+        v[0] = q[0]; v[1] = q[1]; v[2] = q[2];
+    }
+    return ST_OK;
+}
+
+__device__ __forceinline__ int from_ssb_equatorial(double t, int frame, const CenterChain& ch,
+                                                   double p[3], double v[3]) {
+    for (int k = ch.len - 1; k >= 0; --k) {
+        double sp[3], sv[3];
+        if (eph_raw(c_eph, ch.slot[k], t, sp, sv) != ST_OK) return ST_DAF_LIMITS;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            p[i] += -sp[i];
+            v[i] += -sv[i];
+        }
+    }
+    if (frame == FRAME_ECLIPTIC) {
+        double q[3];
+        eq_to_ecl(p, q);
+        p[0] = q[0]; p[1] = q[1]; p[2] = q[2];
+        eq_to_ecl(v, q);
+        v[0] = q[0]; v[1] = q[1]; v[2] = q[2];
+    }
+    return ST_OK;
 }
 
 // Acceleration from the SPK perturbers.  exact=true marks the evaluations at the
@@ -174,7 +234,13 @@ struct SpkForce {
                 acc[0] += j2q[0];
                 acc[1] += j2q[1];
                 acc[2] += j2q[2];
-                if (fe.kind == FK_SUN && ng.kind != 0) nongrav_add(ng, acc, rp, rv);
+                if (fe.kind == FK_SUN && ng.kind != 0) {
+                    const double3 na = nongrav_accel(ng, make_double3(rp[0], rp[1], rp[2]),
+                                                     make_double3(rv[0], rv[1], rv[2]));
+                    acc[0] += na.x;
+                    acc[1] += na.y;
+                    acc[2] += na.z;
+                }
             } else if (fe.kind == FK_EARTH) {
                 double j2[3];
                 j2_correction(rp, fe.radius, EARTH_J2, mass, j2);

@@ -6,6 +6,8 @@
 
 #include <cuda_runtime.h>
 
+#include "ephem.cuh"
+
 namespace kb {
 
 struct Tables;
@@ -18,11 +20,6 @@ int cuda_check(cudaError_t e, const char* what);
 // kernels.cu
 int upload_tables(const Tables& t);
 int upload_ephem(const EphemConst& e);
-
-struct CenterChain {
-    int len = 0;
-    int slot[3] = {-1, -1, -1};
-};
 
 struct NBodyArgs {
     int64_t n;
@@ -41,13 +38,17 @@ struct NBodyArgs {
     double* impact_jd;    // may be null
     double* min_dist;     // may be null
     int32_t* counters;    // 3 x n (steps, iterations, exact evals) or null
-    int max_loops;
+    int max_loops;        // step-loop bound per object (ST_TIMEOUT beyond)
+    int* queue;           // refill counter for the node kernel (null: one object per group)
+    const int32_t* order; // processing order (permutation of 0..n-1) or null
 };
 
 int launch_two_body(int64_t n, const double* pos, const double* vel, const double* jd0,
                     const double* jd1, const double* obs, double* out_pos, double* out_vel,
                     double* out_jd, int32_t* status, cudaStream_t stream);
 int launch_nbody_thread(const NBodyArgs& a, int block, cudaStream_t stream);
+int launch_nbody_nodes(const NBodyArgs& a, int block, int grid, cudaStream_t stream);
+int nodes_grid_size(int block, int* grid);
 int launch_radau_central(int64_t n, const double* pos, const double* vel, const double* t0,
                          const double* t1, double* out_pos, double* out_vel, int32_t* status,
                          cudaStream_t stream);

@@ -9,6 +9,7 @@
 #include "internal.h"
 #include "kepler.cuh"
 #include "radau.cuh"
+#include "radau_nodes.cuh"
 
 namespace kb {
 
@@ -65,61 +66,6 @@ int launch_two_body(int64_t n, const double* pos, const double* vel, const doubl
     two_body_kernel<<<(unsigned)grid, block, 0, stream>>>(n, pos, vel, jd0, jd1, obs, out_pos,
                                                           out_vel, out_jd, status);
     return cuda_check(cudaGetLastError(), "two_body_kernel launch");
-}
-
-// -------------------------------------------------------------------------------------------
-// centre / frame changes around the integration (kete_core/propagation/mod.rs:76-80,
-// 107-116 with SpkCollection::try_change_center, spk.rs:99-126, and State::try_change_center,
-// state.rs:242-281): the SPK states are expressed in the object's frame before they are
-// added, then the sum is rotated into the integration frame (equatorial).
-// -------------------------------------------------------------------------------------------
-__device__ __forceinline__ int to_ssb_equatorial(double t, int frame, const CenterChain& ch,
-                                                 double p[3], double v[3]) {
-    for (int k = 0; k < ch.len; ++k) {
-        double sp[3], sv[3];
-        if (eph_raw(c_eph, ch.slot[k], t, sp, sv) != ST_OK) return ST_DAF_LIMITS;
-        if (frame == FRAME_ECLIPTIC) {
-            double q[3];
-            eq_to_ecl(sp, q);
-            sp[0] = q[0]; sp[1] = q[1]; sp[2] = q[2];
-            eq_to_ecl(sv, q);
-            sv[0] = q[0]; sv[1] = q[1]; sv[2] = q[2];
-        }
-#pragma unroll
-        for (int i = 0; i < 3; ++i) {
-            p[i] += sp[i];
-            v[i] += sv[i];
-        }
-    }
-    if (frame == FRAME_ECLIPTIC) {
-        double q[3];
-        ecl_to_eq(p, q);
-        p[0] = q[0]; p[1] = q[1]; p[2] = q[2];
-        ecl_to_eq(v, q);
-        v[0] = q[0]; v[1] = q[1]; v[2] = q[2];
-    }
-    return ST_OK;
-}
-
-__device__ __forceinline__ int from_ssb_equatorial(double t, int frame, const CenterChain& ch,
-                                                   double p[3], double v[3]) {
-    for (int k = ch.len - 1; k >= 0; --k) {
-        double sp[3], sv[3];
-        if (eph_raw(c_eph, ch.slot[k], t, sp, sv) != ST_OK) return ST_DAF_LIMITS;
-#pragma unroll
-        for (int i = 0; i < 3; ++i) {
-            p[i] += -sp[i];
-            v[i] += -sv[i];
-        }
-    }
-    if (frame == FRAME_ECLIPTIC) {
-        double q[3];
-        eq_to_ecl(p, q);
-        p[0] = q[0]; p[1] = q[1]; p[2] = q[2];
-        eq_to_ecl(v, q);
-        v[0] = q[0]; v[1] = q[1]; v[2] = q[2];
-    }
-    return ST_OK;
 }
 
 // -------------------------------------------------------------------------------------------
@@ -298,6 +244,35 @@ int fp64_probe(int64_t iters, double* tflops, float* ms_out) {
     const double flops = 2.0 * 16.0 * (double)iters * (double)grid * (double)block;
     *tflops = flops / (ms * 1e-3) / 1e12;
     if (ms_out) *ms_out = ms;
+    return 0;
+}
+
+}  // namespace kb
+
+namespace kb {
+
+// Node-parallel Radau: 8 lanes per object.  With a.queue == null each group integrates one
+// object (grid covers n groups); with a queue the grid is persistent and groups refill.
+int launch_nbody_nodes(const NBodyArgs& a, int block, int grid, cudaStream_t stream) {
+    if (a.n <= 0) return 0;
+    if (block <= 0) block = 128;
+    if (grid <= 0) grid = (int)((a.n * NODE_G + block - 1) / block);
+    nbody_nodes_kernel<<<grid, block, 0, stream>>>(a);
+    return cuda_check(cudaGetLastError(), "nbody_nodes_kernel launch");
+}
+
+// Resident grid for the persistent (refill) form: blocks per SM from the occupancy API.
+int nodes_grid_size(int block, int* grid) {
+    int dev = 0, sms = 0, per_sm = 0;
+    int rc = cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    if (rc) return rc;
+    if ((rc = cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attr")))
+        return rc;
+    if ((rc = cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, nbody_nodes_kernel,
+                                                                         block, 0),
+                         "occupancy")))
+        return rc;
+    *grid = sms * (per_sm > 0 ? per_sm : 1);
     return 0;
 }
 

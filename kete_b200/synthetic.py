@@ -145,7 +145,8 @@ def mixed(n, seed=0, neo_frac=0.1, nongrav_frac=0.05, epoch=EPOCH):
     pos = np.concatenate([pm, pn], axis=1)
     vel = np.concatenate([vm, vn], axis=1)
     perm = rng.permutation(n)
-    pos, vel = pos[:, perm], vel[:, perm]
+    pos = np.ascontiguousarray(pos[:, perm])
+    vel = np.ascontiguousarray(vel[:, perm])
     ng = np.zeros((10, n))
     has = rng.random(n) < nongrav_frac
     k = int(has.sum())

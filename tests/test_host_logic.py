@@ -52,3 +52,6 @@ def test_host_arrays_must_be_float64():
     a = _lib.Args()
     with pytest.raises(TypeError):
         a.ptr(np.zeros(3, dtype=np.float32))
+    # non-contiguous float64 inputs are copied, not rejected
+    m = np.zeros((3, 8))[:, ::2]
+    assert a.ptr(m) != 0 and a.keep[-1].flags.c_contiguous
