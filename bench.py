@@ -221,7 +221,15 @@ def run_gpu(args, world, rank, local):
     dev = torch.device("cuda", local)
     d = {k: torch.from_numpy(np.ascontiguousarray(v)).to(dev)
          for k, v in dict(pos=pos, vel=vel, jd0=jd0, jd1=jd1).items()}
-    mode = args.mode
+    from kete_b200 import tune
+
+    sweep = None
+    if args.mode == 0:
+        best, sweep = tune.autotune(d["pos"], d["vel"], d["jd0"], d["jd1"])
+    else:
+        best = dict(mode=args.mode, variant=args.variant, refill=args.refill)
+        tune.set_config(**best)
+    mode = best["mode"]
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
 
     def step():
@@ -294,7 +302,8 @@ def run_gpu(args, world, rank, local):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"plain N-body Radau, {n} main-belt states x {SPAN} d per GPU, "
                    "Sun+8 planets+Moon from a synthetic SPK type-2 file (14-coef records)",
-                   "n_objects_per_gpu": n, "span_days": SPAN, "mode": mode,
+                   "n_objects_per_gpu": n, "span_days": SPAN, "launch": best,
+                   "autotune_sweep_ms": sweep,
                    "l2": "flushed (256 MB write) between timed steps",
                    "parallelism": f"replicas x{world} (objects independent)"},
         "object_steps_per_s": world * steps_total * args.steps / t_total,
@@ -337,7 +346,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="kete_b200", choices=["kete_b200", "reference"])
     ap.add_argument("--n", type=int, default=10_000)
-    ap.add_argument("--mode", type=int, default=0)
+    ap.add_argument("--mode", type=int, default=0, help="0 = autotune, 1 = thread, 2 = nodes")
+    ap.add_argument("--variant", type=int, default=0)
+    ap.add_argument("--refill", type=int, default=0)
     args = ap.parse_args()
     world, rank, local = dist_setup() if args.impl == "kete_b200" else (
         int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0)

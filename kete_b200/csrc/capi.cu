@@ -83,6 +83,8 @@ struct DevState {
 };
 
 static std::mutex g_mu;
+static LaunchConfig g_launch;
+LaunchConfig& launch_config() { return g_launch; }
 static std::vector<HostSeg> g_segs;
 static int g_version = 0;
 static int g_skipped = 0;
@@ -211,6 +213,7 @@ static int rebuild_tables() {
             d.jd_end = s.jd_end;
             d.start_s = s.start_s;
             d.intlen = s.intlen;
+            d.inv_intlen = 1.0 / s.intlen;
             d.n_coef = (int32_t)s.n_coef;
             d.n_pad = (int32_t)((s.n_coef + 1) & ~1LL);
             d.n_rec = (int32_t)s.n_rec;
@@ -595,9 +598,20 @@ int kete_b200_propagate_n_body(int64_t n, const double* pos, const double* vel, 
     a.max_loops = 1 << 20;
     if (S.rc) return S.rc;
     if (mode == KETE_B200_MODE_THREAD) {
-        if ((rc = launch_nbody_thread(a, 128, st))) return rc;
+        if ((rc = launch_nbody_thread(a, g_launch.thread_block, st))) return rc;
     } else if (mode == KETE_B200_MODE_NODES || mode == KETE_B200_MODE_AUTO) {
-        if ((rc = launch_nbody_nodes(a, 128, 0, st))) return rc;
+        int grid = 0;
+        if (g_launch.nodes_refill) {
+            // persistent grid; the object queue counter is a 4-byte scratch word
+            void* q = nullptr;
+            if ((rc = staging(*ds, 31, sizeof(int), &q))) return rc;
+            if ((rc = cuda_check(cudaMemsetAsync(q, 0, sizeof(int), st), "reset object queue"))) return rc;
+            a.queue = (int*)q;
+            if ((rc = nodes_grid_size(g_launch.nodes_variant, &grid))) return rc;
+            const int64_t need = (n * 8 + 127) / 128;
+            if (grid > need) grid = (int)need;
+        }
+        if ((rc = launch_nbody_nodes(a, g_launch.nodes_variant, grid, st))) return rc;
     } else {
         return set_error(KETE_B200_E_ARGUMENT, "unknown propagation mode");
     }
@@ -626,6 +640,17 @@ int kete_b200_radau_central(int64_t n, const double* pos, const double* vel, con
     if (S.rc) return S.rc;
     if ((rc = launch_radau_central(n, d_p, d_v, d_t0, d_t1, d_op, d_ov, d_st, st))) return rc;
     return S.finish();
+}
+
+int kete_b200_set_launch_config(int nodes_variant, int nodes_refill, int thread_block) {
+    if (nodes_variant < 0 || nodes_variant > 2 || thread_block < 32 || thread_block > 1024 ||
+        thread_block % 32)
+        return set_error(KETE_B200_E_ARGUMENT, "bad launch configuration");
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_launch.nodes_variant = nodes_variant;
+    g_launch.nodes_refill = nodes_refill ? 1 : 0;
+    g_launch.thread_block = thread_block;
+    return 0;
 }
 
 int kete_b200_fp64_probe(int64_t iters, double* tflops, float* ms) {

@@ -25,6 +25,7 @@ struct SegDesc {
     double jd_start, jd_end;  // JD, as spice_jds_to_jd(summary) (spice/mod.rs:25-28)
     double start_s;           // jd_to_spice_jd(jd_start), what the reference indexes from
     double intlen;            // record length in seconds (INTLEN)
+    double inv_intlen;        // 1 / intlen
     int64_t offset;           // doubles into the pool of record 0
     int32_t n_coef, n_pad, n_rec, rsize;
 };
@@ -136,7 +137,9 @@ __device__ __forceinline__ int eph_raw(const EphemConst& E, int slot, double jd,
             // jd_to_spice_jd (spice/mod.rs:31-34), rounded as the reference rounds it: an
             // explicit multiply so the compiler cannot fuse it into the subtraction below
             const double jds = __dmul_rn(jd - 2451545.0, 86400.0);
-            double fidx = floor((jds - d.start_s) / d.intlen);
+            // record index floor((t - start) / intlen) (spk_segments.rs:358); the quotient
+            // is formed with the tabulated reciprocal
+            double fidx = floor((jds - d.start_s) * d.inv_intlen);
             int idx = fidx < 0.0 ? 0 : (fidx >= (double)d.n_rec ? d.n_rec - 1 : (int)fidx);
             const double* rec = E.pool + d.offset + (int64_t)idx * d.rsize;
             cheb_record(rec, d.n_coef, d.n_pad, jds, p, v);

@@ -175,23 +175,27 @@ __device__ __forceinline__ int from_ssb_equatorial(double t, int frame, const Ce
     return ST_OK;
 }
 
-// Acceleration from the SPK perturbers.  exact=true marks the evaluations at the
-// integrator's accepted states: only those check for impacts (r <= body radius) and
-// update the closest-approach record.
+// Acceleration from the SPK perturbers.  `exact` marks the evaluations at the integrator's
+// accepted states: only those check for impacts (r <= body radius, acceleration.rs:147-158)
+// and update the closest-approach record.  The flag is a runtime value so that one copy of
+// the force code serves every call site.
+//
+// Distances use one reciprocal square root per body: r = r2 * rsqrt(r2) and r^-3 =
+// rsqrt(r2)^3 replace the reference's sqrt and 1/(r*r*r) (a few ulp apart).
 struct SpkForce {
     int n_force;
     NonGrav ng;
     // outputs of exact evaluations
-    mutable int32_t impact_id;
-    mutable double min_dist;  // smallest distance to a non-Sun body seen at exact evals
-    mutable int32_t min_id;
+    int32_t impact_id;
+    double min_dist;  // smallest distance to a non-Sun body seen at exact evals
+    int32_t min_id;
 
-    template <bool EXACT>
-    __device__ __forceinline__ int eval(double t, const double x[3], const double v[3],
-                                        double out[3]) const {
+    __device__ __forceinline__ int eval(bool exact, double t, const double x[3], const double v[3],
+                                        double out[3]) {
         double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
         int cache_slot = -1;
-        double cp[3] = {0.0, 0.0, 0.0}, cv[3] = {0.0, 0.0, 0.0};
+        double cp0 = 0.0, cp1 = 0.0, cp2 = 0.0, cv0 = 0.0, cv1 = 0.0, cv2 = 0.0;
+#pragma unroll 1
         for (int b = 0; b < n_force; ++b) {
             const ForceEntry fe = c_eph.force[b];
             const int slot = fe.slot;
@@ -200,19 +204,22 @@ struct SpkForce {
             const int parent = c_eph.slot[slot].parent_slot;
             if (parent >= 0) {
                 if (parent != cache_slot) {
-                    if (eph_raw(c_eph, parent, t, cp, cv) != ST_OK) return ST_DAF_LIMITS;
+                    double q[3], w[3];
+                    if (eph_raw(c_eph, parent, t, q, w) != ST_OK) return ST_DAF_LIMITS;
+                    cp0 = q[0]; cp1 = q[1]; cp2 = q[2];
+                    cv0 = w[0]; cv1 = w[1]; cv2 = w[2];
                     cache_slot = parent;
                 }
-#pragma unroll
-                for (int i = 0; i < 3; ++i) {
-                    bp[i] += cp[i];
-                    bv[i] += cv[i];
-                }
+                bp[0] += cp0; bp[1] += cp1; bp[2] += cp2;
+                bv[0] += cv0; bv[1] += cv1; bv[2] += cv2;
             }
             const double rp[3] = {x[0] - bp[0], x[1] - bp[1], x[2] - bp[2]};
             const double rv[3] = {v[0] - bv[0], v[1] - bv[1], v[2] - bv[2]};
-            const double r = norm3(rp[0], rp[1], rp[2]);
-            if (EXACT) {
+            const double r2 = rp[0] * rp[0] + rp[1] * rp[1] + rp[2] * rp[2];
+            const double ir = rsqrt(r2);
+            const double r = r2 * ir;
+            const double ir3 = ir * ir * ir;
+            if (exact) {
                 if (r <= fe.radius) {
                     impact_id = fe.naif_id;
                     return ST_IMPACT;
@@ -223,34 +230,50 @@ struct SpkForce {
                 }
             }
             const double mass = fe.mass;
-            const double kk = mass * powi<-3>(r);
-            double acc[3] = {acc0 - rp[0] * kk, acc1 - rp[1] * kk, acc2 - rp[2] * kk};
+            const double kk = mass * ir3;
+            acc0 -= rp[0] * kk;
+            acc1 -= rp[1] * kk;
+            acc2 -= rp[2] * kk;
             if (fe.kind == FK_SUN || fe.kind == FK_JUPITER) {
-                apply_gr(acc, rp, rv, mass, r);
-                double re[3], j2[3], j2q[3];
-                eq_to_ecl(rp, re);
-                j2_correction(re, fe.radius, fe.kind == FK_JUPITER ? JUPITER_J2 : SUN_J2, mass, j2);
-                ecl_to_eq(j2, j2q);
-                acc[0] += j2q[0];
-                acc[1] += j2q[1];
-                acc[2] += j2q[2];
+                // apply_gr_correction (gravity.rs:239-253)
+                const double r_v = 4.0 * (rp[0] * rv[0] + rp[1] * rv[1] + rp[2] * rv[2]);
+                const double rel_v2 = rv[0] * rv[0] + rv[1] * rv[1] + rv[2] * rv[2];
+                const double gr_const = mass * C_AU_PER_DAY_INV_SQUARED * ir3;
+                const double c = 4. * mass * ir - rel_v2;
+                acc0 += gr_const * (c * rp[0] + r_v * rv[0]);
+                acc1 += gr_const * (c * rp[1] + r_v * rv[1]);
+                acc2 += gr_const * (c * rp[2] + r_v * rv[2]);
+                // J2 in the ecliptic frame (gravity.rs:188-211, 223-235)
+                const double rc = c_tab.rot_c, rs = c_tab.rot_s;
+                const double ez = -rs * rp[1] + rc * rp[2];
+                const double zr = ez * ir;
+                const double z_squared = 5.0 * (zr * zr);
+                const double rr = fe.radius * ir;
+                const double coef = 1.5 * (fe.kind == FK_JUPITER ? JUPITER_J2 : SUN_J2) * mass *
+                                    (rr * rr) * ir3;
+                const double ey = rc * rp[1] + rs * rp[2];
+                const double jx = rp[0] * coef * (z_squared - 1.0);
+                const double jy = ey * coef * (z_squared - 1.0);
+                const double jz = ez * coef * (z_squared - 3.0);
+                acc0 += jx;
+                acc1 += rc * jy - rs * jz;
+                acc2 += rs * jy + rc * jz;
                 if (fe.kind == FK_SUN && ng.kind != 0) {
                     const double3 na = nongrav_accel(ng, make_double3(rp[0], rp[1], rp[2]),
                                                      make_double3(rv[0], rv[1], rv[2]));
-                    acc[0] += na.x;
-                    acc[1] += na.y;
-                    acc[2] += na.z;
+                    acc0 += na.x;
+                    acc1 += na.y;
+                    acc2 += na.z;
                 }
             } else if (fe.kind == FK_EARTH) {
-                double j2[3];
-                j2_correction(rp, fe.radius, EARTH_J2, mass, j2);
-                acc[0] += j2[0];
-                acc[1] += j2[1];
-                acc[2] += j2[2];
+                const double zr = rp[2] * ir;
+                const double z_squared = 5.0 * (zr * zr);
+                const double rr = fe.radius * ir;
+                const double coef = 1.5 * EARTH_J2 * mass * (rr * rr) * ir3;
+                acc0 += rp[0] * coef * (z_squared - 1.0);
+                acc1 += rp[1] * coef * (z_squared - 1.0);
+                acc2 += rp[2] * coef * (z_squared - 3.0);
             }
-            acc0 = acc[0];
-            acc1 = acc[1];
-            acc2 = acc[2];
         }
         out[0] = acc0;
         out[1] = acc1;
@@ -261,12 +284,11 @@ struct SpkForce {
 
 // central_accel (acceleration.rs:66-80): the Sun at the origin only.
 struct CentralForce {
-    mutable int32_t impact_id;
-    mutable double min_dist;
-    mutable int32_t min_id;
-    template <bool EXACT>
-    __device__ __forceinline__ int eval(double, const double x[3], const double[3],
-                                        double out[3]) const {
+    int32_t impact_id;
+    double min_dist;
+    int32_t min_id;
+    __device__ __forceinline__ int eval(bool, double, const double x[3], const double[3],
+                                        double out[3]) {
         const double k = powi<-3>(norm3(x[0], x[1], x[2]));
         out[0] = -x[0] * k * GMS;
         out[1] = -x[1] * k * GMS;

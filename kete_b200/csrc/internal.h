@@ -47,8 +47,16 @@ int launch_two_body(int64_t n, const double* pos, const double* vel, const doubl
                     const double* jd1, const double* obs, double* out_pos, double* out_vel,
                     double* out_jd, int32_t* status, cudaStream_t stream);
 int launch_nbody_thread(const NBodyArgs& a, int block, cudaStream_t stream);
-int launch_nbody_nodes(const NBodyArgs& a, int block, int grid, cudaStream_t stream);
-int nodes_grid_size(int block, int* grid);
+int launch_nbody_nodes(const NBodyArgs& a, int variant, int grid, cudaStream_t stream);
+int nodes_grid_size(int variant, int* grid);
+
+// launch configuration chosen by the tuner (kete_b200_set_launch_config)
+struct LaunchConfig {
+    int nodes_variant = 0;  // register cap of the node kernel (see launch_nbody_nodes)
+    int nodes_refill = 0;   // 1: persistent grid with an object queue
+    int thread_block = 128;
+};
+LaunchConfig& launch_config();
 int launch_radau_central(int64_t n, const double* pos, const double* vel, const double* t0,
                          const double* t1, double* out_pos, double* out_vel, int32_t* status,
                          cudaStream_t stream);

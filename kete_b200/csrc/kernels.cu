@@ -136,6 +136,9 @@ __global__ void radau_central_kernel(int64_t n, const double* pos, const double*
     s.x[0] = pos[i]; s.x[1] = pos[n + i]; s.x[2] = pos[2 * n + i];
     s.v[0] = vel[i]; s.v[1] = vel[n + i]; s.v[2] = vel[2 * n + i];
     CentralForce F;
+    F.impact_id = 0;
+    F.min_dist = 0.0;
+    F.min_id = 0;
     RadauCounters cnt;
     int rc = radau_integrate(s, t1[i], F, cnt, 1 << 20);
     out_pos[i] = s.x[0]; out_pos[n + i] = s.x[1]; out_pos[2 * n + i] = s.x[2];
@@ -253,23 +256,36 @@ namespace kb {
 
 // Node-parallel Radau: 8 lanes per object.  With a.queue == null each group integrates one
 // object (grid covers n groups); with a queue the grid is persistent and groups refill.
-int launch_nbody_nodes(const NBodyArgs& a, int block, int grid, cudaStream_t stream) {
+// variant: 0 = no register cap, 1 = >= 3 blocks/SM (168 registers), 2 = >= 4 blocks/SM.
+static const void* nodes_kernel_ptr(int variant) {
+    switch (variant) {
+        case 1: return (const void*)nbody_nodes_kernel<3>;
+        case 2: return (const void*)nbody_nodes_kernel<4>;
+        default: return (const void*)nbody_nodes_kernel<1>;
+    }
+}
+
+int launch_nbody_nodes(const NBodyArgs& a, int variant, int grid, cudaStream_t stream) {
     if (a.n <= 0) return 0;
-    if (block <= 0) block = 128;
+    const int block = NODES_BLOCK;
     if (grid <= 0) grid = (int)((a.n * NODE_G + block - 1) / block);
-    nbody_nodes_kernel<<<grid, block, 0, stream>>>(a);
+    switch (variant) {
+        case 1: nbody_nodes_kernel<3><<<grid, block, 0, stream>>>(a); break;
+        case 2: nbody_nodes_kernel<4><<<grid, block, 0, stream>>>(a); break;
+        default: nbody_nodes_kernel<1><<<grid, block, 0, stream>>>(a); break;
+    }
     return cuda_check(cudaGetLastError(), "nbody_nodes_kernel launch");
 }
 
 // Resident grid for the persistent (refill) form: blocks per SM from the occupancy API.
-int nodes_grid_size(int block, int* grid) {
+int nodes_grid_size(int variant, int* grid) {
     int dev = 0, sms = 0, per_sm = 0;
     int rc = cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
     if (rc) return rc;
     if ((rc = cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attr")))
         return rc;
-    if ((rc = cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, nbody_nodes_kernel,
-                                                                         block, 0),
+    if ((rc = cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                             &per_sm, nodes_kernel_ptr(variant), NODES_BLOCK, 0),
                          "occupancy")))
         return rc;
     *grid = sms * (per_sm > 0 ? per_sm : 1);

@@ -26,7 +26,7 @@ struct RadauObj {
 };
 
 template <class Force>
-__device__ __forceinline__ int radau_step(RadauObj& s, const Force& F, double h, double& next_h,
+__device__ __forceinline__ int radau_step(RadauObj& s, Force& F, double h, double& next_h,
                                           RadauCounters& cnt) {
     double g[3][7];
 #pragma unroll
@@ -53,7 +53,7 @@ __device__ __forceinline__ int radau_step(RadauObj& s, const Force& F, double h,
                 xs[c] = s.x[c] + f * s.v[c] * h + c_tab.frac2[j] * h2 * (s.a[c] / 2.0 + bw);
                 vs[c] = s.v[c] + f * h * (s.a[c] + bu);
             }
-            const int rc = F.template eval<false>(s.t + f * h, xs, vs, ev);
+            const int rc = F.eval(false, s.t + f * h, xs, vs, ev);
             if (rc != ST_OK) return rc;
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
@@ -96,7 +96,7 @@ __device__ __forceinline__ int radau_step(RadauObj& s, const Force& F, double h,
             }
             s.t += h;
             cnt.exact++;
-            const int rc = F.template eval<true>(s.t, s.x, s.v, s.a);
+            const int rc = F.eval(true, s.t, s.x, s.v, s.a);
             if (rc != ST_OK) return rc;
             cnt.steps++;
             const double mb6 = fmax(fmax(fabs(s.b[0][6]), fabs(s.b[1][6])), fabs(s.b[2][6]));
@@ -110,14 +110,14 @@ __device__ __forceinline__ int radau_step(RadauObj& s, const Force& F, double h,
 
 // Integrate s from s.t to tf.  max_loops bounds the step loop (ST_TIMEOUT when hit).
 template <class Force>
-__device__ int radau_integrate(RadauObj& s, double tf, const Force& F, RadauCounters& cnt,
+__device__ int radau_integrate(RadauObj& s, double tf, Force& F, RadauCounters& cnt,
                                int max_loops) {
 #pragma unroll
     for (int c = 0; c < 3; ++c)
 #pragma unroll
         for (int k = 0; k < 7; ++k) s.b[c][k] = 0.0;
     cnt.exact++;
-    int rc = F.template eval<true>(s.t, s.x, s.v, s.a);
+    int rc = F.eval(true, s.t, s.x, s.v, s.a);
     if (rc != ST_OK) return rc;
     if (fabs(tf - s.t) < 1e-10) return ST_OK;
     double h = copysign(0.1, tf - s.t);

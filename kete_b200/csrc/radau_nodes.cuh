@@ -25,13 +25,6 @@ constexpr int NODE_G = 8;
 
 enum Phase : int { PH_EXACT_INIT = 0, PH_ITER = 1, PH_EXACT_STEP = 2, PH_DONE = 3 };
 
-// Force evaluation with a runtime exact flag (single call site in the round loop).
-__device__ __forceinline__ int spk_eval_rt(SpkForce& F, bool exact, double t, const double x[3],
-                                           const double v[3], double out[3]) {
-    if (exact) return F.template eval<true>(t, x, v, out);
-    return F.template eval<false>(t, x, v, out);
-}
-
 __device__ __forceinline__ void nodes_store(const NBodyArgs& a, int64_t i, int rc, const double x[3],
                                             const double v[3], const SpkForce& F, double t_impact,
                                             const RadauCounters& cnt) {
@@ -55,28 +48,44 @@ __device__ __forceinline__ void nodes_store(const NBodyArgs& a, int64_t i, int r
 }
 
 
-__global__ void __launch_bounds__(128) nbody_nodes_kernel(NBodyArgs a) {
+constexpr int NODES_BLOCK = 128;
+constexpr int NODE_ROW = 17;  // doubles per node row in shared memory (16 used + 1 pad)
+
+// MINB: minimum resident blocks per SM requested from the compiler (1 = no register cap);
+// the host picks the instantiation (occupancy against spills is measured, not guessed).
+template <int MINB>
+__global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_nodes_kernel(NBodyArgs a) {
+    // node table: per node j, w_pow[j][0..6], u_pow[j][0..6], spacing, frac2 (rows padded
+    // to 17 doubles so the 8 lanes of a group read 8 different banks)
+    __shared__ double s_node[8 * NODE_ROW];
+    // per group: b (21 doubles, read by every lane for its predictor) and the 8 lanes'
+    // evaluations (3 doubles each), exchanged after each corrector iteration
+    __shared__ double s_b[NODES_BLOCK / NODE_G][21];
+    __shared__ double s_e[NODES_BLOCK / NODE_G][NODE_G * 3];
+    for (int i = threadIdx.x; i < 8 * NODE_ROW; i += blockDim.x) {
+        const int j = i / NODE_ROW, k = i % NODE_ROW;
+        double val = 0.0;
+        if (k < 7) val = c_tab.w_pow[j][k];
+        else if (k < 14) val = c_tab.u_pow[j][k - 7];
+        else if (k == 14) val = c_tab.spacing[j];
+        else if (k == 15) val = c_tab.frac2[j];
+        s_node[i] = val;
+    }
+    __syncthreads();
+
     const int lane = threadIdx.x & (NODE_G - 1);
     const int warp_lane = threadIdx.x & 31;
     const unsigned gmask = 0xFFu << (warp_lane & ~(NODE_G - 1));
     const int64_t group = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / NODE_G;
-    const int64_t n_groups = ((int64_t)gridDim.x * blockDim.x) / NODE_G;
-
-    // node handled by this lane and its predictor coefficients
-    const int jn = lane < 7 ? lane + 1 : 7;
-    const double f = c_tab.spacing[jn];
-    const double frac2 = c_tab.frac2[jn];
-    double wp[7], up[7];
-#pragma unroll
-    for (int k = 0; k < 7; ++k) {
-        wp[k] = c_tab.w_pow[jn][k];
-        up[k] = c_tab.u_pow[jn][k];
-    }
+    double* sb = s_b[threadIdx.x / NODE_G];
+    double* se = s_e[threadIdx.x / NODE_G];
+    const int comp = lane % 3;  // component this lane forms g and b for (lanes 0-2 publish)
+    const double* nrow = s_node + (lane < 7 ? lane + 1 : 7) * NODE_ROW;
 
     int64_t obj = -1;
     int phase = PH_DONE;
-    RadauObj s;
-    double tf = 0.0, h = 0.0, next_h = 0.0;
+    double t = 0.0, tf = 0.0, h = 0.0, next_h = 0.0;
+    double x[3], v[3], acc[3];
     int iter = 0, failures = 0;
     RadauCounters cnt;
     SpkForce F;
@@ -95,14 +104,15 @@ __global__ void __launch_bounds__(128) nbody_nodes_kernel(NBodyArgs a) {
         if (k >= a.n) return false;
         obj = a.order ? a.order[k] : k;
         const int64_t n = a.n;
-        s.t = a.jd0[obj];
+        t = a.jd0[obj];
         tf = a.jd1[obj];
-        s.x[0] = a.pos[obj]; s.x[1] = a.pos[n + obj]; s.x[2] = a.pos[2 * n + obj];
-        s.v[0] = a.vel[obj]; s.v[1] = a.vel[n + obj]; s.v[2] = a.vel[2 * n + obj];
-#pragma unroll
-        for (int c = 0; c < 3; ++c)
-#pragma unroll
-            for (int k2 = 0; k2 < 7; ++k2) s.b[c][k2] = 0.0;
+        x[0] = a.pos[obj]; x[1] = a.pos[n + obj]; x[2] = a.pos[2 * n + obj];
+        v[0] = a.vel[obj]; v[1] = a.vel[n + obj]; v[2] = a.vel[2 * n + obj];
+        if (lane < 7) {
+            sb[lane] = 0.0;
+            sb[7 + lane] = 0.0;
+            sb[14 + lane] = 0.0;
+        }
         F.ng.base = a.nongrav ? a.nongrav + obj : nullptr;
         F.ng.stride = n;
         F.ng.kind = a.nongrav ? (int)a.nongrav[obj] : 0;
@@ -113,29 +123,29 @@ __global__ void __launch_bounds__(128) nbody_nodes_kernel(NBodyArgs a) {
         iter = 0;
         failures = 0;
         rc = ST_OK;
-        const bool finite = isfinite(s.x[0]) && isfinite(s.x[1]) && isfinite(s.x[2]) &&
-                            isfinite(s.v[0]) && isfinite(s.v[1]) && isfinite(s.v[2]) && isfinite(s.t);
+        const bool finite = isfinite(x[0]) && isfinite(x[1]) && isfinite(x[2]) &&
+                            isfinite(v[0]) && isfinite(v[1]) && isfinite(v[2]) && isfinite(t);
         if (!finite) rc = ST_VALUE_ERROR;
-        if (rc == ST_OK) rc = to_ssb_equatorial(s.t, a.frame, a.chain, s.x, s.v);
+        if (rc == ST_OK) rc = to_ssb_equatorial(t, a.frame, a.chain, x, v);
         phase = PH_EXACT_INIT;
+        __syncwarp(gmask);
         return true;
     };
 
     auto finish = [&](int code) {
-        if (code == ST_OK) code = from_ssb_equatorial(tf, a.frame, a.chain, s.x, s.v);
-        if (lane == 0) nodes_store(a, obj, code, s.x, s.v, F, s.t, cnt);
+        if (code == ST_OK) code = from_ssb_equatorial(tf, a.frame, a.chain, x, v);
+        if (lane == 0) nodes_store(a, obj, code, x, v, F, t, cnt);
         phase = PH_DONE;
     };
 
-    // step start: truncate to the final time and reset the iteration (radau.rs:187-190,226-229)
+    // step start: |h| >= MIN_STEP, then truncate to the final time (radau.rs:187-190,214-216)
     auto start_step = [&]() {
         if (fabs(h) < 0.005) h = copysign(0.005, h);
-        if (fabs(s.t - tf) <= fabs(h)) h = tf - s.t;
+        if (fabs(t - tf) <= fabs(h)) h = tf - t;
         iter = 0;
         phase = PH_ITER;
     };
 
-    if (group >= n_groups) return;
     if (!fetch()) return;
     if (rc != ST_OK) finish(rc);
 
@@ -159,30 +169,31 @@ __global__ void __launch_bounds__(128) nbody_nodes_kernel(NBodyArgs a) {
         const bool exact = phase != PH_ITER;
         double te, xe[3], ve[3];
         if (exact) {
-            te = s.t;
+            te = t;
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-                xe[c] = s.x[c];
-                ve[c] = s.v[c];
+                xe[c] = x[c];
+                ve[c] = v[c];
             }
         } else {
+            const double f = nrow[14], frac2 = nrow[15];
             const double h2 = h * h;
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
                 double bw = 0.0, bu = 0.0;
 #pragma unroll
                 for (int k = 0; k < 7; ++k) {
-                    bw += wp[k] * s.b[c][k];
-                    bu += up[k] * s.b[c][k];
+                    const double bck = sb[7 * c + k];
+                    bw += nrow[k] * bck;
+                    bu += nrow[7 + k] * bck;
                 }
-                xe[c] = s.x[c] + f * s.v[c] * h + frac2 * h2 * (s.a[c] / 2.0 + bw);
-                ve[c] = s.v[c] + f * h * (s.a[c] + bu);
+                xe[c] = x[c] + f * v[c] * h + frac2 * h2 * (acc[c] / 2.0 + bw);
+                ve[c] = v[c] + f * h * (acc[c] + bu);
             }
-            te = s.t + f * h;
+            te = t + f * h;
         }
         double ev[3];
-        int erc = spk_eval_rt(F, exact, te, xe, ve, ev);
-        __syncwarp(gmask);
+        int erc = F.eval(exact, te, xe, ve, ev);
         // any lane of the group failing fails the group (only DAF limits / impacts occur)
         const unsigned bad = __ballot_sync(gmask, erc != ST_OK);
         if (bad) {
@@ -193,20 +204,20 @@ __global__ void __launch_bounds__(128) nbody_nodes_kernel(NBodyArgs a) {
         }
         if (exact) {
             cnt.exact++;
-            s.a[0] = ev[0];
-            s.a[1] = ev[1];
-            s.a[2] = ev[2];
+            acc[0] = ev[0];
+            acc[1] = ev[1];
+            acc[2] = ev[2];
             if (phase == PH_EXACT_INIT) {
-                if (fabs(tf - s.t) < 1e-10) {
+                if (fabs(tf - t) < 1e-10) {
                     finish(ST_OK);
                     continue;
                 }
-                h = copysign(0.1, tf - s.t);
+                h = copysign(0.1, tf - t);
                 failures = 0;
             } else {
                 cnt.steps++;
                 h = next_h;
-                if (fabs(s.t - tf) < 1e-12) {
+                if (fabs(t - tf) < 1e-12) {
                     finish(ST_OK);
                     continue;
                 }
@@ -215,65 +226,65 @@ __global__ void __launch_bounds__(128) nbody_nodes_kernel(NBodyArgs a) {
             start_step();
             continue;
         }
-        // ---- corrector iteration: gather the 7 node evaluations ----
+        // ---- corrector iteration: exchange the 7 node evaluations, form g and b ----
+        // (radau.rs:292-313).  Lanes 0-2 each own one component; every lane then reads the
+        // new b for the convergence test and the state update.
         cnt.iterations++;
-        double g[3][7];
-        double e7[3];
+        se[3 * lane + 0] = ev[0];
+        se[3 * lane + 1] = ev[1];
+        se[3 * lane + 2] = ev[2];
+        const double b6_old0 = sb[6], b6_old1 = sb[13], b6_old2 = sb[20];
+        __syncwarp(gmask);
+        {
+            const double ac = comp == 0 ? acc[0] : (comp == 1 ? acc[1] : acc[2]);
+            double g[7];
 #pragma unroll
-        for (int j = 1; j < 8; ++j) {
-            double e[3];
+            for (int j = 1; j < 8; ++j) {
+                double gk = (se[3 * (j - 1) + comp] - ac) * c_tab.inv_frac[j];
 #pragma unroll
-            for (int c = 0; c < 3; ++c) e[c] = __shfl_sync(gmask, ev[c], j - 1, NODE_G);
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                double gk = (e[c] - s.a[c]) * c_tab.inv_frac[j];
-#pragma unroll
-                for (int z = 1; z < j; ++z) gk = (gk - g[c][z - 1]) * c_tab.inv_diff[j][z];
-                g[c][j - 1] = gk;
+                for (int z = 1; z < j; ++z) gk = (gk - g[z - 1]) * c_tab.inv_diff[j][z];
+                g[j - 1] = gk;
             }
-            if (j == 7) {
-                e7[0] = e[0];
-                e7[1] = e[1];
-                e7[2] = e[2];
+            if (lane < 3) {
+#pragma unroll
+                for (int jj = 0; jj < 7; ++jj) {
+                    double s2 = g[jj];
+#pragma unroll
+                    for (int k = jj + 1; k < 7; ++k) s2 += c_tab.c[k][jj] * g[k];
+                    sb[7 * comp + jj] = s2;
+                }
             }
         }
-        const double b6_old[3] = {s.b[0][6], s.b[1][6], s.b[2][6]};
-#pragma unroll
-        for (int c = 0; c < 3; ++c)
-#pragma unroll
-            for (int jj = 0; jj < 7; ++jj) {
-                double acc = g[c][jj];
-#pragma unroll
-                for (int k = jj + 1; k < 7; ++k) acc += c_tab.c[k][jj] * g[c][k];
-                s.b[c][jj] = acc;
-            }
-        double fem[3], ratio[3];
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            fem[c] = fabs(e7[c]) + 1e-6;
-            ratio[c] = fabs(s.b[c][6] - b6_old[c]) / fem[c];
-        }
+        __syncwarp(gmask);
+        const double e70 = se[18], e71 = se[19], e72 = se[20];  // node 7 = lane 6
+        const double fem0 = fabs(e70) + 1e-6, fem1 = fabs(e71) + 1e-6, fem2 = fabs(e72) + 1e-6;
+        const double b60 = sb[6], b61 = sb[13], b62 = sb[20];
+        const double ratio = fmax(fmax(fabs(b60 - b6_old0) / fem0, fabs(b61 - b6_old1) / fem1),
+                                  fabs(b62 - b6_old2) / fem2);
         ++iter;
-        if (fmax(fmax(ratio[0], ratio[1]), ratio[2]) < 1e-14) {
+        if (ratio < 1e-14) {
             const double h2 = h * h;
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
                 double dw = 0.0, du = 0.0;
 #pragma unroll
                 for (int k = 0; k < 7; ++k) {
-                    dw += s.b[c][k] * c_tab.w[k];
-                    du += s.b[c][k] * c_tab.u[k];
+                    const double bck = sb[7 * c + k];
+                    dw += bck * c_tab.w[k];
+                    du += bck * c_tab.u[k];
                 }
-                s.x[c] += s.v[c] * h + h2 * (s.a[c] * 0.5 + dw);
-                s.v[c] += h * (s.a[c] + du);
+                x[c] += v[c] * h + h2 * (acc[c] * 0.5 + dw);
+                v[c] += h * (acc[c] + du);
             }
-            s.t += h;
-            const double mb6 = fmax(fmax(fabs(s.b[0][6]), fabs(s.b[1][6])), fabs(s.b[2][6]));
-            const double r = pow(1e-6 * fmax(fmax(fem[0], fem[1]), fem[2]) / mb6, 1.0 / 7.0);
+            t += h;
+            const double mb6 = fmax(fmax(fabs(b60), fabs(b61)), fabs(b62));
+            const double r = pow(1e-6 * fmax(fmax(fem0, fem1), fem2) / mb6, 1.0 / 7.0);
             next_h = h * clampd(r, 0.25, 4.0);
             phase = PH_EXACT_STEP;
+            __syncwarp(gmask);  // b and evaluations consumed before the next round rewrites them
             continue;
         }
+        __syncwarp(gmask);
         if (iter >= 10) {  // step failed to converge (radau.rs:345) -> retry smaller
             failures += 1;
             h *= 0.7;

@@ -1,0 +1,75 @@
+"""Launch-configuration autotuner for the N-body kernels.
+
+The node-parallel Radau kernel comes in three register budgets (no cap, 168 registers for
+3 blocks/SM, 128 registers for 4 blocks/SM: more resident lane groups against spills to
+local memory) and in two grid forms (one lane group per object, or a persistent grid
+whose groups take the next object from a queue).  Which is fastest depends on the object
+count and the spread of their step counts, so it is measured: ``autotune`` times every
+configuration on the caller's own inputs (device arrays) and installs the fastest.
+"""
+from __future__ import annotations
+
+import ctypes
+import itertools
+import json
+import os
+
+from . import _lib
+from .propagation import propagate_n_body_arrays
+
+CONFIGS = [dict(mode=_lib.MODE_NODES, variant=v, refill=r) for v, r in
+           itertools.product((0, 1, 2), (0, 1))] + [dict(mode=_lib.MODE_THREAD, variant=0,
+                                                         refill=0)]
+_current = dict(mode=_lib.MODE_NODES, variant=0, refill=0, thread_block=128)
+
+
+def set_config(mode=_lib.MODE_NODES, variant=0, refill=0, thread_block=128):
+    L = _lib.lib()
+    L.kete_b200_set_launch_config.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    _lib.check(L.kete_b200_set_launch_config(int(variant), int(refill), int(thread_block)))
+    _current.update(mode=mode, variant=variant, refill=refill, thread_block=thread_block)
+
+
+def current():
+    return dict(_current)
+
+
+def autotune(pos, vel, jd0, jd1, nongrav=None, reps=2, cache_path=None, key=None):
+    """Time each configuration on these (torch CUDA) inputs; install and return the best.
+
+    Returns (best_config, {label: ms})."""
+    import torch
+
+    if cache_path and key and os.path.exists(cache_path):
+        with open(cache_path) as f:
+            cached = json.load(f).get(key)
+        if cached:
+            set_config(**cached["best"])
+            return cached["best"], cached["times"]
+    times = {}
+    best, best_ms = None, float("inf")
+    for cfg in CONFIGS:
+        set_config(**cfg)
+        propagate_n_body_arrays(pos, vel, jd0, jd1, nongrav=nongrav, mode=cfg["mode"])  # warm
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            propagate_n_body_arrays(pos, vel, jd0, jd1, nongrav=nongrav, mode=cfg["mode"])
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        label = f"mode{cfg['mode']}_v{cfg['variant']}_r{cfg['refill']}"
+        times[label] = ms
+        if ms < best_ms:
+            best, best_ms = dict(cfg), ms
+    set_config(**best)
+    if cache_path and key:
+        data = {}
+        if os.path.exists(cache_path):
+            with open(cache_path) as f:
+                data = json.load(f)
+        data[key] = {"best": best, "times": times}
+        with open(cache_path, "w") as f:
+            json.dump(data, f, indent=1)
+    return best, times

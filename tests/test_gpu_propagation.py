@@ -110,24 +110,36 @@ def test_spk_states_vs_oracle(gpu, oracle_spk):
                 assert np.abs(out6[3:, k] - ref[3:]).max() < 1e-15
 
 
-MODES = (1, 2)  # one object per thread; eight node lanes per object
+# launch configurations: one object per thread; eight node lanes per object without a
+# register cap; with a 128-register cap on a persistent grid that refills from a queue
+CONFIGS = (dict(mode=1, variant=0, refill=0), dict(mode=2, variant=0, refill=0),
+           dict(mode=2, variant=2, refill=1))
+MODES = CONFIGS
+
+
+def _set(gpu, cfg):
+    from kete_b200 import tune
+
+    tune.set_config(**cfg)
+    return cfg["mode"]
 
 
 def _compare_nbody(gpu, oracle, pos, vel, jd0, jd1, ng=None, frame=2, center=10, tol=1e-9):
     op, ov, ost, ons, one = oracle.propagate_n_body(pos, vel, jd0, jd1, frame, center, ng=ng)
-    for mode in MODES:
+    for cfg in CONFIGS:
+        mode = _set(gpu, cfg)
         p, v, st, det = gpu.propagate_n_body_arrays(pos, vel, jd0, jd1, frame, center,
                                                     nongrav=ng, mode=mode, with_details=True)
-        assert (st == ost).all(), (mode, np.bincount(st), np.bincount(ost))
+        assert (st == ost).all(), (cfg, np.bincount(st), np.bincount(ost))
         ok = st == 0
         close = det["min_dist"] < 0.01
         far = ok & ~close
         err = np.linalg.norm(p - op, axis=0)
         if far.any():
-            assert err[far].max() < tol, (mode, err[far].max())
+            assert err[far].max() < tol, (cfg, err[far].max())
         # step counts agree (same adaptive sequence) for nearly all objects
         if ok.any():
-            assert np.mean(det["counters"][0][ok] == ons[ok]) > 0.95, mode
+            assert np.mean(det["counters"][0][ok] == ons[ok]) > 0.95, cfg
     return err, det, close
 
 
@@ -173,7 +185,8 @@ def test_nbody_edge_cases(gpu, oracle_spk):
     jd0 = np.full(4, EPOCH)
     jd1 = np.array([EPOCH + 10, EPOCH, EPOCH + 5000.0, EPOCH + 10])
     op, ov, ost, _, _ = oracle_spk.propagate_n_body(pos, vel, jd0, jd1)
-    for mode in MODES:
+    for cfg in CONFIGS:
+        mode = _set(gpu, cfg)
         p, v, st, det = gpu.propagate_n_body_arrays(pos, vel, jd0, jd1, mode=mode,
                                                     with_details=True)
         assert st.tolist() == ost.tolist() == [2, 0, 3, 6]
@@ -224,3 +237,19 @@ def test_device_arrays_torch(gpu, oracle_spk):
     torch.cuda.synchronize()
     hp, hv, hst = gpu.propagate_n_body_arrays(pos, vel, jd0, jd1)
     assert np.array_equal(p.cpu().numpy(), hp)
+
+
+def test_autotune_installs_a_working_config(gpu, oracle_spk):
+    torch = pytest.importorskip("torch")
+    from kete_b200 import tune
+
+    n = 512
+    pos, vel = synthetic.main_belt(n, seed=81)
+    jd0, jd1 = np.full(n, EPOCH), np.full(n, EPOCH + 20.0)
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    best, times = tune.autotune(dev(pos), dev(vel), dev(jd0), dev(jd1), reps=1)
+    assert len(times) == len(tune.CONFIGS) and best in tune.CONFIGS
+    p, v, st = gpu.propagate_n_body_arrays(pos, vel, jd0, jd1, mode=best["mode"])
+    op, _, ost, _, _ = oracle_spk.propagate_n_body(pos, vel, jd0, jd1)
+    assert (st == 0).all() and np.abs(p - op).max() < 1e-9
+    tune.set_config()
