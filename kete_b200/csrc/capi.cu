@@ -83,6 +83,7 @@ struct DevState {
 };
 
 static std::mutex g_mu;
+static bool g_device_ready = false;  // kete_b200_init has run: loads upload eagerly
 static LaunchConfig g_launch;
 LaunchConfig& launch_config() { return g_launch; }
 static std::vector<HostSeg> g_segs;
@@ -451,7 +452,9 @@ int kete_b200_init(int device) {
     int rc = cuda_check(cudaSetDevice(device), "cudaSetDevice");
     if (rc) return rc;
     DevState* ds;
-    return ensure_device(ds);
+    if ((rc = ensure_device(ds))) return rc;
+    g_device_ready = true;
+    return 0;
 }
 
 int kete_b200_spk_load_buffer(const uint8_t* bytes, int64_t n_bytes) {
@@ -463,7 +466,12 @@ int kete_b200_spk_load_buffer(const uint8_t* bytes, int64_t n_bytes) {
     if (rc) return rc;
     for (auto& s : segs) g_segs.push_back(std::move(s));
     g_skipped += skipped;
-    return rebuild_tables();
+    if ((rc = rebuild_tables())) return rc;
+    if (g_device_ready) {  // make the new ephemeris resident on the current device now
+        DevState* ds;
+        if ((rc = ensure_device(ds))) return rc;
+    }
+    return 0;
 }
 
 int kete_b200_spk_load_file(const char* path) {
@@ -602,11 +610,14 @@ int kete_b200_propagate_n_body(int64_t n, const double* pos, const double* vel, 
     } else if (mode == KETE_B200_MODE_NODES || mode == KETE_B200_MODE_AUTO) {
         int grid = 0;
         if (g_launch.nodes_refill) {
-            // persistent grid; the object queue counter is a 4-byte scratch word
+            // persistent grid taking objects longest span first; scratch holds the queue
+            // counter, the span histogram and the processing order
             void* q = nullptr;
-            if ((rc = staging(*ds, 31, sizeof(int), &q))) return rc;
-            if ((rc = cuda_check(cudaMemsetAsync(q, 0, sizeof(int), st), "reset object queue"))) return rc;
+            if ((rc = staging(*ds, 31, (ORDER_SCRATCH_HEADER + (size_t)n) * sizeof(int), &q)))
+                return rc;
+            if ((rc = launch_span_order(n, a.jd0, a.jd1, (int*)q, st))) return rc;
             a.queue = (int*)q;
+            a.order = (const int32_t*)((int*)q + ORDER_SCRATCH_HEADER);
             if ((rc = nodes_grid_size(g_launch.nodes_variant, &grid))) return rc;
             const int64_t need = (n * 8 + 127) / 128;
             if (grid > need) grid = (int)need;

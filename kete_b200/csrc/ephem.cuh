@@ -20,6 +20,9 @@ constexpr int MAX_SEG = 96;
 constexpr int MAX_SLOT = 32;
 constexpr int MAX_FORCE = 16;
 constexpr int MAX_CHAIN = 3;
+// span ordering of the persistent N-body grid: buckets and scratch header size (ints)
+constexpr int ORDER_BUCKETS = 64;
+constexpr int ORDER_SCRATCH_HEADER = 256;
 
 struct SegDesc {
     double jd_start, jd_end;  // JD, as spice_jds_to_jd(summary) (spice/mod.rs:25-28)

@@ -293,3 +293,75 @@ int nodes_grid_size(int variant, int* grid) {
 }
 
 }  // namespace kb
+
+namespace kb {
+
+// -------------------------------------------------------------------------------------------
+// Processing order for the persistent (refill) grid: objects with the longest integration
+// spans first, so the groups that finish early pick up the short ones and the tail is short.
+// Spans are bucketed on a log2 scale (quarter-octave buckets); within a bucket the order is
+// whatever the atomics give -- it does not affect any object's result.
+//
+// Scratch layout (ints): [0] object queue, [1..64] bucket histogram, [65..128] bucket
+// cursors, then order[n] from int offset ORDER_SCRATCH_HEADER.
+// -------------------------------------------------------------------------------------------
+__device__ __forceinline__ int span_bucket(double jd0, double jd1) {
+    const double span = fabs(jd1 - jd0);
+    if (!(span > 1.0)) return ORDER_BUCKETS - 1;  // short, zero or NaN spans go last
+    const int b = (int)(log2(span) * 4.0);
+    const int k = ORDER_BUCKETS - 1 - (b < 0 ? 0 : (b > ORDER_BUCKETS - 1 ? ORDER_BUCKETS - 1 : b));
+    return k;  // bucket 0 = longest spans
+}
+
+__global__ void order_hist_kernel(int64_t n, const double* __restrict__ jd0,
+                                  const double* __restrict__ jd1, int* __restrict__ scratch) {
+    __shared__ int h[ORDER_BUCKETS];
+    for (int i = threadIdx.x; i < ORDER_BUCKETS; i += blockDim.x) h[i] = 0;
+    __syncthreads();
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        atomicAdd(&h[span_bucket(jd0[i], jd1[i])], 1);
+    __syncthreads();
+    for (int i = threadIdx.x; i < ORDER_BUCKETS; i += blockDim.x)
+        if (h[i]) atomicAdd(&scratch[1 + i], h[i]);
+}
+
+__global__ void order_scan_kernel(int* __restrict__ scratch) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        int run = 0;
+        for (int b = 0; b < ORDER_BUCKETS; ++b) {
+            scratch[1 + ORDER_BUCKETS + b] = run;
+            run += scratch[1 + b];
+        }
+    }
+}
+
+__global__ void order_scatter_kernel(int64_t n, const double* __restrict__ jd0,
+                                     const double* __restrict__ jd1, int* __restrict__ scratch,
+                                     int32_t* __restrict__ order) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int b = span_bucket(jd0[i], jd1[i]);
+        const int pos = atomicAdd(&scratch[1 + ORDER_BUCKETS + b], 1);
+        if (pos >= 0 && pos < n) order[pos] = (int32_t)i;
+    }
+}
+
+// Zero the header, histogram the spans, scan, scatter.  scratch must hold
+// ORDER_SCRATCH_HEADER + n ints; order = scratch + ORDER_SCRATCH_HEADER.
+int launch_span_order(int64_t n, const double* jd0, const double* jd1, int* scratch,
+                      cudaStream_t stream) {
+    int rc = cuda_check(cudaMemsetAsync(scratch, 0, ORDER_SCRATCH_HEADER * sizeof(int), stream),
+                        "clear order header");
+    if (rc || n <= 0) return rc;
+    const int block = 256;
+    int64_t g = (n + block - 1) / block;
+    const int grid = (int)(g > 1184 ? 1184 : g);
+    order_hist_kernel<<<grid, block, 0, stream>>>(n, jd0, jd1, scratch);
+    order_scan_kernel<<<1, 32, 0, stream>>>(scratch);
+    order_scatter_kernel<<<grid, block, 0, stream>>>(n, jd0, jd1, scratch,
+                                                     (int32_t*)(scratch + ORDER_SCRATCH_HEADER));
+    return cuda_check(cudaGetLastError(), "span order launch");
+}
+
+}  // namespace kb
