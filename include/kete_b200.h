@@ -116,6 +116,28 @@ int kete_b200_radau_central(int64_t n, const double* pos, const double* vel, con
                             const double* t1, double* out_pos, double* out_vel,
                             int32_t* status, int on_device, void* stream);
 
+/* --- allocation-free variant (no counterpart in the reference) ---------------------------
+ * kete_b200_propagate_n_body on the persistent lane-group grid, for callers that must not
+ * have device memory allocated or freed during the call: cudaMalloc/cudaFree synchronize
+ * the whole device, so steady-state loops, latency-bound services and processes whose
+ * device memory belongs to another allocator cannot afford them between launches.  The
+ * per-call scratch (object queue, span histogram, processing order) lives in a fixed
+ * device array built into the library (KETE_B200_NOALLOC_MAX_OBJECTS * 4 + 1024 bytes,
+ * held on every device that loads the library until exit); n above
+ * KETE_B200_NOALLOC_MAX_OBJECTS is rejected with KETE_B200_E_ARGUMENT.
+ * All array arguments are device pointers on the current device; the call only enqueues
+ * work on `stream`.  The loaded SPK must already be resident on the device (load it after
+ * kete_b200_init, or make one regular call first).  The first call on each device looks up
+ * the array's device address (make it before any stream capture).  Calls that overlap on
+ * the GPU share the array and race: serialize them. */
+#define KETE_B200_NOALLOC_MAX_OBJECTS 1048576
+int kete_b200_propagate_n_body_noalloc(int64_t n, const double* pos, const double* vel,
+                                       const double* jd0, const double* jd1, int frame,
+                                       int64_t center, int include_asteroids,
+                                       const double* nongrav, double* out_pos, double* out_vel,
+                                       int32_t* status, int32_t* impact_id, double* impact_jd,
+                                       double* min_dist, int32_t* counters, void* stream);
+
 /* --- diagnostics (no counterpart in the reference) ------------------------------------
  * FP64 pipe throughput of the current device, measured with independent DFMA chains
  * (the FP64 roofline denominator).  Synchronous; ms may be NULL. */

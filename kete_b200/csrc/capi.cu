@@ -437,6 +437,28 @@ struct Stager {
     }
 };
 
+// Everything the allocation-free entry point needs, read under the lock without allocating:
+// the ephemeris must already be resident on the current device.
+int noalloc_snapshot(int include_asteroids, int64_t center, NBodyArgs& a, LaunchConfig& cfg) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!g_eph.loaded) return set_error(KETE_B200_E_NO_EPHEMERIS, "no SPK loaded");
+    int dev = 0;
+    int rc = current_device(dev);
+    if (rc) return rc;
+    auto it = g_dev.find(dev);
+    if (it == g_dev.end() || !it->second.tables || it->second.version != g_version)
+        return set_error(KETE_B200_E_NO_EPHEMERIS,
+                         "the loaded SPK is not resident on this device yet: call kete_b200_init "
+                         "on it before loading, or make one allocating call first");
+    const int n_force = include_asteroids ? g_eph.n_force_all : g_eph.n_force_planets;
+    if (n_force == 0)
+        return set_error(KETE_B200_E_NO_EPHEMERIS, "loaded SPKs lack a perturbing body");
+    if ((rc = center_chain(center, a.chain))) return rc;
+    a.n_force = n_force;
+    cfg = g_launch;
+    return 0;
+}
+
 }  // namespace kb
 
 using namespace kb;

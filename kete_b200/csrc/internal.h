@@ -59,6 +59,7 @@ struct LaunchConfig {
     int thread_block = 128;
 };
 LaunchConfig& launch_config();
+int noalloc_snapshot(int include_asteroids, int64_t center, NBodyArgs& a, LaunchConfig& cfg);
 int launch_radau_central(int64_t n, const double* pos, const double* vel, const double* t0,
                          const double* t1, double* out_pos, double* out_vel, int32_t* status,
                          cudaStream_t stream);
