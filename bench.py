@@ -48,13 +48,32 @@ def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
 
-def workload(n, seed=21):
+WORKLOADS = {
+    "nbody_mba_10k": "plain N-body Radau, {n} main-belt states x 365.25 d per GPU, Sun+8 planets"
+                     "+Moon from a synthetic SPK type-2 file (14-coef records)",
+    "nbody_mixed_1m": "batched uneven N-body, {n} states (90% main belt, 10% NEO, 5% JPL comet "
+                      "non-grav A1~N(0,1e-8) A2~N(0,1e-9)), per-object target epochs U(+-5 yr)",
+    "kepler_100k": "two-body Kepler, {n} main-belt states, per-object target epochs U(+-1000 d)",
+}
+DEFAULT_N = {"nbody_mba_10k": 10_000, "nbody_mixed_1m": 1_000_000, "kepler_100k": 100_000}
+
+
+def workload(n, seed=21, kind="nbody_mba_10k"):
+    """Seeded inputs: pos (3,n), vel (3,n), jd0 (n,), jd1 (n,), nongrav (10,n) or None."""
     from kete_b200 import synthetic
 
+    if kind == "nbody_mixed_1m":
+        pos, vel, ng = synthetic.mixed(n, seed=seed)
+        rng = np.random.default_rng(seed + 100)
+        jd0 = np.full(n, EPOCH)
+        jd1 = EPOCH + rng.uniform(-5 * 365.25, 5 * 365.25, n)
+        return pos, vel, jd0, jd1, ng
     pos, vel = synthetic.main_belt(n, seed=seed)
     jd0 = np.full(n, EPOCH)
-    jd1 = np.full(n, EPOCH + SPAN)
-    return pos, vel, jd0, jd1
+    if kind == "kepler_100k":
+        rng = np.random.default_rng(seed + 100)
+        return pos, vel, jd0, EPOCH + rng.uniform(-1000.0, 1000.0, n), None
+    return pos, vel, jd0, np.full(n, EPOCH + SPAN), None
 
 
 class ClockSampler:
@@ -155,17 +174,34 @@ def barrier(world):
         dist.barrier()
 
 
-def cpu_baseline(pos, vel, jd0, jd1, spk_bytes, threads=0):
+def cpu_sample(kind, n):
+    """Indices of the bounded CPU sample for a workload (the full set when it is small)."""
+    if kind == "nbody_mixed_1m":
+        return np.arange(0, n, 100)  # seeded 1% subsample, extrapolated per object-year
+    return np.arange(n)
+
+
+def cpu_baseline(kind, pos, vel, jd0, jd1, ng, spk_bytes, threads=0):
     """Time the oracle (CPU restatement of kete's path) on all host cores."""
     from oracle import oracle as O
 
+    cores = threads or os.cpu_count()
+    if kind == "kepler_100k":
+        t = time.perf_counter()
+        op, ov, ojd, st = O.propagate_two_body(pos, vel, jd0, jd1, threads=cores)
+        return op, st, time.perf_counter() - t, cores
     O.spk_reset()
     O.spk_load_bytes(spk_bytes)
-    cores = threads or os.cpu_count()
     t = time.perf_counter()
-    op, ov, st, ns, ne = O.propagate_n_body(pos, vel, jd0, jd1, threads=cores)
-    dt = time.perf_counter() - t
-    return op, st, dt, cores
+    op, ov, st, ns, ne = O.propagate_n_body(pos, vel, jd0, jd1, ng=ng, threads=cores)
+    return op, st, time.perf_counter() - t, cores
+
+
+def units_of(kind, jd0, jd1):
+    """Work units of a workload: object-years (N-body) or objects (two-body)."""
+    if kind == "kepler_100k":
+        return float(len(jd0)), "objects/s", "two-body objects/s (propagate_two_body)"
+    return float(np.sum(np.abs(jd1 - jd0)) / 365.25), UNIT, METRIC
 
 
 def run_reference(args, world, rank):
@@ -173,31 +209,40 @@ def run_reference(args, world, rank):
         return
     from kete_b200 import synthetic
 
-    pos, vel, jd0, jd1 = workload(args.n)
+    kind = args.workload
+    n = args.n or DEFAULT_N[kind]
+    pos, vel, jd0, jd1, ng = workload(n, kind=kind)
+    idx = cpu_sample(kind, n)
+    sp, sv, s0, s1 = pos[:, idx], vel[:, idx], jd0[idx], jd1[idx]
+    sng = None if ng is None else ng[:, idx]
+    units, unit, metric = units_of(kind, s0, s1)
     with tempfile.TemporaryDirectory() as td:
         spk = synthetic.write_synthetic_spk(os.path.join(td, "syn.bsp"))
         spk_bytes = open(spk, "rb").read()
     for _ in range(args.warmup):
-        cpu_baseline(pos[:, :200], vel[:, :200], jd0[:200], jd1[:200], spk_bytes)
+        w = slice(0, min(200, len(idx)))
+        cpu_baseline(kind, sp[:, w], sv[:, w], s0[w], s1[w], None if sng is None else sng[:, w],
+                     spk_bytes)
     times = []
     cores = os.cpu_count()
     for _ in range(args.steps):
-        _, st, dt, cores = cpu_baseline(pos, vel, jd0, jd1, spk_bytes)
+        _, st, dt, cores = cpu_baseline(kind, sp, sv, s0, s1, sng, spk_bytes)
         times.append(dt)
     total = float(np.sum(times))
-    value = args.n * SPAN / 365.25 * args.steps / total
+    value = units * args.steps / total
+    sample = ("full workload per step" if len(idx) == n else
+              f"seeded 1% subsample ({len(idx)} of {n} objects) per step, rate per object-year")
     line = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "impl": "reference", "metric": metric, "value": value, "unit": unit, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": f"plain N-body Radau, {args.n} main-belt states x {SPAN} d, "
-                   "Sun+8 planets+Moon from a synthetic SPK type-2 file", "n_objects": args.n},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"full workload ({args.n} objects) per step; the reference "
-                                   "Rust/rayon path cannot be built (no Rust toolchain), so the "
-                                   "C restatement of kete's FP64 code runs under OpenMP"},
-        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "config": {"workload": WORKLOADS[kind].format(n=n), "n_objects": n},
+        "cpu_baseline": {"value": value, "unit": unit, "cores": cores, "kind": "port",
+                         "sample": sample + "; the reference Rust/rayon path cannot be built "
+                                   "(no Rust toolchain), so the C restatement of kete's FP64 code "
+                                   "runs under OpenMP on all host cores"},
+        "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
@@ -206,7 +251,7 @@ def run_gpu(args, world, rank, local):
     import torch
 
     import kete_b200
-    from kete_b200 import _lib, build, synthetic
+    from kete_b200 import _lib, build, synthetic, tune
 
     build.build()
     torch.cuda.set_device(local)
@@ -216,35 +261,49 @@ def run_gpu(args, world, rank, local):
     spk_bytes = open(spk, "rb").read()
     kete_b200.spice.kernel_reload([spk])
 
-    n = args.n
-    pos, vel, jd0, jd1 = workload(n, seed=21 + rank)
+    kind = args.workload
+    n = args.n or DEFAULT_N[kind]
+    nbody = kind != "kepler_100k"
+    pos, vel, jd0, jd1, ng = workload(n, seed=21 + rank, kind=kind)
+    units, unit, metric = units_of(kind, jd0, jd1)
     dev = torch.device("cuda", local)
-    d = {k: torch.from_numpy(np.ascontiguousarray(v)).to(dev)
-         for k, v in dict(pos=pos, vel=vel, jd0=jd0, jd1=jd1).items()}
-    from kete_b200 import tune
+    host = dict(pos=pos, vel=vel, jd0=jd0, jd1=jd1)
+    if ng is not None:
+        host["ng"] = ng
+    d = {k: torch.from_numpy(np.ascontiguousarray(v)).to(dev) for k, v in host.items()}
 
     sweep = None
-    if args.mode == 0:
-        best, sweep = tune.autotune(d["pos"], d["vel"], d["jd0"], d["jd1"])
-    else:
-        best = dict(mode=args.mode, variant=args.variant, refill=args.refill)
-        tune.set_config(**best)
-    mode = best["mode"]
+    best = None
+    if nbody:
+        if args.mode == 0:
+            best, sweep = tune.autotune(d["pos"], d["vel"], d["jd0"], d["jd1"], nongrav=d.get("ng"))
+        else:
+            best = dict(mode=args.mode, variant=args.variant, refill=args.refill)
+            tune.set_config(**best)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
 
-    def step():
-        return kete_b200.propagate_n_body_arrays(d["pos"], d["vel"], d["jd0"], d["jd1"],
-                                                 mode=mode)
+    def step(arrs):
+        if nbody:
+            return kete_b200.propagate_n_body_arrays(arrs["pos"], arrs["vel"], arrs["jd0"],
+                                                     arrs["jd1"], nongrav=arrs.get("ng"),
+                                                     mode=best["mode"])
+        return kete_b200.propagate_two_body_arrays(arrs["pos"], arrs["vel"], arrs["jd0"],
+                                                   arrs["jd1"])
 
-    # counts for the flop model (deterministic: same inputs every step)
-    _, _, st_d, det = kete_b200.propagate_n_body_arrays(d["pos"], d["vel"], d["jd0"], d["jd1"],
-                                                        mode=mode, with_details=True)
-    cnt = det["counters"].to(torch.int64).sum(dim=1).cpu().numpy()
-    steps_total, iters_total, exact_total = (int(x) for x in cnt)
-    flops = iters_total * FLOPS_PER_ITER + exact_total * FLOPS_PER_EVAL + steps_total * FLOPS_PER_STEP
+    flops = None
+    steps_total = iters_total = 0
+    if nbody:  # counts for the flop model (deterministic: same inputs every step)
+        _, _, _, det = kete_b200.propagate_n_body_arrays(d["pos"], d["vel"], d["jd0"], d["jd1"],
+                                                         nongrav=d.get("ng"), mode=best["mode"],
+                                                         with_details=True)
+        cnt = det["counters"].to(torch.int64).sum(dim=1).cpu().numpy()
+        steps_total, iters_total, exact_total = (int(x) for x in cnt)
+        flops = (iters_total * FLOPS_PER_ITER + exact_total * FLOPS_PER_EVAL +
+                 steps_total * FLOPS_PER_STEP)
+    launches_per_step = (3 if (nbody and best.get("refill")) else 0) + 1
 
     for _ in range(args.warmup):
-        step()
+        step(d)
     torch.cuda.synchronize()
     stream = torch.cuda.current_stream(dev)
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
@@ -255,76 +314,87 @@ def run_gpu(args, world, rank, local):
         for k in range(args.steps):
             flush.zero_()  # write > L2 (126 MB) between steps, outside the timed pair
             evs[k][0].record(stream)
-            out = step()
+            step(d)
             evs[k][1].record(stream)
         torch.cuda.synchronize()
         barrier(world)
     ms = [a.elapsed_time(b) for a, b in evs]
     t_total = reduce_max(float(np.sum(ms)) * 1e-3, world)
     ms_step = 1e3 * t_total / args.steps
-    obj_years = n * SPAN / 365.25
-    value = world * obj_years * args.steps / t_total
+    value = world * units * args.steps / t_total
 
     # end to end through the C ABI with pinned host buffers
-    hp = {k: torch.from_numpy(np.ascontiguousarray(v)).pin_memory()
-          for k, v in dict(pos=pos, vel=vel, jd0=jd0, jd1=jd1).items()}
+    hp = {k: torch.from_numpy(np.ascontiguousarray(v)).pin_memory() for k, v in host.items()}
     hnp = {k: v.numpy() for k, v in hp.items()}
-    kete_b200.propagate_n_body_arrays(hnp["pos"], hnp["vel"], hnp["jd0"], hnp["jd1"], mode=mode)
+    step(hnp)
     e2e_t = []
+    out = None
     for _ in range(args.steps):
         t = time.perf_counter()
-        op_h, ov_h, st_h = kete_b200.propagate_n_body_arrays(hnp["pos"], hnp["vel"], hnp["jd0"],
-                                                             hnp["jd1"], mode=mode)
+        out = step(hnp)
         e2e_t.append(time.perf_counter() - t)
     e2e_total = reduce_max(float(np.sum(e2e_t)), world)
-    e2e_value = world * obj_years * args.steps / e2e_total
-    h2d = 8 * n * 8
-    d2h = 6 * n * 8 + 4 * n
+    e2e_value = world * units * args.steps / e2e_total
+    h2d = sum(int(v.nbytes) for v in hnp.values())
+    d2h = 6 * n * 8 + 4 * n + (0 if nbody else 8 * n)
 
     if rank != 0:
         return
-    peaks = measured_peaks()
     tflops_probe = ctypes_probe(_lib)
-    achieved = flops / (ms_step * 1e-3) / 1e12
-    roof = {"bound": "fp64", "achieved": achieved, "peak": tflops_probe, "unit": "TFLOP/s",
-            "frac": achieved / tflops_probe if tflops_probe else None, "traffic": None,
-            "peak_source": "measured DFMA probe (kete_b200_fp64_probe) in this run",
-            "flops_per_launch": flops,
-            "hbm_bytes_algorithmic": int(n * (8 * 8 + 6 * 8 + 4))}
+    peaks = measured_peaks()
+    hbm_bytes = int(h2d + d2h)
+    if nbody:
+        achieved = flops / (ms_step * 1e-3) / 1e12
+        roof = {"bound": "fp64", "achieved": achieved, "peak": tflops_probe, "unit": "TFLOP/s",
+                "frac": achieved / tflops_probe if tflops_probe else None, "traffic": None,
+                "peak_source": "measured DFMA probe (kete_b200_fp64_probe) in this run",
+                "flops_per_launch": flops, "hbm_bytes_algorithmic": hbm_bytes}
+    else:
+        gbs = hbm_bytes / (ms_step * 1e-3) / 1e9
+        roof = {"bound": "hbm", "achieved": gbs, "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
+                "frac": gbs / peaks["hbm_gbs"] if peaks.get("hbm_gbs") else None,
+                "traffic": None, "peak_source": "MEASURED_PEAKS.json hbm_gbs",
+                "note": "the two-body solve is transcendental-bound; HBM is the nominal bound"}
 
-    # CPU baseline (oracle on all host cores) on the full workload, and a parity check
-    op, st_cpu, cpu_dt, cores = cpu_baseline(pos, vel, jd0, jd1, spk_bytes)
-    err = np.linalg.norm(op_h - op, axis=0)
-    ok = (st_h == 0) & (st_cpu == 0)
+    # CPU baseline (oracle on all host cores) on the bounded sample, and a parity check
+    idx = cpu_sample(kind, n)
+    op, st_cpu, cpu_dt, cores = cpu_baseline(kind, pos[:, idx], vel[:, idx], jd0[idx], jd1[idx],
+                                             None if ng is None else ng[:, idx], spk_bytes)
+    cpu_units, _, _ = units_of(kind, jd0[idx], jd1[idx])
+    gp = out[0][:, idx]
+    gst = (out[2] if nbody else out[3])[idx]
+    err = np.linalg.norm(gp - op, axis=0)
+    ok = (gst == 0) & (st_cpu == 0)
+    tol = 1e-9 if nbody else 1e-12
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "metric": metric, "value": value, "unit": unit, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"plain N-body Radau, {n} main-belt states x {SPAN} d per GPU, "
-                   "Sun+8 planets+Moon from a synthetic SPK type-2 file (14-coef records)",
-                   "n_objects_per_gpu": n, "span_days": SPAN, "launch": best,
-                   "autotune_sweep_ms": sweep,
+        "config": {"workload": WORKLOADS[kind].format(n=n), "n_objects_per_gpu": n,
+                   "launch": best, "autotune_sweep_ms": sweep,
                    "l2": "flushed (256 MB write) between timed steps",
                    "parallelism": f"replicas x{world} (objects independent)"},
-        "object_steps_per_s": world * steps_total * args.steps / t_total,
-        "corrector_iterations_per_step": iters_total / max(steps_total, 1),
         "roofline": roof,
-        "cpu_baseline": {"value": obj_years / cpu_dt, "unit": UNIT, "cores": cores,
+        "cpu_baseline": {"value": cpu_units / cpu_dt, "unit": unit, "cores": cores,
                          "kind": "port",
-                         "sample": f"the full {n}-object workload once, oracle (C restatement "
-                                   "of kete's FP64 path) with OpenMP on all host cores"},
-        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                         "sample": ("the full workload" if len(idx) == n else
+                                    f"seeded 1% subsample ({len(idx)} objects)") +
+                                   ", oracle (C restatement of kete's FP64 path) with OpenMP on "
+                                   "all host cores"},
+        "e2e": {"value": e2e_value, "unit": unit, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
-        "gpu_launches": args.steps,
+        "gpu_launches": args.steps * launches_per_step,
         "clocks": clk.summary(),
         "parity": {"max_err_au": float(err[ok].max()) if ok.any() else None,
-                   "status_match": bool((st_h == st_cpu).all()),
-                   "status_mismatches": int((st_h != st_cpu).sum()),
-                   "gpu_status_counts": np.bincount(st_h, minlength=8).tolist(),
+                   "objects_compared": int(ok.sum()),
+                   "status_mismatches": int((gst != st_cpu).sum()),
+                   "gpu_status_counts": np.bincount(gst, minlength=8).tolist(),
                    "cpu_status_counts": np.bincount(st_cpu, minlength=8).tolist(),
-                   "tolerance_au": 1e-9},
-        "mem_peaks_hbm_gbs": peaks.get("hbm_gbs"),
+                   "tolerance_au": tol},
     }
+    if nbody:
+        line["object_steps_per_s"] = world * steps_total * args.steps / t_total
+        line["corrector_iterations_per_step"] = iters_total / max(steps_total, 1)
     print(json.dumps(line), flush=True)
 
 
@@ -345,7 +415,8 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="kete_b200", choices=["kete_b200", "reference"])
-    ap.add_argument("--n", type=int, default=10_000)
+    ap.add_argument("--n", type=int, default=0, help="objects (0 = the workload's size)")
+    ap.add_argument("--workload", default="nbody_mba_10k", choices=sorted(WORKLOADS))
     ap.add_argument("--mode", type=int, default=0, help="0 = autotune, 1 = thread, 2 = nodes")
     ap.add_argument("--variant", type=int, default=0)
     ap.add_argument("--refill", type=int, default=0)

@@ -1432,6 +1432,15 @@ static double wise_cc(int band, double temp) {
 static double *g_shape = NULL;
 static double g_shape_area = 0.0;
 
+/* All lazily built tables are built once when the library loads, before any OpenMP
+ * region can race on them. */
+__attribute__((constructor)) static void ko_init_tables(void) {
+    rot_init();
+    radau_init();
+    g_shape = (double *)malloc(2048 * 3 * sizeof(double));
+    ko_fib_lattice(2048, g_shape, &g_shape_area);
+}
+
 int ko_neatm_total_flux(const double sun2obj[3], const double sun2obs[3], double h_mag,
                         double g_param, double diam, double vis_albedo, double beaming,
                         double emissivity, int n_bands, const double *bands,
@@ -1439,10 +1448,6 @@ int ko_neatm_total_flux(const double sun2obj[3], const double sun2obs[3], double
                         const double *zero_mags, int wise_color_correction, double *fluxes,
                         double *hg_fluxes, double *thermal, double *mags, double *v_mag,
                         double *v_flux) {
-    if (!g_shape) {
-        g_shape = (double *)malloc(2048 * 3 * sizeof(double));
-        ko_fib_lattice(2048, g_shape, &g_shape_area);
-    }
     double obj2sun[3] = {-sun2obj[0], -sun2obj[1], -sun2obj[2]};
     double obs2obj[3] = {sun2obj[0] - sun2obs[0], sun2obj[1] - sun2obs[1], sun2obj[2] - sun2obs[2]};
     double obs2obj_r = norm3(obs2obj);

@@ -176,3 +176,13 @@ def test_spk_roundtrip(oracle_spk):
 def test_spk_limits(oracle_spk):
     rc, _ = oracle_spk.spk_get_state(5, 2400000.5, 0, 1)
     assert rc == 3  # DAFLimits
+
+
+def test_oracle_thread_count_does_not_change_results(oracle_spk):
+    """The CPU baseline runs under OpenMP; results must not depend on the thread count."""
+    from kete_b200 import synthetic
+
+    pos, vel = synthetic.main_belt(400, seed=17)
+    a = oracle_spk.propagate_n_body(pos, vel, synthetic.EPOCH, synthetic.EPOCH + 120.0, threads=1)
+    b = oracle_spk.propagate_n_body(pos, vel, synthetic.EPOCH, synthetic.EPOCH + 120.0, threads=8)
+    assert (a[2] == 0).all() and np.array_equal(a[0], b[0]) and np.array_equal(a[2], b[2])
