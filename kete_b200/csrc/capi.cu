@@ -4,6 +4,7 @@
 // The ephemeris side restates DafFile::from_buffer / try_load_segments
 // (src/kete_core/src/spice/daf.rs:148-262), SpkSegment / SpkSegmentType2 construction
 // (spice/spk_segments.rs:105-135,379-397) and SpkCollection::load_file (spice/spk.rs:307-329).
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -179,6 +180,46 @@ static int parse_daf(const uint8_t* buf, int64_t n, std::vector<HostSeg>& out, i
     return 0;
 }
 
+// Fast-path plan for the first n_force entries of the force table: the evaluation order
+// (a centre is evaluated before the bodies chained through it, again whenever it changes),
+// each item's first segment, and the time window where all those segments cover and share
+// FAST_NC coefficients.
+static void build_fast_plan(int n_force, FastPlan& P) {
+    std::memset(&P, 0, sizeof P);
+    if (n_force <= 0) return;
+    int n = 0;
+    int current_parent = -1;
+    double lo = -1e300, hi = 1e300;
+    bool ok = true;
+    auto add = [&](int slot, int role) {
+        if (n >= MAX_ITEMS || g_eph.slot[slot].count < 1) {
+            ok = false;
+            return;
+        }
+        const int seg = g_eph.slot[slot].first;
+        const SegDesc& d = g_eph.seg[seg];
+        if (d.n_coef != FAST_NC) ok = false;
+        lo = std::max(lo, d.jd_start);
+        hi = std::min(hi, d.jd_end);
+        P.seg[n] = seg;
+        P.role[n] = role;
+        ++n;
+    };
+    for (int b = 0; b < n_force && ok; ++b) {
+        const int slot = g_eph.force[b].slot;
+        const int parent = g_eph.slot[slot].parent_slot;
+        if (parent >= 0 && parent != current_parent) {
+            add(parent, -1);
+            current_parent = parent;
+        }
+        add(slot, b);
+    }
+    P.n_items = n;
+    P.lo = lo;
+    P.hi = hi;
+    P.ok = (ok && n > 0 && lo <= hi) ? 1 : 0;
+}
+
 // Build the slot / segment / force tables and the device record pool from g_segs.
 static int rebuild_tables() {
     std::memset(&g_eph, 0, sizeof g_eph);
@@ -276,6 +317,8 @@ static int rebuild_tables() {
     }
     g_eph.n_force_planets = planets_ok ? N_PLANETS : 0;
     g_eph.n_force_all = (planets_ok && all_ok) ? N_MASSES : 0;
+    build_fast_plan(g_eph.n_force_planets, g_eph.fast_planets);
+    build_fast_plan(g_eph.n_force_all, g_eph.fast_all);
     g_eph.sun_slot = g_slot_of.count(10) ? g_slot_of[10] : -1;
     g_eph.loaded = 1;
     ++g_version;

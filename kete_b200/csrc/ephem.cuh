@@ -56,10 +56,25 @@ struct CenterChain {
     int slot[3] = {-1, -1, -1};
 };
 
+// Fast evaluation plan: inside [fast_lo, fast_hi] every force body and every centre it is
+// chained through is covered by its first segment (the one the reference's scan returns),
+// all with FAST_NC coefficients.  Items are evaluated two at a time in this order; an item
+// is either a force body (role = index into force[]) or a centre kept for the bodies after
+// it (role = -1).
+constexpr int FAST_NC = 14;
+constexpr int MAX_ITEMS = 24;
+struct FastPlan {
+    double lo, hi;
+    int32_t n_items, ok;
+    int32_t seg[MAX_ITEMS];
+    int32_t role[MAX_ITEMS];
+};
+
 struct EphemConst {
     int32_t n_seg, n_slot;
     int32_t n_force_planets, n_force_all;  // PLANETS (10) and MASSES (15) lengths
     int32_t sun_slot, loaded;
+    FastPlan fast_planets, fast_all;
     SegDesc seg[MAX_SEG];
     Slot slot[MAX_SLOT];
     ForceEntry force[MAX_FORCE];
@@ -127,6 +142,73 @@ __device__ __forceinline__ void cheb_record(const double* __restrict__ rec, int 
     v[0] = dx * tss;
     v[1] = dy * tss;
     v[2] = dz * tss;
+}
+
+// Position/velocity of two records evaluated in lockstep (two independent recurrence chains),
+// NC coefficients per coordinate, fully unrolled.
+template <int NC>
+__device__ __forceinline__ void cheb_pair(const double* __restrict__ ra, const double* __restrict__ rb,
+                                          double jds, double pa[3], double va[3], double pb[3],
+                                          double vb[3]) {
+    constexpr int NP = (NC + 1) & ~1;
+    const double2 ha0 = __ldg(reinterpret_cast<const double2*>(ra));
+    const double2 ha1 = __ldg(reinterpret_cast<const double2*>(ra + 2));
+    const double2 hb0 = __ldg(reinterpret_cast<const double2*>(rb));
+    const double2 hb1 = __ldg(reinterpret_cast<const double2*>(rb + 2));
+    const double xa = (jds - ha0.x) * ha1.x, xb = (jds - hb0.x) * hb1.x;
+    const double xa2 = 2.0 * xa, xb2 = 2.0 * xb;
+    const double2* cxa = reinterpret_cast<const double2*>(ra + 4);
+    const double2* cya = reinterpret_cast<const double2*>(ra + 4 + NP);
+    const double2* cza = reinterpret_cast<const double2*>(ra + 4 + 2 * NP);
+    const double2* cxb = reinterpret_cast<const double2*>(rb + 4);
+    const double2* cyb = reinterpret_cast<const double2*>(rb + 4 + NP);
+    const double2* czb = reinterpret_cast<const double2*>(rb + 4 + 2 * NP);
+    double2 ax = __ldg(cxa), ay = __ldg(cya), az = __ldg(cza);
+    double2 bx = __ldg(cxb), by = __ldg(cyb), bz = __ldg(czb);
+    double avx = ax.x + ax.y * xa, avy = ay.x + ay.y * xa, avz = az.x + az.y * xa;
+    double bvx = bx.x + bx.y * xb, bvy = by.x + by.y * xb, bvz = bz.x + bz.y * xb;
+    double adx = ax.y, ady = ay.y, adz = az.y;
+    double bdx = bx.y, bdy = by.y, bdz = bz.y;
+    double at2 = 1.0, at1 = xa, au2 = 1.0, au1 = xa2;
+    double bt2 = 1.0, bt1 = xb, bu2 = 1.0, bu1 = xb2;
+#pragma unroll
+    for (int k = 1; 2 * k < NC; ++k) {
+        ax = __ldg(cxa + k); ay = __ldg(cya + k); az = __ldg(cza + k);
+        bx = __ldg(cxb + k); by = __ldg(cyb + k); bz = __ldg(czb + k);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int idx = 2 * k + h;
+            if (idx < NC) {
+                const double cax = h ? ax.y : ax.x, cay = h ? ay.y : ay.x, caz = h ? az.y : az.x;
+                const double cbx = h ? bx.y : bx.x, cby = h ? by.y : by.x, cbz = h ? bz.y : bz.x;
+                const double fi = (double)idx;
+                const double ant = xa2 * at1 - at2, bnt = xb2 * bt1 - bt2;
+                avx += cax * ant; avy += cay * ant; avz += caz * ant;
+                bvx += cbx * bnt; bvy += cby * bnt; bvz += cbz * bnt;
+                at2 = at1; at1 = ant;
+                bt2 = bt1; bt1 = bnt;
+                const double anu = xa2 * au1 - au2, bnu = xb2 * bu1 - bu2;
+                const double alu = au1 * fi, blu = bu1 * fi;
+                adx += cax * alu; ady += cay * alu; adz += caz * alu;
+                bdx += cbx * blu; bdy += cby * blu; bdz += cbz * blu;
+                au2 = au1; au1 = anu;
+                bu2 = bu1; bu1 = bnu;
+            }
+        }
+    }
+    constexpr double INV_AU_KM = 1.0 / AU_KM;
+    pa[0] = avx * INV_AU_KM; pa[1] = avy * INV_AU_KM; pa[2] = avz * INV_AU_KM;
+    pb[0] = bvx * INV_AU_KM; pb[1] = bvy * INV_AU_KM; pb[2] = bvz * INV_AU_KM;
+    va[0] = adx * ha1.y; va[1] = ady * ha1.y; va[2] = adz * ha1.y;
+    vb[0] = bdx * hb1.y; vb[1] = bdy * hb1.y; vb[2] = bdz * hb1.y;
+}
+
+// Record of segment `seg` holding TDB seconds `jds` (index clamped to the segment).
+__device__ __forceinline__ const double* eph_record(const EphemConst& E, int seg, double jds) {
+    const SegDesc& d = E.seg[seg];
+    const double fidx = floor((jds - d.start_s) * d.inv_intlen);
+    const int idx = fidx < 0.0 ? 0 : (fidx >= (double)d.n_rec ? d.n_rec - 1 : (int)fidx);
+    return E.pool + d.offset + (int64_t)idx * d.rsize;
 }
 
 // try_get_raw_state for the body in `slot`: first segment (scan order) whose

@@ -175,13 +175,7 @@ __device__ __forceinline__ int from_ssb_equatorial(double t, int frame, const Ce
     return ST_OK;
 }
 
-// Acceleration from the SPK perturbers.  `exact` marks the evaluations at the integrator's
-// accepted states: only those check for impacts (r <= body radius, acceleration.rs:147-158)
-// and update the closest-approach record.  The flag is a runtime value so that one copy of
-// the force code serves every call site.
-//
-// Distances use one reciprocal square root per body: r = r2 * rsqrt(r2) and r^-3 =
-// rsqrt(r2)^3 replace the reference's sqrt and 1/(r*r*r) (a few ulp apart).
+// Acceleration from the SPK perturbers (spk_accel, acceleration.rs:121-168).
 struct SpkForce {
     int n_force;
     NonGrav ng;
@@ -190,11 +184,130 @@ struct SpkForce {
     double min_dist;  // smallest distance to a non-Sun body seen at exact evals
     int32_t min_id;
 
+    // One body's contribution (GravParams::add_acceleration, gravity.rs:171-216, plus the
+    // non-gravitational term relative to the Sun, acceleration.rs:161-165).
+    __device__ __forceinline__ int body(const ForceEntry& fe, bool exact, const double x[3],
+                                        const double v[3], const double bp[3], const double bv[3],
+                                        double& acc0, double& acc1, double& acc2) {
+        const double rp[3] = {x[0] - bp[0], x[1] - bp[1], x[2] - bp[2]};
+        const double rv[3] = {v[0] - bv[0], v[1] - bv[1], v[2] - bv[2]};
+        const double r2 = rp[0] * rp[0] + rp[1] * rp[1] + rp[2] * rp[2];
+        const double ir = rsqrt(r2);
+        const double r = r2 * ir;
+        const double ir3 = ir * ir * ir;
+        if (exact) {
+            if (r <= fe.radius) {
+                impact_id = fe.naif_id;
+                return ST_IMPACT;
+            }
+            if (fe.kind != FK_SUN && r < min_dist) {
+                min_dist = r;
+                min_id = fe.naif_id;
+            }
+        }
+        const double mass = fe.mass;
+        const double kk = mass * ir3;
+        acc0 -= rp[0] * kk;
+        acc1 -= rp[1] * kk;
+        acc2 -= rp[2] * kk;
+        if (fe.kind == FK_SUN || fe.kind == FK_JUPITER) {
+            // apply_gr_correction (gravity.rs:239-253)
+            const double r_v = 4.0 * (rp[0] * rv[0] + rp[1] * rv[1] + rp[2] * rv[2]);
+            const double rel_v2 = rv[0] * rv[0] + rv[1] * rv[1] + rv[2] * rv[2];
+            const double gr_const = mass * C_AU_PER_DAY_INV_SQUARED * ir3;
+            const double c = 4. * mass * ir - rel_v2;
+            acc0 += gr_const * (c * rp[0] + r_v * rv[0]);
+            acc1 += gr_const * (c * rp[1] + r_v * rv[1]);
+            acc2 += gr_const * (c * rp[2] + r_v * rv[2]);
+            // J2 in the ecliptic frame (gravity.rs:188-211, 223-235)
+            const double rc = c_tab.rot_c, rs = c_tab.rot_s;
+            const double ez = -rs * rp[1] + rc * rp[2];
+            const double zr = ez * ir;
+            const double z_squared = 5.0 * (zr * zr);
+            const double rr = fe.radius * ir;
+            const double coef =
+                1.5 * (fe.kind == FK_JUPITER ? JUPITER_J2 : SUN_J2) * mass * (rr * rr) * ir3;
+            const double ey = rc * rp[1] + rs * rp[2];
+            const double jx = rp[0] * coef * (z_squared - 1.0);
+            const double jy = ey * coef * (z_squared - 1.0);
+            const double jz = ez * coef * (z_squared - 3.0);
+            acc0 += jx;
+            acc1 += rc * jy - rs * jz;
+            acc2 += rs * jy + rc * jz;
+            if (fe.kind == FK_SUN && ng.kind != 0) {
+                const double3 na = nongrav_accel(ng, make_double3(rp[0], rp[1], rp[2]),
+                                                 make_double3(rv[0], rv[1], rv[2]));
+                acc0 += na.x;
+                acc1 += na.y;
+                acc2 += na.z;
+            }
+        } else if (fe.kind == FK_EARTH) {
+            const double zr = rp[2] * ir;
+            const double z_squared = 5.0 * (zr * zr);
+            const double rr = fe.radius * ir;
+            const double coef = 1.5 * EARTH_J2 * mass * (rr * rr) * ir3;
+            acc0 += rp[0] * coef * (z_squared - 1.0);
+            acc1 += rp[1] * coef * (z_squared - 1.0);
+            acc2 += rp[2] * coef * (z_squared - 3.0);
+        }
+        return ST_OK;
+    }
+
+    // Fast path: the host-verified window where every body's first segment covers t and all
+    // records have FAST_NC coefficients.  Two records are evaluated per step.
+    __device__ __forceinline__ int eval_fast(const FastPlan& P, bool exact, double t,
+                                             const double x[3], const double v[3], double out[3]) {
+        const double jds = __dmul_rn(t - 2451545.0, 86400.0);
+        double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
+        double cp[3] = {0.0, 0.0, 0.0}, cv[3] = {0.0, 0.0, 0.0};
+        const int n_items = P.n_items;
+#pragma unroll 1
+        for (int it = 0; it < n_items; it += 2) {
+            const bool has_b = it + 1 < n_items;
+            const int sa = P.seg[it];
+            const int sb = has_b ? P.seg[it + 1] : sa;
+            const double* ra = eph_record(c_eph, sa, jds);
+            const double* rb = eph_record(c_eph, sb, jds);
+            double pa[3], va[3], pb[3], vb[3];
+            cheb_pair<FAST_NC>(ra, rb, jds, pa, va, pb, vb);
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                if (h == 1 && !has_b) break;
+                const int role = P.role[it + h];
+                double* bp = h ? pb : pa;
+                double* bv = h ? vb : va;
+                if (role < 0) {
+                    cp[0] = bp[0]; cp[1] = bp[1]; cp[2] = bp[2];
+                    cv[0] = bv[0]; cv[1] = bv[1]; cv[2] = bv[2];
+                    continue;
+                }
+                const ForceEntry fe = c_eph.force[role];
+                if (c_eph.slot[fe.slot].parent_slot >= 0) {
+                    bp[0] += cp[0]; bp[1] += cp[1]; bp[2] += cp[2];
+                    bv[0] += cv[0]; bv[1] += cv[1]; bv[2] += cv[2];
+                }
+                const int rc = body(fe, exact, x, v, bp, bv, acc0, acc1, acc2);
+                if (rc != ST_OK) return rc;
+            }
+        }
+        out[0] = acc0;
+        out[1] = acc1;
+        out[2] = acc2;
+        return ST_OK;
+    }
+
+    // `exact` marks the evaluations at the integrator's accepted states: only those check
+    // for impacts (r <= body radius, acceleration.rs:147-158) and update the closest-approach
+    // record.  The flag is a runtime value so one copy of the force code serves every call
+    // site.  Distances use one reciprocal square root per body: r = r2 * rsqrt(r2) and
+    // r^-3 = rsqrt(r2)^3 replace the reference's sqrt and 1/(r*r*r) (a few ulp apart).
     __device__ __forceinline__ int eval(bool exact, double t, const double x[3], const double v[3],
                                         double out[3]) {
+        const FastPlan& P = n_force == c_eph.n_force_planets ? c_eph.fast_planets : c_eph.fast_all;
+        if (P.ok && t >= P.lo && t <= P.hi) return eval_fast(P, exact, t, x, v, out);
         double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
         int cache_slot = -1;
-        double cp0 = 0.0, cp1 = 0.0, cp2 = 0.0, cv0 = 0.0, cv1 = 0.0, cv2 = 0.0;
+        double cp[3] = {0.0, 0.0, 0.0}, cv[3] = {0.0, 0.0, 0.0};
 #pragma unroll 1
         for (int b = 0; b < n_force; ++b) {
             const ForceEntry fe = c_eph.force[b];
@@ -204,76 +317,14 @@ struct SpkForce {
             const int parent = c_eph.slot[slot].parent_slot;
             if (parent >= 0) {
                 if (parent != cache_slot) {
-                    double q[3], w[3];
-                    if (eph_raw(c_eph, parent, t, q, w) != ST_OK) return ST_DAF_LIMITS;
-                    cp0 = q[0]; cp1 = q[1]; cp2 = q[2];
-                    cv0 = w[0]; cv1 = w[1]; cv2 = w[2];
+                    if (eph_raw(c_eph, parent, t, cp, cv) != ST_OK) return ST_DAF_LIMITS;
                     cache_slot = parent;
                 }
-                bp[0] += cp0; bp[1] += cp1; bp[2] += cp2;
-                bv[0] += cv0; bv[1] += cv1; bv[2] += cv2;
+                bp[0] += cp[0]; bp[1] += cp[1]; bp[2] += cp[2];
+                bv[0] += cv[0]; bv[1] += cv[1]; bv[2] += cv[2];
             }
-            const double rp[3] = {x[0] - bp[0], x[1] - bp[1], x[2] - bp[2]};
-            const double rv[3] = {v[0] - bv[0], v[1] - bv[1], v[2] - bv[2]};
-            const double r2 = rp[0] * rp[0] + rp[1] * rp[1] + rp[2] * rp[2];
-            const double ir = rsqrt(r2);
-            const double r = r2 * ir;
-            const double ir3 = ir * ir * ir;
-            if (exact) {
-                if (r <= fe.radius) {
-                    impact_id = fe.naif_id;
-                    return ST_IMPACT;
-                }
-                if (fe.kind != FK_SUN && r < min_dist) {
-                    min_dist = r;
-                    min_id = fe.naif_id;
-                }
-            }
-            const double mass = fe.mass;
-            const double kk = mass * ir3;
-            acc0 -= rp[0] * kk;
-            acc1 -= rp[1] * kk;
-            acc2 -= rp[2] * kk;
-            if (fe.kind == FK_SUN || fe.kind == FK_JUPITER) {
-                // apply_gr_correction (gravity.rs:239-253)
-                const double r_v = 4.0 * (rp[0] * rv[0] + rp[1] * rv[1] + rp[2] * rv[2]);
-                const double rel_v2 = rv[0] * rv[0] + rv[1] * rv[1] + rv[2] * rv[2];
-                const double gr_const = mass * C_AU_PER_DAY_INV_SQUARED * ir3;
-                const double c = 4. * mass * ir - rel_v2;
-                acc0 += gr_const * (c * rp[0] + r_v * rv[0]);
-                acc1 += gr_const * (c * rp[1] + r_v * rv[1]);
-                acc2 += gr_const * (c * rp[2] + r_v * rv[2]);
-                // J2 in the ecliptic frame (gravity.rs:188-211, 223-235)
-                const double rc = c_tab.rot_c, rs = c_tab.rot_s;
-                const double ez = -rs * rp[1] + rc * rp[2];
-                const double zr = ez * ir;
-                const double z_squared = 5.0 * (zr * zr);
-                const double rr = fe.radius * ir;
-                const double coef = 1.5 * (fe.kind == FK_JUPITER ? JUPITER_J2 : SUN_J2) * mass *
-                                    (rr * rr) * ir3;
-                const double ey = rc * rp[1] + rs * rp[2];
-                const double jx = rp[0] * coef * (z_squared - 1.0);
-                const double jy = ey * coef * (z_squared - 1.0);
-                const double jz = ez * coef * (z_squared - 3.0);
-                acc0 += jx;
-                acc1 += rc * jy - rs * jz;
-                acc2 += rs * jy + rc * jz;
-                if (fe.kind == FK_SUN && ng.kind != 0) {
-                    const double3 na = nongrav_accel(ng, make_double3(rp[0], rp[1], rp[2]),
-                                                     make_double3(rv[0], rv[1], rv[2]));
-                    acc0 += na.x;
-                    acc1 += na.y;
-                    acc2 += na.z;
-                }
-            } else if (fe.kind == FK_EARTH) {
-                const double zr = rp[2] * ir;
-                const double z_squared = 5.0 * (zr * zr);
-                const double rr = fe.radius * ir;
-                const double coef = 1.5 * EARTH_J2 * mass * (rr * rr) * ir3;
-                acc0 += rp[0] * coef * (z_squared - 1.0);
-                acc1 += rp[1] * coef * (z_squared - 1.0);
-                acc2 += rp[2] * coef * (z_squared - 3.0);
-            }
+            const int rc = body(fe, exact, x, v, bp, bv, acc0, acc1, acc2);
+            if (rc != ST_OK) return rc;
         }
         out[0] = acc0;
         out[1] = acc1;
