@@ -116,6 +116,49 @@ int kete_b200_radau_central(int64_t n, const double* pos, const double* vel, con
                             const double* t1, double* out_pos, double* out_vel,
                             int32_t* status, int on_device, void* stream);
 
+/* --- fields of view ----------------------------------------------------------------------
+ * FovLike::check_visible (src/kete_core/src/fov/fov_like.rs:134-192) of n_obj heliocentric
+ * ecliptic states (each at its own epoch jd[i]; valid: NULL or n_obj flags, 0 = skip) in
+ * n_fov rectangular fields at once.  fov is 19 x n_fov: observer jd, observer position[3]
+ * and velocity[3] (heliocentric ecliptic), then the 4 edge normals (12 values) of
+ * OnSkyRectangle (fov/patches.rs:122-155).  Objects within dt_limit days of a field are
+ * pre-filtered by linear motion and confirmed by two-body propagation with light delay;
+ * the others by two-body then N-body propagation (include_asteroids as for
+ * propagate_n_body).  Each visible (field, object) pair writes out_fov, out_obj and the
+ * light-time corrected state out_state (7 x capacity: jd, pos[3], vel[3]); *n_visible is
+ * the total found, which may exceed capacity (the excess is not written: call again with
+ * more capacity).  Order of the pairs is unspecified. */
+int kete_b200_fov_check_visible(int64_t n_obj, const double* pos, const double* vel,
+                                const double* jd, const uint8_t* valid, int64_t n_fov,
+                                const double* fov, double dt_limit, int include_asteroids,
+                                int64_t capacity, int32_t* out_fov, int32_t* out_obj,
+                                double* out_state, int64_t* n_visible, int on_device,
+                                void* stream);
+
+/* --- magnitudes ---------------------------------------------------------------------------
+ * hg_apparent_mag (src/kete/rust/flux/reflected.rs:120-132, HGParams::apparent_mag
+ * src/kete_core/src/flux/reflected.rs:255-268) for n geometries: sun2obj and sun2obs are
+ * 3 x n (AU), h_mag and g_param n each.  Phase angles above 160 degrees give NaN. */
+int kete_b200_hg_apparent_mag(int64_t n, const double* sun2obj, const double* sun2obs,
+                              const double* h_mag, const double* g_param, double* out_mag,
+                              int on_device, void* stream);
+
+/* NeatmParams::apparent_total_flux (src/kete_core/src/flux/neatm.rs:143-185) for n
+ * geometries, each with its own filled H-G parameters (h_mag, g_param, diam km, vis_albedo;
+ * HGParams::fill, reflected.rs:177-238, is the caller's job), beaming and emissivity.  Bands
+ * (1..8) share band_wavelength (nm), sun_correction and zero_mags (NULL = no magnitudes);
+ * band_albedos is n_bands x n.  wise_color_correction applies the WISE W1-W4 colour
+ * corrections (src/kete_core/src/constants/wise.rs:24-78; 4 bands).  Outputs n_bands x n
+ * (fluxes = thermal + reflected, Jy), and v_mag / v_flux (n) as ModelResults. */
+int kete_b200_neatm(int64_t n, const double* sun2obj, const double* sun2obs, const double* h_mag,
+                    const double* g_param, const double* diam, const double* vis_albedo,
+                    const double* beaming, const double* emissivity, int n_bands,
+                    const double* band_wavelength, const double* band_albedos,
+                    const double* sun_correction, const double* zero_mags,
+                    int wise_color_correction, double* fluxes, double* thermal_fluxes,
+                    double* hg_fluxes, double* magnitudes, double* v_mag, double* v_flux,
+                    int on_device, void* stream);
+
 /* --- allocation-free variant (no counterpart in the reference) ---------------------------
  * kete_b200_propagate_n_body on the persistent lane-group grid, for callers that must not
  * have device memory allocated or freed during the call: cudaMalloc/cudaFree synchronize

@@ -4,7 +4,8 @@ Drop-in GPU versions of kete's ``propagate_two_body``, ``propagate_n_body``,
 ``fov_state_check``, ``hg_apparent_mag`` and ``NeatmParams.evaluate``, computed in FP64
 by hand-written sm_100a CUDA kernels in ``libketeb200.so`` (C ABI: include/kete_b200.h).
 """
-from . import spice
+from . import flux, fov, spice
+from .fov import RectangleFOV, fov_state_check
 from ._lib import KeteB200Error, init
 from .propagation import (
     NonGravModel,
@@ -17,6 +18,10 @@ from .propagation import (
 from .state import Frames, SimultaneousStates, State
 
 __all__ = [
+    "flux",
+    "fov",
+    "RectangleFOV",
+    "fov_state_check",
     "spice",
     "init",
     "KeteB200Error",

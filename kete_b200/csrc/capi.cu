@@ -17,6 +17,8 @@
 #include "../../include/kete_b200.h"
 #include "common.cuh"
 #include "ephem.cuh"
+#include "flux.cuh"
+#include "fov_args.h"
 #include "internal.h"
 
 namespace kb {
@@ -77,6 +79,7 @@ struct HostSeg {
 struct DevState {
     int version = -1;       // ephemeris version resident on this device
     bool tables = false;
+    double* facets = nullptr;  // NEATM shape: 2048 unit normals, 3 x 2048
     double* pool = nullptr;
     size_t pool_cap = 0;
     // grow-only staging buffers for host-pointer calls
@@ -369,6 +372,25 @@ static int ensure_tables(DevState& ds) {
     }
     int rc = upload_tables(t);
     if (rc) return rc;
+    // DEFAULT_SHAPE: 2048-facet Fibonacci lattice, total area 1 (flux/shapes.rs:9, 42-66)
+    {
+        const double TAUD = 6.283185307179586, GOLDEN_RATIO = 1.618033988749894, EPS = 0.36;
+        const double nf = (double)N_FACETS;
+        std::vector<double> f(3 * N_FACETS);
+        for (int idx = 0; idx < N_FACETS; ++idx) {
+            const double theta = TAUD * (double)idx / GOLDEN_RATIO;
+            const double phi = std::acos(1.0 - 2.0 * ((double)idx + EPS) / (nf - 1.0 + 2.0 * EPS));
+            f[idx] = std::cos(theta) * std::sin(phi);
+            f[N_FACETS + idx] = std::sin(theta) * std::sin(phi);
+            f[2 * N_FACETS + idx] = std::cos(phi);
+        }
+        if ((rc = cuda_check(cudaMalloc(&ds.facets, f.size() * sizeof(double)), "cudaMalloc facets")))
+            return rc;
+        if ((rc = cuda_check(cudaMemcpy(ds.facets, f.data(), f.size() * sizeof(double),
+                                        cudaMemcpyHostToDevice),
+                             "upload facets")))
+            return rc;
+    }
     ds.tables = true;
     return 0;
 }
@@ -716,6 +738,185 @@ int kete_b200_radau_central(int64_t n, const double* pos, const double* vel, con
     if (S.rc) return S.rc;
     if ((rc = launch_radau_central(n, d_p, d_v, d_t0, d_t1, d_op, d_ov, d_st, st))) return rc;
     return S.finish();
+}
+
+int kete_b200_hg_apparent_mag(int64_t n, const double* sun2obj, const double* sun2obs,
+                              const double* h_mag, const double* g_param, double* out_mag,
+                              int on_device, void* stream) {
+    if (n < 0 || (n > 0 && (!sun2obj || !sun2obs || !h_mag || !g_param || !out_mag)))
+        return set_error(KETE_B200_E_ARGUMENT, "null array");
+    std::lock_guard<std::mutex> lk(g_mu);
+    DevState* ds;
+    int rc = ensure_device(ds);
+    if (rc || n == 0) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    Stager S{*ds, st, on_device};
+    const double* a = S.in(sun2obj, 3 * (size_t)n);
+    const double* b = S.in(sun2obs, 3 * (size_t)n);
+    const double* h = S.in(h_mag, (size_t)n);
+    const double* g = S.in(g_param, (size_t)n);
+    double* o = S.out(out_mag, (size_t)n);
+    if (S.rc) return S.rc;
+    if ((rc = launch_hg_mag(n, a, b, h, g, o, st))) return rc;
+    return S.finish();
+}
+
+int kete_b200_neatm(int64_t n, const double* sun2obj, const double* sun2obs, const double* h_mag,
+                    const double* g_param, const double* diam, const double* vis_albedo,
+                    const double* beaming, const double* emissivity, int n_bands,
+                    const double* band_wavelength, const double* band_albedos,
+                    const double* sun_correction, const double* zero_mags,
+                    int wise_color_correction, double* fluxes, double* thermal_fluxes,
+                    double* hg_fluxes, double* magnitudes, double* v_mag, double* v_flux,
+                    int on_device, void* stream) {
+    if (n_bands < 1 || n_bands > MAX_BANDS)
+        return set_error(KETE_B200_E_ARGUMENT, "n_bands must be 1..8");
+    if (!band_wavelength || !sun_correction) return set_error(KETE_B200_E_ARGUMENT, "null band table");
+    if (wise_color_correction && n_bands != 4)
+        return set_error(KETE_B200_E_ARGUMENT, "WISE colour correction needs the 4 WISE bands");
+    if (n < 0 || (n > 0 && (!sun2obj || !sun2obs || !h_mag || !g_param || !diam || !vis_albedo ||
+                            !beaming || !emissivity || !band_albedos || !fluxes || !thermal_fluxes ||
+                            !hg_fluxes || !v_mag || !v_flux)))
+        return set_error(KETE_B200_E_ARGUMENT, "null array");
+    std::lock_guard<std::mutex> lk(g_mu);
+    DevState* ds;
+    int rc = ensure_device(ds);
+    if (rc || n == 0) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    NeatmArgs a;
+    std::memset(&a, 0, sizeof a);
+    a.n = n;
+    a.n_bands = n_bands;
+    for (int b = 0; b < n_bands; ++b) {
+        a.wavelength[b] = band_wavelength[b];
+        a.sun_correction[b] = sun_correction[b];
+        a.zero_mag[b] = zero_mags ? zero_mags[b] : 0.0;
+    }
+    a.have_zero_mags = zero_mags ? 1 : 0;
+    a.wise_cc = wise_color_correction ? 1 : 0;
+    a.facets = ds->facets;
+    a.facet_area = 1.0 / (double)N_FACETS;
+    Stager S{*ds, st, on_device};
+    a.sun2obj = S.in(sun2obj, 3 * (size_t)n);
+    a.sun2obs = S.in(sun2obs, 3 * (size_t)n);
+    a.h_mag = S.in(h_mag, (size_t)n);
+    a.g_param = S.in(g_param, (size_t)n);
+    a.diam = S.in(diam, (size_t)n);
+    a.vis_albedo = S.in(vis_albedo, (size_t)n);
+    a.beaming = S.in(beaming, (size_t)n);
+    a.emissivity = S.in(emissivity, (size_t)n);
+    a.band_albedo = S.in(band_albedos, (size_t)n_bands * n);
+    a.fluxes = S.out(fluxes, (size_t)n_bands * n);
+    a.thermal = S.out(thermal_fluxes, (size_t)n_bands * n);
+    a.hg_fluxes = S.out(hg_fluxes, (size_t)n_bands * n);
+    a.mags = S.out(magnitudes, (size_t)n_bands * n);
+    a.v_mag = S.out(v_mag, (size_t)n);
+    a.v_flux = S.out(v_flux, (size_t)n);
+    if (S.rc) return S.rc;
+    if ((rc = launch_neatm(a, st))) return rc;
+    return S.finish();
+}
+
+int kete_b200_fov_check_visible(int64_t n_obj, const double* pos, const double* vel,
+                                const double* jd, const uint8_t* valid, int64_t n_fov,
+                                const double* fov, double dt_limit, int include_asteroids,
+                                int64_t capacity, int32_t* out_fov, int32_t* out_obj,
+                                double* out_state, int64_t* n_visible, int on_device,
+                                void* stream) {
+    if (n_obj < 0 || n_fov < 0 || capacity < 0 || !n_visible)
+        return set_error(KETE_B200_E_ARGUMENT, "negative size or null count");
+    if (n_obj > 0 && (!pos || !vel || !jd)) return set_error(KETE_B200_E_ARGUMENT, "null array");
+    if (n_fov > 0 && !fov) return set_error(KETE_B200_E_ARGUMENT, "null field table");
+    if (capacity > 0 && (!out_fov || !out_obj || !out_state))
+        return set_error(KETE_B200_E_ARGUMENT, "null output");
+    if (n_obj > INT32_MAX || n_fov > INT32_MAX)
+        return set_error(KETE_B200_E_ARGUMENT, "more than 2^31 objects or fields");
+    std::lock_guard<std::mutex> lk(g_mu);
+    DevState* ds;
+    int rc = ensure_device(ds);
+    if (rc) return rc;
+    *n_visible = 0;
+    if (n_obj == 0 || n_fov == 0) return 0;
+    cudaStream_t st = (cudaStream_t)stream;
+    Stager S{*ds, st, on_device};
+    FovArgs a;
+    std::memset(&a, 0, sizeof a);
+    a.n_obj = n_obj;
+    a.pos = S.in(pos, 3 * (size_t)n_obj);
+    a.vel = S.in(vel, 3 * (size_t)n_obj);
+    a.jd = S.in(jd, (size_t)n_obj);
+    a.valid = S.in(valid, (size_t)n_obj);
+    a.n_fov = n_fov;
+    a.fov = S.in(fov, (size_t)FOV_STRIDE * n_fov);
+    a.dt_limit = dt_limit;
+    a.capacity = capacity;
+    a.out_fov = S.out(out_fov, (size_t)capacity);
+    a.out_obj = S.out(out_obj, (size_t)capacity);
+    a.out_state = S.out(out_state, 7 * (size_t)capacity);
+    if (S.rc) return S.rc;
+    // scratch: counters and the n-body candidate list (grown and re-run on overflow)
+    void* cnt = nullptr;
+    if ((rc = staging(*ds, 20, 2 * sizeof(unsigned long long), &cnt))) return rc;
+    a.counters = (unsigned long long*)cnt;
+    int64_t cand_cap = std::max<int64_t>(1024, n_obj / 16);
+    unsigned long long h[2] = {0, 0};
+    for (int attempt = 0; attempt < 3; ++attempt) {
+        void *cf = nullptr, *co = nullptr;
+        if ((rc = staging(*ds, 21, (size_t)cand_cap * sizeof(int32_t), &cf))) return rc;
+        if ((rc = staging(*ds, 22, (size_t)cand_cap * sizeof(int32_t), &co))) return rc;
+        a.cand_fov = (int32_t*)cf;
+        a.cand_obj = (int32_t*)co;
+        a.cand_capacity = cand_cap;
+        if ((rc = cuda_check(cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned long long), st), "clear counters")))
+            return rc;
+        if ((rc = launch_fov_prefilter(a, st))) return rc;
+        if ((rc = cuda_check(cudaMemcpyAsync(h, cnt, sizeof h, cudaMemcpyDeviceToHost, st), "read counters")))
+            return rc;
+        if ((rc = cuda_check(cudaStreamSynchronize(st), "stream synchronize"))) return rc;
+        if ((int64_t)h[1] <= cand_cap) break;
+        cand_cap = (int64_t)h[1] + 1024;
+        if (attempt == 2) return set_error(KETE_B200_E_CUDA, "candidate list kept overflowing");
+    }
+    const int64_t m = (int64_t)h[1];
+    if (m > 0) {
+        // n-body branch (fov_like.rs:90-108): Radau every candidate to its field's epoch
+        const int n_force = include_asteroids ? g_eph.n_force_all : g_eph.n_force_planets;
+        if (!g_eph.loaded || n_force == 0)
+            return set_error(KETE_B200_E_NO_EPHEMERIS, "the n-body FOV check needs a loaded SPK");
+        void *gp, *gv, *g0, *g1, *op, *ov, *os;
+        if ((rc = staging(*ds, 23, 3 * (size_t)m * sizeof(double), &gp)) ||
+            (rc = staging(*ds, 24, 3 * (size_t)m * sizeof(double), &gv)) ||
+            (rc = staging(*ds, 25, (size_t)m * sizeof(double), &g0)) ||
+            (rc = staging(*ds, 26, (size_t)m * sizeof(double), &g1)) ||
+            (rc = staging(*ds, 27, 3 * (size_t)m * sizeof(double), &op)) ||
+            (rc = staging(*ds, 28, 3 * (size_t)m * sizeof(double), &ov)) ||
+            (rc = staging(*ds, 29, (size_t)m * sizeof(int32_t), &os)))
+            return rc;
+        if ((rc = launch_fov_gather(a, m, (double*)gp, (double*)gv, (double*)g0, (double*)g1, st)))
+            return rc;
+        NBodyArgs nb;
+        std::memset(&nb, 0, sizeof nb);
+        if ((rc = center_chain(10, nb.chain))) return rc;
+        nb.n = m;
+        nb.pos = (double*)gp;
+        nb.vel = (double*)gv;
+        nb.jd0 = (double*)g0;
+        nb.jd1 = (double*)g1;
+        nb.frame = FRAME_ECLIPTIC;
+        nb.n_force = n_force;
+        nb.out_pos = (double*)op;
+        nb.out_vel = (double*)ov;
+        nb.status = (int32_t*)os;
+        nb.max_loops = 1 << 20;
+        if ((rc = launch_nbody_nodes(nb, g_launch.nodes_variant, 0, st))) return rc;
+        if ((rc = launch_fov_finish(a, m, (double*)op, (double*)ov, (int32_t*)os, st))) return rc;
+        if ((rc = cuda_check(cudaMemcpyAsync(h, cnt, sizeof h, cudaMemcpyDeviceToHost, st), "read counters")))
+            return rc;
+    }
+    if ((rc = S.finish())) return rc;
+    if ((rc = cuda_check(cudaStreamSynchronize(st), "stream synchronize"))) return rc;
+    *n_visible = (int64_t)h[0];
+    return 0;
 }
 
 int kete_b200_set_launch_config(int nodes_variant, int nodes_refill, int thread_block) {

@@ -1,0 +1,156 @@
+// fov.cuh -- field-of-view visibility of many objects in many rectangular fields.
+//
+// Restates FovLike::check_visible (kete_core/fov/fov_like.rs:134-192) with check_linear
+// (:43-66), check_two_body (:71-85), the n-body branch (:90-108, finished by
+// fov_nbody_finish_kernel after a batched Radau pass) and SphericalPolygon::contains
+// (kete_core/fov/patches.rs:214-234).  States and observers are heliocentric ecliptic.
+#pragma once
+#include "common.cuh"
+#include "fov_args.h"
+#include "kepler.cuh"
+
+namespace kb {
+
+
+// SphericalPolygon::contains: inside when no edge normal has a negative (or -0.0) dot
+// product; otherwise the distance to move inside, min(largest violation, |v|).
+__device__ __forceinline__ bool rect_contains(const double* __restrict__ nrm, const double v[3],
+                                              double& dist) {
+    double closest = -INFINITY;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        const double d = v[0] * nrm[3 * e] + v[1] * nrm[3 * e + 1] + v[2] * nrm[3 * e + 2];
+        if (isnan(d)) {
+            dist = d;
+            return false;
+        }
+        if (signbit(d) && fabs(d) > closest) closest = fabs(d);
+    }
+    if (isfinite(closest)) {
+        dist = fmin(closest, norm3(v[0], v[1], v[2]));
+        return false;
+    }
+    dist = 0.0;
+    return true;
+}
+
+// check_two_body: Kepler to the observer epoch, back by the light time, Kepler again.
+__device__ __forceinline__ int fov_two_body(const double* __restrict__ f, double jd,
+                                            const double pos[3], const double vel[3], bool& inside,
+                                            double& dist, double fin[7]) {
+    double p[3] = {pos[0], pos[1], pos[2]}, v[3] = {vel[0], vel[1], vel[2]};
+    const double ojd = f[0];
+    int rc = analytic_2_body(ojd - jd, p, v);
+    if (rc != ST_OK) return rc;
+    const double dt = -norm3(p[0] - f[1], p[1] - f[2], p[2] - f[3]) * C_AU_PER_DAY_INV;
+    const double t2 = ojd + dt;
+    rc = analytic_2_body(t2 - ojd, p, v);
+    if (rc != ST_OK) return rc;
+    const double rel[3] = {p[0] - f[1], p[1] - f[2], p[2] - f[3]};
+    inside = rect_contains(f + 7, rel, dist);
+    fin[0] = t2;
+    fin[1] = p[0]; fin[2] = p[1]; fin[3] = p[2];
+    fin[4] = v[0]; fin[5] = v[1]; fin[6] = v[2];
+    return ST_OK;
+}
+
+__device__ __forceinline__ void fov_emit(const FovArgs& a, int f, int64_t i, const double fin[7]) {
+    const unsigned long long k = atomicAdd(&a.counters[0], 1ULL);
+    if ((int64_t)k < a.capacity) {
+        a.out_fov[k] = f;
+        a.out_obj[k] = (int32_t)i;
+#pragma unroll
+        for (int q = 0; q < 7; ++q) a.out_state[(int64_t)q * a.capacity + k] = fin[q];
+    }
+}
+
+// One thread per object, looping over a tile of fields staged in shared memory.
+__global__ void __launch_bounds__(128) fov_prefilter_kernel(FovArgs a) {
+    __shared__ double s_f[FOV_TILE * FOV_STRIDE];
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool active = i < a.n_obj && (a.valid == nullptr || a.valid[i]);
+    double pos[3] = {0, 0, 0}, vel[3] = {0, 0, 0}, jd = 0.0;
+    if (active) {
+        pos[0] = a.pos[i]; pos[1] = a.pos[a.n_obj + i]; pos[2] = a.pos[2 * a.n_obj + i];
+        vel[0] = a.vel[i]; vel[1] = a.vel[a.n_obj + i]; vel[2] = a.vel[2 * a.n_obj + i];
+        jd = a.jd[i];
+    }
+    for (int64_t base = 0; base < a.n_fov; base += FOV_TILE) {
+        const int nt = (int)((a.n_fov - base) < FOV_TILE ? (a.n_fov - base) : FOV_TILE);
+        __syncthreads();
+        for (int q = threadIdx.x; q < nt * FOV_STRIDE; q += blockDim.x) {
+            const int f = q / FOV_STRIDE, c = q % FOV_STRIDE;
+            s_f[q] = a.fov[(int64_t)c * a.n_fov + base + f];
+        }
+        __syncthreads();
+        if (!active) continue;
+        for (int t = 0; t < nt; ++t) {
+            const double* f = s_f + t * FOV_STRIDE;
+            const double dvx = vel[0] - f[4], dvy = vel[1] - f[5], dvz = vel[2] - f[6];
+            const double max_dist = norm3(dvx, dvy, dvz) * a.dt_limit * 2.0;
+            double dist;
+            double fin[7];
+            bool inside;
+            if (fabs(jd - f[0]) < a.dt_limit) {
+                // check_linear: first-order light delay, straight-line motion
+                const double rel0 = pos[0] - f[1], rel1 = pos[1] - f[2], rel2 = pos[2] - f[3];
+                const double dt = f[0] - jd - norm3(rel0, rel1, rel2) * C_AU_PER_DAY_INV;
+                const double nrel[3] = {pos[0] + vel[0] * dt - f[1], pos[1] + vel[1] * dt - f[2],
+                                        pos[2] + vel[2] * dt - f[3]};
+                if (!rect_contains(f + 7, nrel, dist) && dist > max_dist) continue;
+                if (fov_two_body(f, jd, pos, vel, inside, dist, fin) == ST_OK && inside)
+                    fov_emit(a, (int)(base + t), i, fin);
+            } else {
+                if (fov_two_body(f, jd, pos, vel, inside, dist, fin) != ST_OK) continue;
+                if (!inside && dist > max_dist) continue;
+                const unsigned long long k = atomicAdd(&a.counters[1], 1ULL);
+                if ((int64_t)k < a.cand_capacity) {
+                    a.cand_fov[k] = (int32_t)(base + t);
+                    a.cand_obj[k] = (int32_t)i;
+                }
+            }
+        }
+    }
+}
+
+// Gather the n-body candidates' states (object state, target epoch = observer epoch).
+__global__ void fov_gather_kernel(FovArgs a, int64_t m, double* __restrict__ gpos,
+                                  double* __restrict__ gvel, double* __restrict__ gjd0,
+                                  double* __restrict__ gjd1) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= m) return;
+    const int64_t i = a.cand_obj[k];
+    const int f = a.cand_fov[k];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        gpos[c * m + k] = a.pos[c * a.n_obj + i];
+        gvel[c * m + k] = a.vel[c * a.n_obj + i];
+    }
+    gjd0[k] = a.jd[i];
+    gjd1[k] = a.fov[f];  // row 0 = observer jd
+}
+
+// check_n_body after the Radau pass: light delay by two-body, then containment.
+__global__ void fov_nbody_finish_kernel(FovArgs a, int64_t m, const double* __restrict__ npos,
+                                        const double* __restrict__ nvel,
+                                        const int32_t* __restrict__ nst) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= m || nst[k] != ST_OK) return;
+    const int f = a.cand_fov[k];
+    double fcol[FOV_STRIDE];
+#pragma unroll
+    for (int c = 0; c < FOV_STRIDE; ++c) fcol[c] = a.fov[(int64_t)c * a.n_fov + f];
+    double p[3] = {npos[k], npos[m + k], npos[2 * m + k]};
+    double v[3] = {nvel[k], nvel[m + k], nvel[2 * m + k]};
+    const double ojd = fcol[0];
+    const double dt = -norm3(p[0] - fcol[1], p[1] - fcol[2], p[2] - fcol[3]) * C_AU_PER_DAY_INV;
+    const double t2 = ojd + dt;
+    if (analytic_2_body(t2 - ojd, p, v) != ST_OK) return;
+    const double rel[3] = {p[0] - fcol[1], p[1] - fcol[2], p[2] - fcol[3]};
+    double dist;
+    if (!rect_contains(fcol + 7, rel, dist)) return;
+    const double fin[7] = {t2, p[0], p[1], p[2], v[0], v[1], v[2]};
+    fov_emit(a, f, a.cand_obj[k], fin);
+}
+
+}  // namespace kb

@@ -69,4 +69,15 @@ int launch_spk_states(int64_t n, const int32_t* slot, const double* jd,
 
 int fp64_probe(int64_t iters, double* tflops, float* ms_out);
 
+struct NeatmArgs;
+struct FovArgs;
+int launch_fov_prefilter(const FovArgs& a, cudaStream_t stream);
+int launch_fov_gather(const FovArgs& a, int64_t m, double* gpos, double* gvel, double* gjd0,
+                      double* gjd1, cudaStream_t stream);
+int launch_fov_finish(const FovArgs& a, int64_t m, const double* npos, const double* nvel,
+                      const int32_t* nst, cudaStream_t stream);
+int launch_hg_mag(int64_t n, const double* s2obj, const double* s2obs, const double* h,
+                  const double* g, double* out, cudaStream_t stream);
+int launch_neatm(const NeatmArgs& a, cudaStream_t stream);
+
 }  // namespace kb

@@ -365,3 +365,137 @@ int launch_span_order(int64_t n, const double* jd0, const double* jd1, int* scra
 }
 
 }  // namespace kb
+
+#include "flux.cuh"
+
+namespace kb {
+
+// -------------------------------------------------------------------------------------------
+// hg_apparent_mag for n geometries (src/kete/rust/flux/reflected.rs:120-132)
+// -------------------------------------------------------------------------------------------
+__global__ void hg_mag_kernel(int64_t n, const double* __restrict__ s2obj,
+                              const double* __restrict__ s2obs, const double* __restrict__ h,
+                              const double* __restrict__ g, double* __restrict__ out) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double a[3] = {s2obj[i], s2obj[n + i], s2obj[2 * n + i]};
+    const double b[3] = {s2obs[i], s2obs[n + i], s2obs[2 * n + i]};
+    out[i] = hg_apparent_mag(a, b, h[i], g[i]);
+}
+
+int launch_hg_mag(int64_t n, const double* s2obj, const double* s2obs, const double* h,
+                  const double* g, double* out, cudaStream_t stream) {
+    if (n <= 0) return 0;
+    hg_mag_kernel<<<(unsigned)((n + 127) / 128), 128, 0, stream>>>(n, s2obj, s2obs, h, g, out);
+    return cuda_check(cudaGetLastError(), "hg_mag_kernel launch");
+}
+
+// -------------------------------------------------------------------------------------------
+// NEATM total flux (NeatmParams::apparent_total_flux, flux/neatm.rs:143-185): one warp per
+// geometry, the 2048 facets strided over the lanes, band sums reduced across the warp.
+// -------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) neatm_kernel(NeatmArgs a) {
+    const int lane = threadIdx.x & 31;
+    const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (i >= a.n) return;
+    const int64_t n = a.n;
+    const double s2obj[3] = {a.sun2obj[i], a.sun2obj[n + i], a.sun2obj[2 * n + i]};
+    const double s2obs[3] = {a.sun2obs[i], a.sun2obs[n + i], a.sun2obs[2 * n + i]};
+    const double g = a.g_param[i], diam = a.diam[i], emis = a.emissivity[i];
+    const double obj2sun[3] = {-s2obj[0], -s2obj[1], -s2obj[2]};
+    const double obs2obj[3] = {s2obj[0] - s2obs[0], s2obj[1] - s2obs[1], s2obj[2] - s2obs[2]};
+    const double obs2obj_r = norm3(obs2obj[0], obs2obj[1], obs2obj[2]);
+    // sub_solar_temperature (common.rs:220-236)
+    const double phase_integral = 0.29 + 0.684 * g;
+    const double bond_albedo = a.vis_albedo[i] * phase_integral;
+    const double r2 = obj2sun[0] * obj2sun[0] + obj2sun[1] * obj2sun[1] + obj2sun[2] * obj2sun[2];
+    const double reflected = (1.0 - bond_albedo) * SOLAR_FLUX / r2;
+    double ss_temp = reflected / (a.beaming[i] * emis * STEFAN_BOLTZMANN);
+    ss_temp = ss_temp <= 0.0 ? 0.0 : sqrt(sqrt(ss_temp));
+    const double ns = norm3(obj2sun[0], obj2sun[1], obj2sun[2]);
+    const double o2s[3] = {obj2sun[0] / ns, obj2sun[1] / ns, obj2sun[2] / ns};
+    const double o2o[3] = {obs2obj[0] / obs2obj_r, obs2obj[1] / obs2obj_r, obs2obj[2] / obs2obj_r};
+    const double dscale = obs2obj_r * AU_KM / diam;
+    const double scale = 1.0 / (dscale * dscale);  // powi(-2), common.rs:200
+    double th[MAX_BANDS];
+#pragma unroll
+    for (int b = 0; b < MAX_BANDS; ++b) th[b] = 0.0;
+    for (int f = lane; f < N_FACETS; f += 32) {
+        const double nx = __ldg(a.facets + f), ny = __ldg(a.facets + N_FACETS + f),
+                     nz = __ldg(a.facets + 2 * N_FACETS + f);
+        const double tmp = nx * o2s[0] + ny * o2s[1] + nz * o2s[2];
+        const double temp = tmp > 0.0 ? sqrt(sqrt(tmp)) * ss_temp : 0.0;
+        const double observed = -(nx * o2o[0] + ny * o2o[1] + nz * o2o[2]);
+        const double sc = observed > 0.0 ? observed * emis * PI * scale : 0.0;
+        if (temp == 0.0 || sc == 0.0) continue;
+#pragma unroll
+        for (int b = 0; b < MAX_BANDS; ++b) {
+            if (b < a.n_bands) {
+                double ff = black_body_flux(temp, a.wavelength[b]);
+                if (a.wise_cc) ff *= wise_color_correction(b, temp);
+                ff *= a.facet_area;
+                th[b] += sc * ff;
+            }
+        }
+    }
+#pragma unroll
+    for (int b = 0; b < MAX_BANDS; ++b)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) th[b] += __shfl_xor_sync(0xffffffffu, th[b], o);
+    if (lane < a.n_bands) {
+        const int b = lane;
+        double thb = 0.0;
+#pragma unroll
+        for (int q = 0; q < MAX_BANDS; ++q)
+            if (q == b) thb = th[q];
+        const double refl =
+            hg_apparent_flux(s2obj, s2obs, g, diam, a.wavelength[b], a.band_albedo[(int64_t)b * n + i]) *
+            a.sun_correction[b];
+        const double total = thb + refl;
+        a.thermal[(int64_t)b * n + i] = thb;
+        a.hg_fluxes[(int64_t)b * n + i] = refl;
+        a.fluxes[(int64_t)b * n + i] = total;
+        if (a.mags) a.mags[(int64_t)b * n + i] = a.have_zero_mags ? -2.5 * log10(total / a.zero_mag[b])
+                                                                  : __longlong_as_double(0x7ff8000000000000LL);
+    }
+    if (lane == 0) {
+        const double vm = hg_apparent_mag(s2obj, s2obs, a.h_mag[i], g);
+        a.v_mag[i] = vm;
+        a.v_flux[i] = -2.5 * log10(vm / V_MAG_ZERO);  // flux_to_mag(v_mag, V_MAG_ZERO), neatm.rs:167
+    }
+}
+
+int launch_neatm(const NeatmArgs& a, cudaStream_t stream) {
+    if (a.n <= 0) return 0;
+    const int64_t threads = a.n * 32;
+    neatm_kernel<<<(unsigned)((threads + 127) / 128), 128, 0, stream>>>(a);
+    return cuda_check(cudaGetLastError(), "neatm_kernel launch");
+}
+
+}  // namespace kb
+
+#include "fov.cuh"
+
+namespace kb {
+
+int launch_fov_prefilter(const FovArgs& a, cudaStream_t stream) {
+    if (a.n_obj <= 0 || a.n_fov <= 0) return 0;
+    fov_prefilter_kernel<<<(unsigned)((a.n_obj + 127) / 128), 128, 0, stream>>>(a);
+    return cuda_check(cudaGetLastError(), "fov_prefilter_kernel launch");
+}
+
+int launch_fov_gather(const FovArgs& a, int64_t m, double* gpos, double* gvel, double* gjd0,
+                      double* gjd1, cudaStream_t stream) {
+    if (m <= 0) return 0;
+    fov_gather_kernel<<<(unsigned)((m + 127) / 128), 128, 0, stream>>>(a, m, gpos, gvel, gjd0, gjd1);
+    return cuda_check(cudaGetLastError(), "fov_gather_kernel launch");
+}
+
+int launch_fov_finish(const FovArgs& a, int64_t m, const double* npos, const double* nvel,
+                      const int32_t* nst, cudaStream_t stream) {
+    if (m <= 0) return 0;
+    fov_nbody_finish_kernel<<<(unsigned)((m + 127) / 128), 128, 0, stream>>>(a, m, npos, nvel, nst);
+    return cuda_check(cudaGetLastError(), "fov_nbody_finish_kernel launch");
+}
+
+}  // namespace kb
