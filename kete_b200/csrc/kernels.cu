@@ -256,12 +256,16 @@ namespace kb {
 
 // Node-parallel Radau: 8 lanes per object.  With a.queue == null each group integrates one
 // object (grid covers n groups); with a queue the grid is persistent and groups refill.
-// variant: 0 = no register cap, 1 = >= 3 blocks/SM (168 registers), 2 = >= 4 blocks/SM.
+// variant: 0 = no register cap, 1 = >= 3 blocks/SM (168 registers), 2 = >= 4 blocks/SM;
+// +3: the step-end lane form (exact evaluations taken from lane 7, see radau_nodes.cuh).
 static const void* nodes_kernel_ptr(int variant) {
     switch (variant) {
-        case 1: return (const void*)nbody_nodes_kernel<3>;
-        case 2: return (const void*)nbody_nodes_kernel<4>;
-        default: return (const void*)nbody_nodes_kernel<1>;
+        case 1: return (const void*)nbody_nodes_kernel<3, false>;
+        case 2: return (const void*)nbody_nodes_kernel<4, false>;
+        case 3: return (const void*)nbody_nodes_kernel<1, true>;
+        case 4: return (const void*)nbody_nodes_kernel<3, true>;
+        case 5: return (const void*)nbody_nodes_kernel<4, true>;
+        default: return (const void*)nbody_nodes_kernel<1, false>;
     }
 }
 
@@ -270,9 +274,12 @@ int launch_nbody_nodes(const NBodyArgs& a, int variant, int grid, cudaStream_t s
     const int block = NODES_BLOCK;
     if (grid <= 0) grid = (int)((a.n * NODE_G + block - 1) / block);
     switch (variant) {
-        case 1: nbody_nodes_kernel<3><<<grid, block, 0, stream>>>(a); break;
-        case 2: nbody_nodes_kernel<4><<<grid, block, 0, stream>>>(a); break;
-        default: nbody_nodes_kernel<1><<<grid, block, 0, stream>>>(a); break;
+        case 1: nbody_nodes_kernel<3, false><<<grid, block, 0, stream>>>(a); break;
+        case 2: nbody_nodes_kernel<4, false><<<grid, block, 0, stream>>>(a); break;
+        case 3: nbody_nodes_kernel<1, true><<<grid, block, 0, stream>>>(a); break;
+        case 4: nbody_nodes_kernel<3, true><<<grid, block, 0, stream>>>(a); break;
+        case 5: nbody_nodes_kernel<4, true><<<grid, block, 0, stream>>>(a); break;
+        default: nbody_nodes_kernel<1, false><<<grid, block, 0, stream>>>(a); break;
     }
     return cuda_check(cudaGetLastError(), "nbody_nodes_kernel launch");
 }

@@ -53,22 +53,37 @@ constexpr int NODE_ROW = 17;  // doubles per node row in shared memory (16 used 
 
 // MINB: minimum resident blocks per SM requested from the compiler (1 = no register cap);
 // the host picks the instantiation (occupancy against spills is measured, not guessed).
-template <int MINB>
+// SE (step-end lane): lane 7, otherwise idle during a corrector iteration, evaluates the
+// force at the step end t+h with the predictor of the current iteration (f = 1).  When the
+// iteration converges, that evaluation becomes the exact evaluation of the new state, so
+// no separate round is spent on it.  The point differs from the updated state by the b
+// change of the converged iteration (< 1e-14 of |a| in b6 by the convergence test), far
+// below the integration tolerance; impacts and closest approaches found by lane 7 only
+// count when the iteration converges.  SE = false evaluates the updated state in a round
+// of its own, as radau.rs:331-338 does.
+template <int MINB, bool SE>
 __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_nodes_kernel(NBodyArgs a) {
     // node table: per node j, w_pow[j][0..6], u_pow[j][0..6], spacing, frac2 (rows padded
-    // to 17 doubles so the 8 lanes of a group read 8 different banks)
-    __shared__ double s_node[8 * NODE_ROW];
+    // to 17 doubles so the 8 lanes of a group read 8 different banks); row 8 is the step
+    // end (f = 1: W, U, 1, 1)
+    __shared__ double s_node[9 * NODE_ROW];
     // per group: b (21 doubles, read by every lane for its predictor) and the 8 lanes'
     // evaluations (3 doubles each), exchanged after each corrector iteration
     __shared__ double s_b[NODES_BLOCK / NODE_G][21];
     __shared__ double s_e[NODES_BLOCK / NODE_G][NODE_G * 3];
-    for (int i = threadIdx.x; i < 8 * NODE_ROW; i += blockDim.x) {
+    for (int i = threadIdx.x; i < 9 * NODE_ROW; i += blockDim.x) {
         const int j = i / NODE_ROW, k = i % NODE_ROW;
         double val = 0.0;
-        if (k < 7) val = c_tab.w_pow[j][k];
-        else if (k < 14) val = c_tab.u_pow[j][k - 7];
-        else if (k == 14) val = c_tab.spacing[j];
-        else if (k == 15) val = c_tab.frac2[j];
+        if (j < 8) {
+            if (k < 7) val = c_tab.w_pow[j][k];
+            else if (k < 14) val = c_tab.u_pow[j][k - 7];
+            else if (k == 14) val = c_tab.spacing[j];
+            else if (k == 15) val = c_tab.frac2[j];
+        } else {
+            if (k < 7) val = c_tab.w[k];
+            else if (k < 14) val = c_tab.u[k - 7];
+            else if (k == 14 || k == 15) val = 1.0;
+        }
         s_node[i] = val;
     }
     __syncthreads();
@@ -80,7 +95,8 @@ __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_nodes_kernel(NBodyArg
     double* sb = s_b[threadIdx.x / NODE_G];
     double* se = s_e[threadIdx.x / NODE_G];
     const int comp = lane % 3;  // component this lane forms g and b for (lanes 0-2 publish)
-    const double* nrow = s_node + (lane < 7 ? lane + 1 : 7) * NODE_ROW;
+    const double* nrow = s_node + (lane < 7 ? lane + 1 : (SE ? 8 : 7)) * NODE_ROW;
+    const bool se_lane = SE && lane == 7;
 
     int64_t obj = -1;
     int phase = PH_DONE;
@@ -166,9 +182,12 @@ __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_nodes_kernel(NBodyArg
             }
         }
         // ---- evaluation point of this lane ----
-        const bool exact = phase != PH_ITER;
+        const bool iter_round = phase == PH_ITER;
+        const bool exact = !iter_round || se_lane;
         double te, xe[3], ve[3];
-        if (exact) {
+        double saved_min = F.min_dist;
+        int32_t saved_min_id = F.min_id;
+        if (!iter_round) {
             te = t;
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
@@ -194,15 +213,16 @@ __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_nodes_kernel(NBodyArg
         }
         double ev[3];
         int erc = F.eval(exact, te, xe, ve, ev);
-        // any lane of the group failing fails the group (only DAF limits / impacts occur)
-        const unsigned bad = __ballot_sync(gmask, erc != ST_OK);
+        // any lane of the group failing fails the group (only DAF limits / impacts occur);
+        // the step-end lane's outcome only counts once the iteration converges
+        const unsigned bad = __ballot_sync(gmask, erc != ST_OK && !(iter_round && se_lane));
         if (bad) {
             const int src = __ffs(bad) - 1 - (warp_lane & ~(NODE_G - 1));
             erc = __shfl_sync(gmask, erc, src, NODE_G);
             finish(erc);
             continue;
         }
-        if (exact) {
+        if (!iter_round) {
             cnt.exact++;
             acc[0] = ev[0];
             acc[1] = ev[1];
@@ -280,9 +300,38 @@ __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_nodes_kernel(NBodyArg
             const double mb6 = fmax(fmax(fabs(b60), fabs(b61)), fabs(b62));
             const double r = pow(1e-6 * fmax(fmax(fem0, fem1), fem2) / mb6, 1.0 / 7.0);
             next_h = h * clampd(r, 0.25, 4.0);
-            phase = PH_EXACT_STEP;
-            __syncwarp(gmask);  // b and evaluations consumed before the next round rewrites them
+            if (!SE) {
+                phase = PH_EXACT_STEP;
+                __syncwarp(gmask);  // b and evaluations consumed before the next round rewrites them
+                continue;
+            }
+            // the step-end lane's evaluation is the exact evaluation of the new state
+            const int se_rc = __shfl_sync(gmask, erc, 7, NODE_G);
+            F.min_dist = __shfl_sync(gmask, F.min_dist, 7, NODE_G);
+            F.min_id = __shfl_sync(gmask, F.min_id, 7, NODE_G);
+            F.impact_id = __shfl_sync(gmask, F.impact_id, 7, NODE_G);
+            acc[0] = se[21];
+            acc[1] = se[22];
+            acc[2] = se[23];
+            __syncwarp(gmask);
+            cnt.exact++;
+            if (se_rc != ST_OK) {
+                finish(se_rc);
+                continue;
+            }
+            cnt.steps++;
+            h = next_h;
+            if (fabs(t - tf) < 1e-12) {
+                finish(ST_OK);
+                continue;
+            }
+            failures = 0;
+            start_step();
             continue;
+        }
+        if (se_lane) {  // iteration not converged: forget the step-end lane's record
+            F.min_dist = saved_min;
+            F.min_id = saved_min_id;
         }
         __syncwarp(gmask);
         if (iter >= 10) {  // step failed to converge (radau.rs:345) -> retry smaller

@@ -2,7 +2,9 @@
 
 The node-parallel Radau kernel comes in three register budgets (no cap, 168 registers for
 3 blocks/SM, 128 registers for 4 blocks/SM: more resident lane groups against spills to
-local memory) and in two grid forms (one lane group per object, or a persistent grid
+local memory), each with or without the step-end lane (variants 3-5: the eighth lane
+evaluates the step end during every corrector iteration instead of a separate round) and
+in two grid forms (one lane group per object, or a persistent grid
 whose groups take the next object from a queue).  Which is fastest depends on the object
 count and the spread of their step counts, so it is measured: ``autotune`` times every
 configuration on the caller's own inputs (device arrays) and installs the fastest.
@@ -18,8 +20,8 @@ from . import _lib
 from .propagation import propagate_n_body_arrays
 
 CONFIGS = [dict(mode=_lib.MODE_NODES, variant=v, refill=r) for v, r in
-           itertools.product((0, 1, 2), (0, 1))] + [dict(mode=_lib.MODE_THREAD, variant=0,
-                                                         refill=0)]
+           itertools.product((0, 1, 2, 3, 4, 5), (0, 1))] + [dict(mode=_lib.MODE_THREAD,
+                                                                 variant=0, refill=0)]
 _current = dict(mode=_lib.MODE_NODES, variant=0, refill=0, thread_block=128)
 
 

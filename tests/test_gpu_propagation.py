@@ -111,9 +111,11 @@ def test_spk_states_vs_oracle(gpu, oracle_spk):
 
 
 # launch configurations: one object per thread; eight node lanes per object without a
-# register cap; with a 128-register cap on a persistent grid that refills from a queue
+# register cap; with a 128-register cap on a persistent grid that refills from a queue; and
+# the step-end-lane forms (lane 7 supplies the exact evaluation of each accepted step)
 CONFIGS = (dict(mode=1, variant=0, refill=0), dict(mode=2, variant=0, refill=0),
-           dict(mode=2, variant=2, refill=1))
+           dict(mode=2, variant=2, refill=1), dict(mode=2, variant=3, refill=1),
+           dict(mode=2, variant=5, refill=0))
 MODES = CONFIGS
 
 
