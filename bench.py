@@ -157,12 +157,14 @@ def dist_setup():
 
 
 def reduce_max(x, world):
+    """Maximum of a per-rank value over all ranks (the job's time is its slowest rank)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 

@@ -201,7 +201,7 @@ static void build_fast_plan(int n_force, FastPlan& P) {
         }
         const int seg = g_eph.slot[slot].first;
         const SegDesc& d = g_eph.seg[seg];
-        if (d.n_coef != FAST_NC) ok = false;
+        if (d.n_pad != FAST_NC) ok = false;
         lo = std::max(lo, d.jd_start);
         hi = std::min(hi, d.jd_end);
         P.seg[n] = seg;
@@ -237,6 +237,12 @@ static int rebuild_tables() {
         }
     if ((int)ids.size() > MAX_SLOT) return set_error(KETE_B200_E_UNSUPPORTED, "too many SPK bodies for the device table");
     if ((int)g_segs.size() > MAX_SEG) return set_error(KETE_B200_E_UNSUPPORTED, "too many SPK segments for the device table");
+    // coefficient blocks padded to one common width when every segment fits the fast path's
+    // FAST_NC, so mixed coefficient counts (as in DE440s) still take it: the extra zero
+    // coefficients add exactly nothing to the sums
+    int64_t max_coef = 0;
+    for (const auto& sg : g_segs) max_coef = std::max<int64_t>(max_coef, sg.n_coef);
+    const bool common_pad = max_coef <= FAST_NC;
     int nseg = 0;
     for (size_t si = 0; si < ids.size(); ++si) {
         Slot& sl = g_eph.slot[si];
@@ -260,7 +266,7 @@ static int rebuild_tables() {
             d.intlen = s.intlen;
             d.inv_intlen = 1.0 / s.intlen;
             d.n_coef = (int32_t)s.n_coef;
-            d.n_pad = (int32_t)((s.n_coef + 1) & ~1LL);
+            d.n_pad = common_pad ? FAST_NC : (int32_t)((s.n_coef + 1) & ~1LL);
             d.n_rec = (int32_t)s.n_rec;
             d.rsize = 4 + 3 * d.n_pad;
             d.offset = (int64_t)g_pool_host.size();

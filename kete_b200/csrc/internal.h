@@ -69,6 +69,24 @@ int launch_spk_states(int64_t n, const int32_t* slot, const double* jd,
 
 int fp64_probe(int64_t iters, double* tflops, float* ms_out);
 
+struct StmArgs {
+    int64_t n;
+    const double* pos;
+    const double* vel;
+    const double* jd0;
+    int n_epochs;
+    const double* epochs;   // device, n_epochs
+    const double* nongrav;  // 10 x n or null
+    int frame;
+    CenterChain chain;
+    int n_force;
+    double* out_state;  // n_epochs x 6 x n
+    double* out_stm;    // n_epochs x 48 x n (row-major 6 x 8 per object)
+    int32_t* status;
+    int max_loops;
+};
+int launch_nbody_stm(const StmArgs& a, cudaStream_t stream);
+
 struct NeatmArgs;
 struct FovArgs;
 int launch_fov_prefilter(const FovArgs& a, cudaStream_t stream);

@@ -208,6 +208,14 @@ def synthetic_bodies(t_jd, seed=2024):
     f_moon = MASS_RATIO[399] / m_emb
     out[399] = (-(1 - f_moon) * mp, -(1 - f_moon) * mv, 3)
     out[301] = (f_moon * mp, f_moon * mv, 3)
+    # the five large asteroids kete adds with include_asteroids (gravity.rs:104-133), given
+    # relative to the Sun (10) as asteroid SPKs are
+    rng = np.random.default_rng(seed + 7)
+    for aid in ASTEROIDS:
+        a_, e_, i_ = rng.uniform(2.2, 3.2), rng.uniform(0.05, 0.25), np.radians(rng.uniform(2, 20))
+        lan, argp, m0 = rng.uniform(0, 2 * np.pi, 3)
+        ap, av = kepler_state(a_, e_, i_, lan, argp, m0, EPOCH, t_jd)
+        out[aid] = (ap, av, 10)
     res = {}
     for k, (p, v, c) in out.items():
         res[k] = (ecl_to_eq(p) * AU_KM, ecl_to_eq(v) * AU_KM / 86400.0, c)
@@ -286,15 +294,21 @@ def write_daf_spk(path, segments, internal_name="kete_b200 synthetic ephemeris")
 
 
 SPK_BODIES = (10, 1, 2, 3, 399, 301, 4, 5, 6, 7, 8)
+ASTEROIDS = (20000001, 20000002, 20000004, 20000010, 20000704)
 
 
 def write_synthetic_spk(path, jd_start=2457000.5, jd_end=2463000.5, record_days=32.0,
-                        moon_record_days=8.0, n_coef=14, seed=2024):
-    """Write the synthetic perturber SPK used by the tests and the benchmark."""
+                        moon_record_days=8.0, n_coef=14, seed=2024, asteroids=False):
+    """Write the synthetic perturber SPK used by the tests and the benchmark.
+
+    n_coef: coefficients per coordinate, one count for every body or a dict body -> count
+    (real ephemerides mix counts).  asteroids: also write the five large asteroids."""
     segs = []
-    for body in SPK_BODIES:
+    bodies = SPK_BODIES + (ASTEROIDS if asteroids else ())
+    for body in bodies:
         rd = moon_record_days if body in (399, 301) else record_days
-        data, center = fit_type2_segment(body, jd_start, jd_end, rd, n_coef, seed)
+        nc = n_coef.get(body, 14) if isinstance(n_coef, dict) else n_coef
+        data, center = fit_type2_segment(body, jd_start, jd_end, rd, nc, seed)
         n_rec = int(data[-1])
         s0 = (jd_start - J2000) * 86400.0
         s1 = s0 + n_rec * rd * 86400.0

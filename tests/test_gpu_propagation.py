@@ -255,3 +255,44 @@ def test_autotune_installs_a_working_config(gpu, oracle_spk):
     op, _, ost, _, _ = oracle_spk.propagate_n_body(pos, vel, jd0, jd1)
     assert (st == 0).all() and np.abs(p - op).max() < 1e-9
     tune.set_config()
+
+
+@pytest.fixture(scope="module")
+def mixed_spk(tmp_path_factory):
+    """An ephemeris with per-body coefficient counts like DE440s and the five asteroids."""
+    p = tmp_path_factory.mktemp("spk_mixed") / "mixed.bsp"
+    counts = {10: 11, 1: 14, 2: 10, 3: 13, 399: 13, 301: 13, 4: 11, 5: 8, 6: 7, 7: 6, 8: 6}
+    synthetic.write_synthetic_spk(str(p), n_coef=counts, asteroids=True)
+    return str(p)
+
+
+def test_mixed_coefficients_and_asteroids_vs_oracle(gpu, oracle, mixed_spk, spk_path):
+    try:
+        gpu.spice.kernel_reload([mixed_spk])
+        oracle.spk_reset()
+        oracle.spk_load_bytes(open(mixed_spk, "rb").read())
+        rng = np.random.default_rng(101)
+        jd = rng.uniform(2457100, 2462900, 200)
+        for body in (10, 5, 8, 399, 301, 20000001, 20000704):
+            out6, st = gpu.spice.get_states_arrays(body, jd, 0, 1)
+            assert (st == 0).all()
+            for k in range(0, 200, 20):
+                rc, ref = oracle.spk_get_state(body, jd[k], 0, 1)
+                assert rc == 0
+                assert np.abs(out6[:3, k] - ref[:3]).max() < 5e-14 * max(1.0, np.abs(ref[:3]).max())
+        n = 600
+        pos, vel = synthetic.main_belt(n, seed=102)
+        jd0, jd1 = np.full(n, EPOCH), np.full(n, EPOCH + 200.0)
+        for inc in (False, True):
+            op, ov, ost, _, _ = oracle.propagate_n_body(pos, vel, jd0, jd1, include_extended=inc)
+            for cfg in CONFIGS[:2] + CONFIGS[3:4]:
+                mode = _set(gpu, cfg)
+                p, v, st = gpu.propagate_n_body_arrays(pos, vel, jd0, jd1, include_asteroids=inc,
+                                                       mode=mode)
+                assert (st == ost).all() and (st == 0).all()
+                assert np.abs(p - op).max() < 1e-9, (inc, cfg)
+    finally:  # restore the session ephemeris for the tests that follow
+        gpu.spice.kernel_reload([spk_path])
+        oracle.spk_reset()
+        oracle.spk_load_bytes(open(spk_path, "rb").read())
+        _set(gpu, dict(mode=2, variant=0, refill=0))
