@@ -110,6 +110,20 @@ int kete_b200_propagate_n_body(int64_t n, const double* pos, const double* vel,
                                double* impact_jd, double* min_dist, int32_t* counters, int mode,
                                int on_device, void* stream);
 
+/* propagate_n_body_spk (src/kete_core/src/propagation/mod.rs:70-118) to a sequence of epochs
+ * with forward sensitivities.  Object i starts at jd0[i]; each of the n_epochs epochs
+ * (shared, in the order to visit) starts a fresh integration from the previous one.  For
+ * every epoch k: out_state (n_epochs x 6 x n: pos, vel in `frame`/`center`) and out_stm
+ * (n_epochs x 48 x n: the 6 x 8 matrix d(pos, vel)/d(pos0, vel0, A1, A2), row-major), the
+ * derivative of the executed Radau steps (step sizes held fixed) with respect to the
+ * initial state and the JPL comet A1/A2 parameters (nongrav kind 1, dt = 0).  status[i]
+ * reports the first failure; later epochs of a failed object are NaN. */
+int kete_b200_propagate_n_body_stm(int64_t n, const double* pos, const double* vel,
+                                   const double* jd0, int n_epochs, const double* epochs,
+                                   int frame, int64_t center, int include_asteroids,
+                                   const double* nongrav, double* out_state, double* out_stm,
+                                   int32_t* status, int on_device, void* stream);
+
 /* RadauIntegrator::integrate with central_accel (propagation/mod.rs:35-46,126-138): the
  * integrator alone, for checking it against kete's closed-form two-body result. */
 int kete_b200_radau_central(int64_t n, const double* pos, const double* vel, const double* t0,

@@ -4,7 +4,7 @@ Drop-in GPU versions of kete's ``propagate_two_body``, ``propagate_n_body``,
 ``fov_state_check``, ``hg_apparent_mag`` and ``NeatmParams.evaluate``, computed in FP64
 by hand-written sm_100a CUDA kernels in ``libketeb200.so`` (C ABI: include/kete_b200.h).
 """
-from . import flux, fov, spice
+from . import autodiff, flux, fov, spice
 from .fov import RectangleFOV, fov_state_check
 from ._lib import KeteB200Error, init
 from .propagation import (
@@ -18,6 +18,7 @@ from .propagation import (
 from .state import Frames, SimultaneousStates, State
 
 __all__ = [
+    "autodiff",
     "flux",
     "fov",
     "RectangleFOV",

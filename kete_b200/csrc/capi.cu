@@ -823,6 +823,47 @@ int kete_b200_neatm(int64_t n, const double* sun2obj, const double* sun2obs, con
     return S.finish();
 }
 
+int kete_b200_propagate_n_body_stm(int64_t n, const double* pos, const double* vel,
+                                   const double* jd0, int n_epochs, const double* epochs,
+                                   int frame, int64_t center, int include_asteroids,
+                                   const double* nongrav, double* out_state, double* out_stm,
+                                   int32_t* status, int on_device, void* stream) {
+    if (n < 0 || n_epochs < 1 || !epochs)
+        return set_error(KETE_B200_E_ARGUMENT, "need n >= 0 and at least one epoch");
+    if (n > 0 && (!pos || !vel || !jd0 || !out_state || !out_stm || !status))
+        return set_error(KETE_B200_E_ARGUMENT, "null array");
+    std::lock_guard<std::mutex> lk(g_mu);
+    int rc = check_frame(frame);
+    if (rc) return rc;
+    if (!g_eph.loaded) return set_error(KETE_B200_E_NO_EPHEMERIS, "no SPK loaded");
+    const int n_force = include_asteroids ? g_eph.n_force_all : g_eph.n_force_planets;
+    if (n_force == 0) return set_error(KETE_B200_E_NO_EPHEMERIS, "loaded SPKs lack a perturber");
+    StmArgs a;
+    std::memset(&a, 0, sizeof a);
+    if ((rc = center_chain(center, a.chain))) return rc;
+    DevState* ds;
+    if ((rc = ensure_device(ds))) return rc;
+    if (n == 0) return 0;
+    cudaStream_t st = (cudaStream_t)stream;
+    Stager S{*ds, st, on_device};
+    a.n = n;
+    a.pos = S.in(pos, 3 * (size_t)n);
+    a.vel = S.in(vel, 3 * (size_t)n);
+    a.jd0 = S.in(jd0, (size_t)n);
+    a.n_epochs = n_epochs;
+    a.epochs = S.in(epochs, (size_t)n_epochs);
+    a.nongrav = S.in(nongrav, 10 * (size_t)n);
+    a.frame = frame;
+    a.n_force = n_force;
+    a.out_state = S.out(out_state, (size_t)n_epochs * 6 * n);
+    a.out_stm = S.out(out_stm, (size_t)n_epochs * 48 * n);
+    a.status = S.out(status, (size_t)n);
+    a.max_loops = 1 << 20;
+    if (S.rc) return S.rc;
+    if ((rc = launch_nbody_stm(a, st))) return rc;
+    return S.finish();
+}
+
 int kete_b200_fov_check_visible(int64_t n_obj, const double* pos, const double* vel,
                                 const double* jd, const uint8_t* valid, int64_t n_fov,
                                 const double* fov, double dt_limit, int include_asteroids,
