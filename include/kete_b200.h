@@ -35,6 +35,7 @@ extern "C" {
 #define KETE_B200_IO_ERROR 5
 #define KETE_B200_IMPACT 6
 #define KETE_B200_TIMEOUT 7
+#define KETE_B200_CHECKPOINT_FULL 8  /* checkpoint capacity too small; ckpt_count says how many */
 
 /* call return codes */
 #define KETE_B200_E_ARGUMENT (-1)
@@ -123,6 +124,41 @@ int kete_b200_propagate_n_body_stm(int64_t n, const double* pos, const double* v
                                    int frame, int64_t center, int include_asteroids,
                                    const double* nongrav, double* out_state, double* out_stm,
                                    int32_t* status, int on_device, void* stream);
+
+/* Reverse-mode gradients of propagate_n_body_spk (src/kete_core/src/propagation/mod.rs:70-118)
+ * through a sequence of epochs, in two calls.
+ *
+ * kete_b200_propagate_n_body_checkpointed: the forward pass.  Same integration and outputs
+ * (out_state: n_epochs x 6 x n, status: n) as kete_b200_propagate_n_body_stm without the
+ * matrices.  Before every 16th step attempt of each epoch segment it stores a checkpoint
+ * (34 doubles: t, h, failures, x, v, a and the Radau b) in `checkpoints`
+ * (n x ckpt_capacity x 34 doubles); ckpt_count (n) receives how many were taken and
+ * ckpt_segment (n_epochs x n) the first checkpoint of each segment.  An object that needs
+ * more than ckpt_capacity gets status KETE_B200_CHECKPOINT_FULL (its states are still
+ * valid): call again with ckpt_capacity >= max(ckpt_count).  Non-gravitational models must
+ * have dt = 0 (status KETE_B200_VALUE_ERROR otherwise).
+ *
+ * kete_b200_propagate_n_body_adjoint: the adjoint pass.  Given the forward pass's
+ * checkpoints and status and seed = dL/d(out_state) (n_epochs x 6 x n), writes
+ * out_grad (8 x n) = dL/d(pos0, vel0, A1, A2) in the caller's frame: the transposed
+ * executed Radau steps (step sizes and iteration counts held fixed), recomputed block by
+ * block from the checkpoints.  Objects whose forward status is not OK get NaN; grad_status
+ * (n, may be NULL) reports failures of the adjoint pass itself.  epochs, frame,
+ * include_asteroids and nongrav must be those of the forward pass. */
+int kete_b200_propagate_n_body_checkpointed(int64_t n, const double* pos, const double* vel,
+                                            const double* jd0, int n_epochs, const double* epochs,
+                                            int frame, int64_t center, int include_asteroids,
+                                            const double* nongrav, double* out_state,
+                                            int32_t* status, int ckpt_capacity,
+                                            double* checkpoints, int32_t* ckpt_count,
+                                            int32_t* ckpt_segment, int on_device, void* stream);
+int kete_b200_propagate_n_body_adjoint(int64_t n, int n_epochs, const double* epochs, int frame,
+                                       int include_asteroids, const double* nongrav,
+                                       int ckpt_capacity, const double* checkpoints,
+                                       const int32_t* ckpt_count, const int32_t* ckpt_segment,
+                                       const int32_t* status, const double* seed,
+                                       double* out_grad, int32_t* grad_status, int on_device,
+                                       void* stream);
 
 /* RadauIntegrator::integrate with central_accel (propagation/mod.rs:35-46,126-138): the
  * integrator alone, for checking it against kete's closed-form two-body result. */

@@ -1,11 +1,19 @@
-"""Gradients of N-body predictions: forward sensitivities behind torch.autograd.
+"""Gradients of N-body predictions behind torch.autograd.
 
-``propagate_n_body_stm_arrays`` runs kete's N-body propagation (src/kete_core/src/
-propagation/mod.rs:70-118) through a sequence of epochs and returns, with each state, its
-6 x 8 derivative with respect to the initial position, initial velocity and the JPL comet
-A1/A2 parameters -- the exact derivative of the Radau steps the GPU executed (step sizes
-held fixed).  ``NBodyPositions`` wraps it as a torch.autograd.Function, so losses built on
-the predicted positions (e.g. RA/Dec residuals) differentiate with torch.
+Two GPU routes differentiate kete's N-body propagation (src/kete_core/src/propagation/
+mod.rs:70-118) through a sequence of epochs with respect to the initial position, initial
+velocity and the JPL comet A1/A2 parameters, both as derivatives of the Radau steps the
+GPU executed (step sizes held fixed):
+
+* reverse mode (the default): ``propagate_n_body_checkpointed`` integrates and stores a
+  checkpoint every 16 step attempts; ``propagate_n_body_adjoint`` turns dL/d(states) into
+  dL/d(pos0, vel0, A1, A2) by re-running each checkpoint block and transposing its steps;
+* forward mode: ``propagate_n_body_stm_arrays`` returns the 6 x 8 sensitivity matrix of
+  every state (the check of the reverse mode, and the tool when the matrices themselves
+  are wanted, e.g. for covariance propagation).
+
+``nbody_states`` / ``nbody_positions`` wrap either as a torch.autograd.Function, so losses
+built on predicted positions (RA/Dec residuals) differentiate with torch.
 """
 from __future__ import annotations
 
@@ -17,12 +25,20 @@ from . import _lib
 from .state import Frames
 
 
+CHECKPOINT_FULL = 8
+SENS_STRIDE = 34
+SENS_CK_ATTEMPTS = 16
+
+
 def _bind():
     L = _lib.lib()
     v = ctypes.c_void_p
-    L.kete_b200_propagate_n_body_stm.argtypes = [ctypes.c_int64, v, v, v, ctypes.c_int, v,
-                                                 ctypes.c_int, ctypes.c_int64, ctypes.c_int, v, v,
-                                                 v, v, ctypes.c_int, v]
+    i, i64 = ctypes.c_int, ctypes.c_int64
+    L.kete_b200_propagate_n_body_stm.argtypes = [i64, v, v, v, i, v, i, i64, i, v, v, v, v, i, v]
+    L.kete_b200_propagate_n_body_checkpointed.argtypes = [i64, v, v, v, i, v, i, i64, i, v, v, v,
+                                                          i, v, v, v, i, v]
+    L.kete_b200_propagate_n_body_adjoint.argtypes = [i64, i, v, i, i, v, i, v, v, v, v, v, v, v,
+                                                     i, v]
     return L
 
 
@@ -58,48 +74,145 @@ def propagate_n_body_stm_arrays(pos, vel, jd0, epochs, frame=Frames.Ecliptic, ce
     return states, stm, st
 
 
+class Checkpoints:
+    """What the adjoint pass needs from a checkpointed forward pass."""
+
+    def __init__(self, n, epochs, frame, include_asteroids, nongrav, capacity, ckpt, count,
+                 segment, status):
+        self.n, self.epochs, self.frame = n, epochs, frame
+        self.include_asteroids, self.nongrav, self.capacity = include_asteroids, nongrav, capacity
+        self.ckpt, self.count, self.segment, self.status = ckpt, count, segment, status
+
+
+def _default_capacity(jd0, epochs):
+    """Checkpoints per object for spans of at least 1 day per attempt on average."""
+    e = np.asarray(epochs.detach().cpu() if hasattr(epochs, "detach") else epochs, np.float64)
+    j = np.asarray(jd0.detach().cpu() if hasattr(jd0, "detach") else jd0, np.float64)
+    span = np.abs(e[0] - j).max() + np.abs(np.diff(e)).sum() if e.size else 0.0
+    return int(e.size + np.ceil(span / SENS_CK_ATTEMPTS) + 2)
+
+
+def propagate_n_body_checkpointed(pos, vel, jd0, epochs, frame=Frames.Ecliptic, center=10,
+                                  include_asteroids=False, nongrav=None, capacity=None):
+    """Forward pass of the reverse-mode gradient: states (K, 6, n), status (n,) and the
+    Checkpoints for ``propagate_n_body_adjoint``.  Objects that need more checkpoints than
+    the capacity are re-run once with the capacity they reported."""
+    _lib.init()
+    L = _bind()
+    n = int(pos.shape[1])
+    dev = _lib._is_torch_cuda(pos)
+    if dev:
+        import torch
+
+        if not _lib._is_torch_cuda(epochs):
+            epochs = torch.as_tensor(np.asarray(epochs, np.float64), device=pos.device)
+        K = int(epochs.shape[0])
+    else:
+        epochs = np.ascontiguousarray(np.atleast_1d(np.asarray(epochs, np.float64)))
+        K = int(epochs.size)
+    cap = int(capacity or _default_capacity(jd0, epochs))
+    for _ in range(2):
+        if dev:
+            states = torch.empty((K, 6, n), dtype=torch.float64, device=pos.device)
+            st = torch.empty(n, dtype=torch.int32, device=pos.device)
+            ck = torch.empty((n, cap, SENS_STRIDE), dtype=torch.float64, device=pos.device)
+            cnt = torch.empty(n, dtype=torch.int32, device=pos.device)
+            seg = torch.empty((K, n), dtype=torch.int32, device=pos.device)
+        else:
+            states, st = np.empty((K, 6, n)), np.empty(n, dtype=np.int32)
+            ck = np.empty((n, cap, SENS_STRIDE))
+            cnt, seg = np.empty(n, dtype=np.int32), np.empty((K, n), dtype=np.int32)
+        a = _lib.Args()
+        args = [a.ptr(pos), a.ptr(vel), a.ptr(jd0), K, a.ptr(epochs), int(frame), int(center),
+                int(bool(include_asteroids)), a.ptr(nongrav), a.ptr(states), a.ptr(st, np.int32),
+                cap, a.ptr(ck), a.ptr(cnt, np.int32), a.ptr(seg, np.int32)]
+        _lib.check(L.kete_b200_propagate_n_body_checkpointed(n, *args, a.on_device, a.stream))
+        full = (st == CHECKPOINT_FULL)
+        if not bool(full.any()):
+            break
+        cap = int(cnt.max())
+    return states, st, Checkpoints(n, epochs, frame, include_asteroids, nongrav, cap, ck, cnt, seg,
+                                   st)
+
+
+def propagate_n_body_adjoint(ck: Checkpoints, seed):
+    """dL/d(pos0, vel0, A1, A2) (8, n) from seed = dL/d(states) (K, 6, n); also the
+    adjoint pass's own status (n,)."""
+    L = _bind()
+    n = ck.n
+    K = int(ck.epochs.shape[0])
+    if _lib._is_torch_cuda(ck.ckpt):
+        import torch
+
+        grad = torch.empty((8, n), dtype=torch.float64, device=ck.ckpt.device)
+        gst = torch.empty(n, dtype=torch.int32, device=ck.ckpt.device)
+        seed = seed.to(torch.float64).contiguous()
+    else:
+        grad, gst = np.empty((8, n)), np.empty(n, dtype=np.int32)
+        seed = np.ascontiguousarray(seed, dtype=np.float64)
+    a = _lib.Args()
+    args = [K, a.ptr(ck.epochs), int(ck.frame), int(bool(ck.include_asteroids)),
+            a.ptr(ck.nongrav), ck.capacity, a.ptr(ck.ckpt), a.ptr(ck.count, np.int32),
+            a.ptr(ck.segment, np.int32), a.ptr(ck.status, np.int32), a.ptr(seed), a.ptr(grad),
+            a.ptr(gst, np.int32)]
+    _lib.check(L.kete_b200_propagate_n_body_adjoint(n, *args, a.on_device, a.stream))
+    return grad, gst
+
+
 def _torch_function():
     import torch
 
-    class NBodyPositions(torch.autograd.Function):
-        """Positions (K, 3, n) at `epochs` as a differentiable function of the initial
+    class NBodyStates(torch.autograd.Function):
+        """States (K, 6, n) at `epochs` as a differentiable function of the initial
         position (3, n), velocity (3, n) and JPL comet A1, A2 (n,) of each object."""
 
         @staticmethod
-        def forward(ctx, pos0, vel0, a1, a2, jd0, epochs, frame, center, nongrav_rest):
-            ng = nongrav_rest.clone()
-            ng[1] = a1
-            ng[2] = a2
-            states, stm, st = propagate_n_body_stm_arrays(pos0.detach().contiguous(),
-                                                          vel0.detach().contiguous(), jd0,
-                                                          epochs, frame, center, False,
-                                                          ng.contiguous())
-            ctx.save_for_backward(stm)
+        def forward(ctx, pos0, vel0, a1, a2, jd0, epochs, frame, center, nongrav_rest, method):
+            ng = nongrav_rest.detach().clone()
+            ng[1] = a1.detach()
+            ng[2] = a2.detach()
+            ng = ng.contiguous()
+            p0, v0 = pos0.detach().contiguous(), vel0.detach().contiguous()
+            ctx.method = method
+            if method == "stm":
+                states, stm, st = propagate_n_body_stm_arrays(p0, v0, jd0, epochs, frame, center,
+                                                              False, ng)
+                ctx.save_for_backward(stm)
+            else:
+                states, st, ck = propagate_n_body_checkpointed(p0, v0, jd0, epochs, frame, center,
+                                                               False, ng)
+                ctx.ck = ck
             ctx.status = st
-            return states[:, 0:3, :].clone()
+            return states
 
         @staticmethod
-        def backward(ctx, grad_pos):
-            (stm,) = ctx.saved_tensors
-            # d loss / d p = sum_k sum_c grad_pos[k, c] * dpos_c/dp
-            g = torch.einsum("kcn,kcpn->pn", grad_pos, stm[:, 0:3, :, :])
-            return g[0:3], g[3:6], g[6], g[7], None, None, None, None, None
+        def backward(ctx, grad_states):
+            if ctx.method == "stm":
+                (stm,) = ctx.saved_tensors
+                # d loss / d p = sum_k sum_c grad[k, c] * d state_c / d p
+                g = torch.einsum("kcn,kcpn->pn", grad_states, stm)
+            else:
+                g, _ = propagate_n_body_adjoint(ctx.ck, grad_states)
+            return g[0:3], g[3:6], g[6], g[7], None, None, None, None, None, None
 
-    return NBodyPositions
+    return NBodyStates
 
 
 _NBody = None
 
 
-def nbody_positions(pos0, vel0, a1, a2, jd0, epochs, nongrav_rest=None, frame=Frames.Ecliptic,
-                    center=10):
-    """Differentiable predicted positions (K, 3, n) (torch CUDA tensors in and out).
+def nbody_states(pos0, vel0, a1, a2, jd0, epochs, nongrav_rest=None, frame=Frames.Ecliptic,
+                 center=10, method="adjoint"):
+    """Differentiable predicted states (K, 6, n) (torch CUDA tensors in and out).
 
     nongrav_rest: (10, n) rows supplying the comet model's other terms (kind, A3, alpha, r0,
-    m, n, k, dt); defaults to the JPL comet defaults (nongrav.rs:97-109)."""
+    m, n, k, dt = 0); defaults to the JPL comet defaults (nongrav.rs:97-109).  method:
+    "adjoint" (reverse mode, checkpointed) or "stm" (forward sensitivities)."""
     global _NBody
     import torch
 
+    if method not in ("adjoint", "stm"):
+        raise ValueError("method must be 'adjoint' or 'stm'")
     if _NBody is None:
         _NBody = _torch_function()
     n = pos0.shape[1]
@@ -107,7 +220,15 @@ def nbody_positions(pos0, vel0, a1, a2, jd0, epochs, nongrav_rest=None, frame=Fr
         base = torch.tensor([1.0, 0.0, 0.0, 0.0, 0.1112620426, 2.808, 2.15, 5.093, 4.6142, 0.0],
                             dtype=torch.float64, device=pos0.device)
         nongrav_rest = base[:, None].expand(10, n).contiguous()
-    return _NBody.apply(pos0, vel0, a1, a2, jd0, epochs, int(frame), int(center), nongrav_rest)
+    return _NBody.apply(pos0, vel0, a1, a2, jd0, epochs, int(frame), int(center), nongrav_rest,
+                        method)
+
+
+def nbody_positions(pos0, vel0, a1, a2, jd0, epochs, nongrav_rest=None, frame=Frames.Ecliptic,
+                    center=10, method="adjoint"):
+    """Differentiable predicted positions (K, 3, n); see ``nbody_states``."""
+    return nbody_states(pos0, vel0, a1, a2, jd0, epochs, nongrav_rest, frame, center,
+                        method)[:, 0:3, :]
 
 
 def radec(vec_eq):

@@ -376,6 +376,20 @@ static int ensure_tables(DevState& ds) {
         t.inv_frac[j] = 1.0 / sp[j];
         for (int z = 1; z < j; ++z) t.inv_diff[j][z] = 1.0 / (sp[j] - sp[z]);
     }
+    // the corrector's map from node evaluations to b, b = P (E - a), column by column
+    for (int col = 0; col < 7; ++col) {
+        double g[7];
+        for (int j = 1; j < 8; ++j) {
+            double gk = (j - 1 == col ? 1.0 : 0.0) * t.inv_frac[j];
+            for (int z = 1; z < j; ++z) gk = (gk - g[z - 1]) * t.inv_diff[j][z];
+            g[j - 1] = gk;
+        }
+        for (int jj = 0; jj < 7; ++jj) {
+            double s2 = g[jj];
+            for (int k = jj + 1; k < 7; ++k) s2 += t.c[k][jj] * g[k];
+            t.adj_p[jj][col] = s2;
+        }
+    }
     int rc = upload_tables(t);
     if (rc) return rc;
     // DEFAULT_SHAPE: 2048-facet Fibonacci lattice, total area 1 (flux/shapes.rs:9, 42-66)
@@ -861,6 +875,102 @@ int kete_b200_propagate_n_body_stm(int64_t n, const double* pos, const double* v
     a.max_loops = 1 << 20;
     if (S.rc) return S.rc;
     if ((rc = launch_nbody_stm(a, st))) return rc;
+    return S.finish();
+}
+
+int kete_b200_propagate_n_body_checkpointed(int64_t n, const double* pos, const double* vel,
+                                             const double* jd0, int n_epochs, const double* epochs,
+                                             int frame, int64_t center, int include_asteroids,
+                                             const double* nongrav, double* out_state,
+                                             int32_t* status, int ckpt_capacity,
+                                             double* checkpoints, int32_t* ckpt_count,
+                                             int32_t* ckpt_segment, int on_device, void* stream) {
+    if (n < 0 || n_epochs < 1 || !epochs || ckpt_capacity < 1)
+        return set_error(KETE_B200_E_ARGUMENT, "need n >= 0, at least one epoch and a checkpoint capacity >= 1");
+    if (n > 0 && (!pos || !vel || !jd0 || !out_state || !status || !checkpoints || !ckpt_count ||
+                  !ckpt_segment))
+        return set_error(KETE_B200_E_ARGUMENT, "null array");
+    std::lock_guard<std::mutex> lk(g_mu);
+    int rc = check_frame(frame);
+    if (rc) return rc;
+    if (!g_eph.loaded) return set_error(KETE_B200_E_NO_EPHEMERIS, "no SPK loaded");
+    const int n_force = include_asteroids ? g_eph.n_force_all : g_eph.n_force_planets;
+    if (n_force == 0) return set_error(KETE_B200_E_NO_EPHEMERIS, "loaded SPKs lack a perturber");
+    SensArgs a;
+    std::memset(&a, 0, sizeof a);
+    if ((rc = center_chain(center, a.chain))) return rc;
+    DevState* ds;
+    if ((rc = ensure_device(ds))) return rc;
+    if (n == 0) return 0;
+    cudaStream_t st = (cudaStream_t)stream;
+    Stager S{*ds, st, on_device};
+    a.n = n;
+    a.pos = S.in(pos, 3 * (size_t)n);
+    a.vel = S.in(vel, 3 * (size_t)n);
+    a.jd0 = S.in(jd0, (size_t)n);
+    a.n_epochs = n_epochs;
+    a.epochs = S.in(epochs, (size_t)n_epochs);
+    a.nongrav = S.in(nongrav, 10 * (size_t)n);
+    a.frame = frame;
+    a.n_force = n_force;
+    a.out_state = S.out(out_state, (size_t)n_epochs * 6 * n);
+    a.status = S.out(status, (size_t)n);
+    a.ckpt_cap = ckpt_capacity;
+    a.ckpt = S.out(checkpoints, (size_t)n * ckpt_capacity * SENS_STRIDE);
+    a.ckpt_count = S.out(ckpt_count, (size_t)n);
+    a.ckpt_seg = S.out(ckpt_segment, (size_t)n_epochs * n);
+    a.max_loops = 1 << 20;
+    if (S.rc) return S.rc;
+    if ((rc = launch_sens_forward(a, st))) return rc;
+    return S.finish();
+}
+
+int kete_b200_propagate_n_body_adjoint(int64_t n, int n_epochs, const double* epochs, int frame,
+                                       int include_asteroids, const double* nongrav,
+                                       int ckpt_capacity, const double* checkpoints,
+                                       const int32_t* ckpt_count, const int32_t* ckpt_segment,
+                                       const int32_t* status, const double* seed,
+                                       double* out_grad, int32_t* grad_status, int on_device,
+                                       void* stream) {
+    if (n < 0 || n_epochs < 1 || !epochs || ckpt_capacity < 1)
+        return set_error(KETE_B200_E_ARGUMENT, "need n >= 0, at least one epoch and a checkpoint capacity >= 1");
+    if (n > 0 && (!checkpoints || !ckpt_count || !ckpt_segment || !status || !seed || !out_grad))
+        return set_error(KETE_B200_E_ARGUMENT, "null array");
+    std::lock_guard<std::mutex> lk(g_mu);
+    int rc = check_frame(frame);
+    if (rc) return rc;
+    if (!g_eph.loaded) return set_error(KETE_B200_E_NO_EPHEMERIS, "no SPK loaded");
+    const int n_force = include_asteroids ? g_eph.n_force_all : g_eph.n_force_planets;
+    if (n_force == 0) return set_error(KETE_B200_E_NO_EPHEMERIS, "loaded SPKs lack a perturber");
+    SensArgs a;
+    std::memset(&a, 0, sizeof a);
+    DevState* ds;
+    if ((rc = ensure_device(ds))) return rc;
+    if (n == 0) return 0;
+    cudaStream_t st = (cudaStream_t)stream;
+    Stager S{*ds, st, on_device};
+    a.n = n;
+    a.n_epochs = n_epochs;
+    a.epochs = S.in(epochs, (size_t)n_epochs);
+    a.nongrav = S.in(nongrav, 10 * (size_t)n);
+    a.frame = frame;
+    a.n_force = n_force;
+    a.ckpt_cap = ckpt_capacity;
+    a.ckpt = const_cast<double*>(S.in(checkpoints, (size_t)n * ckpt_capacity * SENS_STRIDE));
+    a.ckpt_count = const_cast<int32_t*>(S.in(ckpt_count, (size_t)n));
+    a.ckpt_seg = const_cast<int32_t*>(S.in(ckpt_segment, (size_t)n_epochs * n));
+    a.status = const_cast<int32_t*>(S.in(status, (size_t)n));
+    a.seed = S.in(seed, (size_t)n_epochs * 6 * n);
+    a.out_grad = S.out(out_grad, 8 * (size_t)n);
+    a.grad_status = S.out(grad_status, (size_t)n);
+    a.max_loops = 1 << 20;
+    if (S.rc) return S.rc;
+    // per-object attempt records of the block being transposed (library scratch)
+    void* rec;
+    if ((rc = staging(*ds, 33, (size_t)n * (SENS_CK_ATTEMPTS + 1) * SENS_STRIDE * sizeof(double), &rec)))
+        return rc;
+    a.rec = (double*)rec;
+    if ((rc = launch_sens_backward(a, st))) return rc;
     return S.finish();
 }
 

@@ -17,6 +17,7 @@ enum Status : int32_t {
     ST_IO_ERROR = 5,
     ST_IMPACT = 6,
     ST_TIMEOUT = 7,  // a bounded device loop ran out of iterations
+    ST_CHECKPOINT_FULL = 8,  // more checkpoints were needed than the caller provided
 };
 
 enum Frame : int32_t { FRAME_EQUATORIAL = 1, FRAME_ECLIPTIC = 2 };
@@ -45,6 +46,7 @@ struct Tables {
     double frac2[8];        // spacing^2
     double inv_frac[8];     // 1 / spacing
     double inv_diff[8][8];  // 1 / (spacing[j] - spacing[z])
+    double adj_p[7][7];     // b = adj_p (E - a): divided differences, then C_MAT
 };
 
 // LLVM's constant-exponent powi: repeated squaring, reciprocal for negative exponents.

@@ -87,6 +87,35 @@ struct StmArgs {
 };
 int launch_nbody_stm(const StmArgs& a, cudaStream_t stream);
 
+// reverse-mode gradients: checkpointed forward pass and adjoint pass (adjoint.cuh)
+constexpr int SENS_STRIDE = 34;       // doubles per checkpoint / attempt record
+constexpr int SENS_CK_ATTEMPTS = 16;  // step attempts between checkpoints
+struct SensArgs {
+    int64_t n;
+    const double* pos;  // 3 x n (forward)
+    const double* vel;
+    const double* jd0;
+    int n_epochs;
+    const double* epochs;   // n_epochs
+    const double* nongrav;  // 10 x n or null
+    int frame;
+    CenterChain chain;
+    int n_force;
+    double* out_state;   // n_epochs x 6 x n (forward)
+    int32_t* status;     // n: written by the forward pass, read by the adjoint pass
+    double* ckpt;        // n x ckpt_cap x SENS_STRIDE
+    int ckpt_cap;
+    int32_t* ckpt_count; // n: checkpoints taken (may exceed ckpt_cap: ST_CHECKPOINT_FULL)
+    int32_t* ckpt_seg;   // n_epochs x n: first checkpoint of each epoch segment
+    const double* seed;  // n_epochs x 6 x n: dL/d(state at each epoch) (adjoint)
+    double* out_grad;    // 8 x n: dL/d(pos0, vel0, A1, A2) (adjoint)
+    int32_t* grad_status;  // n or null (adjoint)
+    double* rec;         // n x (SENS_CK_ATTEMPTS + 1) x SENS_STRIDE scratch (adjoint)
+    int max_loops;
+};
+int launch_sens_forward(const SensArgs& a, cudaStream_t stream);
+int launch_sens_backward(const SensArgs& a, cudaStream_t stream);
+
 struct NeatmArgs;
 struct FovArgs;
 int launch_fov_prefilter(const FovArgs& a, cudaStream_t stream);

@@ -696,6 +696,8 @@ __global__ void __launch_bounds__(64) nbody_stm_kernel(StmArgs a) {
     if (!(isfinite(x[0]) && isfinite(x[1]) && isfinite(x[2]) && isfinite(v[0]) && isfinite(v[1]) &&
           isfinite(v[2]) && isfinite(t)))
         rc = ST_VALUE_ERROR;
+    // the derivative of the comet model is taken with its time delay dt = 0
+    if (F.ng.kind == 1 && F.ng.p(9) != 0.0) rc = ST_VALUE_ERROR;
     if (rc == ST_OK) rc = to_ssb_equatorial(t, a.frame, a.chain, x, v);
     const double nan = __longlong_as_double(0x7ff8000000000000LL);
     for (int k = 0; k < a.n_epochs; ++k) {
@@ -728,6 +730,26 @@ int launch_nbody_stm(const StmArgs& a, cudaStream_t stream) {
     if (a.n <= 0) return 0;
     nbody_stm_kernel<<<(unsigned)((a.n + 63) / 64), 64, 0, stream>>>(a);
     return cuda_check(cudaGetLastError(), "nbody_stm_kernel launch");
+}
+
+}  // namespace kb
+
+#include "adjoint.cuh"
+
+namespace kb {
+
+int launch_sens_forward(const SensArgs& a, cudaStream_t stream) {
+    if (a.n <= 0) return 0;
+    const int64_t threads = a.n * SG;
+    nbody_sens_forward_kernel<1><<<(unsigned)((threads + SENS_BLOCK - 1) / SENS_BLOCK), SENS_BLOCK, 0, stream>>>(a);
+    return cuda_check(cudaGetLastError(), "nbody_sens_forward_kernel launch");
+}
+
+int launch_sens_backward(const SensArgs& a, cudaStream_t stream) {
+    if (a.n <= 0) return 0;
+    const int64_t threads = a.n * SG;
+    nbody_sens_backward_kernel<1><<<(unsigned)((threads + SENS_BLOCK - 1) / SENS_BLOCK), SENS_BLOCK, 0, stream>>>(a);
+    return cuda_check(cudaGetLastError(), "nbody_sens_backward_kernel launch");
 }
 
 }  // namespace kb

@@ -122,7 +122,8 @@ def test_stm_failure_is_nan(gpu):
     assert np.isfinite(s[:, :, 0]).all()
 
 
-def test_radec_loss_gradient_through_autograd(gpu):
+@pytest.mark.parametrize("method", ["adjoint", "stm"])
+def test_radec_loss_gradient_through_autograd(gpu, method):
     """d(RA/Dec residual loss)/d(pos0, vel0, A1, A2) from torch.autograd against
     Richardson-extrapolated differences of the loss (relative agreement 2e-5)."""
     import torch
@@ -142,7 +143,7 @@ def test_radec_loss_gradient_through_autograd(gpu):
 
     def loss_of(p0, v0, a1, a2):
         nonlocal ra_obs
-        pos_k = nbody_positions(p0, v0, a1, a2, jd0, epochs, nongrav_rest=rest)
+        pos_k = nbody_positions(p0, v0, a1, a2, jd0, epochs, nongrav_rest=rest, method=method)
         ra, dec = radec(ecliptic_to_equatorial_torch(pos_k - obs))
         if ra_obs is None:
             ra_obs = (ra + T(rng.normal(0, 1e-5, tuple(ra.shape)))).detach()
