@@ -48,6 +48,14 @@ def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
 
+# differentiation workload: NEOs with JPL comet A1/A2 over two years, 20 observation epochs
+ADJ_N, ADJ_EPOCHS, ADJ_SPAN = 4096, 20, 730.5
+ADJ_WORKLOAD = (f"differentiation: {ADJ_N} NEO states with JPL comet A1~N(0,1e-8), A2~N(0,1e-9), "
+                f"{ADJ_SPAN} d to {ADJ_EPOCHS} uniform epochs; observer on a 1 AU, e=0.0167 orbit; "
+                "loss = sum of squared RA/Dec residuals against perturbed truth orbits "
+                "(dr~N(0,1e-6 AU), dv~N(0,1e-8 AU/d)); gradient w.r.t. (pos0, vel0, A1, A2)")
+
+
 WORKLOADS = {
     "nbody_mba_10k": "plain N-body Radau, {n} main-belt states x 365.25 d per GPU, Sun+8 planets"
                      "+Moon from a synthetic SPK type-2 file (14-coef records)",
@@ -397,7 +405,105 @@ def run_gpu(args, world, rank, local):
     if nbody:
         line["object_steps_per_s"] = world * steps_total * args.steps / t_total
         line["corrector_iterations_per_step"] = iters_total / max(steps_total, 1)
+    if kind == "nbody_mba_10k" and not args.no_adjoint:
+        line["adjoint"] = adjoint_section(dev, max(1, args.warmup), max(1, min(args.steps, 3)))
     print(json.dumps(line), flush=True)
+
+
+def adjoint_population(n, seed=33):
+    """NEO states with comet A1/A2, their perturbed truth, the epochs and observer positions."""
+    from kete_b200 import synthetic
+
+    pos, vel = synthetic.neo(n, seed=seed)
+    rng = np.random.default_rng(seed + 1)
+    ng = np.repeat(synthetic.comet_nongrav(0.0, 0.0)[:, None], n, axis=1)
+    ng[1] = rng.normal(0.0, 1e-8, n)
+    ng[2] = rng.normal(0.0, 1e-9, n)
+    tpos = pos + rng.normal(0.0, 1e-6, (3, n))
+    tvel = vel + rng.normal(0.0, 1e-8, (3, n))
+    epochs = EPOCH + np.linspace(ADJ_SPAN / ADJ_EPOCHS, ADJ_SPAN, ADJ_EPOCHS)
+    obs, _ = synthetic.kepler_state(1.0, 0.0167, 0.0, 0.0, 1.7967, 0.0, EPOCH, epochs)
+    return pos, vel, np.ascontiguousarray(ng), tpos, tvel, epochs, np.ascontiguousarray(obs)
+
+
+def adjoint_section(dev, warmup, steps):
+    """Cost of the reverse-mode gradient beside one forward pass on the differentiation
+    workload, and its agreement with the transposed forward sensitivities."""
+    import torch
+
+    from kete_b200 import autodiff as A
+    from kete_b200 import propagate_n_body_arrays, tune
+
+    pos, vel, ng, tpos, tvel, epochs, obs = adjoint_population(ADJ_N)
+    n, K = ADJ_N, ADJ_EPOCHS
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    P, V, G, E = T(pos), T(vel), T(ng), T(epochs)
+    O = T(obs.T)[:, :, None]  # observer (K, 3, 1)
+    jd0 = torch.full((n,), EPOCH, dtype=torch.float64, device=dev)
+    ts, tst, _ = A.propagate_n_body_checkpointed(T(tpos), T(tvel), jd0, E, nongrav=G)
+    ra_t, dec_t = A.radec(A.ecliptic_to_equatorial_torch(ts[:, 0:3] - O))
+
+    def seed_of(states):
+        s = states.detach().clone().requires_grad_(True)
+        ra, dec = A.radec(A.ecliptic_to_equatorial_torch(s[:, 0:3] - O))
+        dra = torch.remainder(ra - ra_t + np.pi, 2 * np.pi) - np.pi
+        loss = (dra ** 2 + (dec - dec_t) ** 2).sum()
+        (g,) = torch.autograd.grad(loss, s)
+        return g.contiguous()
+
+    best, _ = tune.autotune(P, V, jd0, torch.full((n,), EPOCH + ADJ_SPAN, dtype=torch.float64,
+                                                  device=dev), nongrav=G)
+    jds = [torch.full((n,), float(e), dtype=torch.float64, device=dev) for e in epochs]
+
+    def forward():  # the product path: one propagate_n_body call per epoch
+        p, v, t0 = P, V, jd0
+        for k in range(K):
+            p, v, _ = propagate_n_body_arrays(p, v, t0, jds[k], nongrav=G, mode=best["mode"])
+            t0 = jds[k]
+        return p
+
+    states, st, ck = A.propagate_n_body_checkpointed(P, V, jd0, E, nongrav=G)
+    cap = ck.capacity
+    seed = seed_of(states)
+    g_adj, gst = A.propagate_n_body_adjoint(ck, seed)
+    _, stm, sst = A.propagate_n_body_stm_arrays(P, V, jd0, E, nongrav=G)
+    g_stm = torch.einsum("kcn,kcpn->pn", seed, stm)
+    ok = ((st == 0) & (gst == 0) & (sst == 0)).cpu().numpy()
+    rel = {}
+    for name, rows in (("pos0", slice(0, 3)), ("vel0", slice(3, 6)), ("A1", slice(6, 7)),
+                       ("A2", slice(7, 8))):
+        a_, b_ = g_adj[rows].cpu().numpy()[:, ok], g_stm[rows].cpu().numpy()[:, ok]
+        rel[name] = float((np.abs(a_ - b_).max(axis=0) / np.abs(b_).max(axis=0)).max())
+
+    def timed(fn):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    fwd_ms = timed(forward)
+    ck_ms = timed(lambda: A.propagate_n_body_checkpointed(P, V, jd0, E, nongrav=G, capacity=cap))
+    adj_ms = timed(lambda: A.propagate_n_body_adjoint(ck, seed))
+    stm_ms = timed(lambda: A.propagate_n_body_stm_arrays(P, V, jd0, E, nongrav=G))
+    return {
+        "workload": ADJ_WORKLOAD,
+        "forward_ms": fwd_ms, "forward_launch": best,
+        "checkpointed_forward_ms": ck_ms, "adjoint_ms": adj_ms,
+        "adjoint_over_forward": adj_ms / fwd_ms,
+        "adjoint_over_checkpointed_forward": adj_ms / ck_ms,
+        "checkpointed_forward_plus_adjoint_over_forward": (ck_ms + adj_ms) / fwd_ms,
+        "stm_ms": stm_ms, "stm_over_forward": stm_ms / fwd_ms,
+        "checkpoints_per_object": cap, "objects_ok": int(ok.sum()),
+        "adjoint_vs_transposed_stm_max_rel_err": rel,
+        "note": "forward = one node-kernel propagate_n_body call per epoch (autotuned); "
+                "adjoint = kete_b200_propagate_n_body_adjoint given dL/d(states)",
+    }
 
 
 def ctypes_probe(_lib):
@@ -422,6 +528,8 @@ def main():
     ap.add_argument("--mode", type=int, default=0, help="0 = autotune, 1 = thread, 2 = nodes")
     ap.add_argument("--variant", type=int, default=0)
     ap.add_argument("--refill", type=int, default=0)
+    ap.add_argument("--no-adjoint", action="store_true",
+                    help="skip the gradient-cost measurement on the differentiation workload")
     args = ap.parse_args()
     world, rank, local = dist_setup() if args.impl == "kete_b200" else (
         int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0)
