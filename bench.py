@@ -36,10 +36,13 @@ UNIT = "object-years/s"
 EPOCH = 2460000.5
 SPAN = 365.25
 
-# algorithmic FP64 flops (add/sub/mul = 1, fma = 2, div = 1, sqrt = 1) of the kernel's
-# arithmetic, derived term by term from the force model and the Radau step for the
-# PLANETS force list with 14-coefficient Chebyshev records.
-FLOPS_PER_EVAL = 2867      # 11 Chebyshev records (223 each) + 10 bodies + GR/J2 terms
+# algorithmic FP64 flops (add/sub/mul = 1, fma = 2, div = 1, sqrt = 1) the force model and
+# the Radau step need, term by term, for the PLANETS force list with 14-coefficient Chebyshev
+# records: positions and velocities of the Sun and Jupiter (2 x 223: their velocities enter
+# the relativistic and non-gravitational terms), positions of the other 9 records (9 x 108),
+# Earth/Moon + barycentre (6), 10 Newtonian terms (10 x 19) with 2 relative velocities (6),
+# relativistic terms (2 x 34), solar/Jovian J2 (2 x 42), Earth J2 (30).
+FLOPS_PER_EVAL = 1802
 FLOPS_PER_ITER = 7 * FLOPS_PER_EVAL + 1201  # 7 node evaluations + predictor/g/b/test
 FLOPS_PER_STEP = 120       # state update + step-size control
 

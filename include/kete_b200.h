@@ -37,6 +37,9 @@ extern "C" {
 #define KETE_B200_TIMEOUT 7
 #define KETE_B200_CHECKPOINT_FULL 8  /* checkpoint capacity too small; ckpt_count says how many */
 
+/* doubles per checkpoint of kete_b200_propagate_n_body_checkpointed */
+#define KETE_B200_CHECKPOINT_DOUBLES 36
+
 /* call return codes */
 #define KETE_B200_E_ARGUMENT (-1)
 #define KETE_B200_E_CUDA (-2)
@@ -131,8 +134,9 @@ int kete_b200_propagate_n_body_stm(int64_t n, const double* pos, const double* v
  * kete_b200_propagate_n_body_checkpointed: the forward pass.  Same integration and outputs
  * (out_state: n_epochs x 6 x n, status: n) as kete_b200_propagate_n_body_stm without the
  * matrices.  Before every 16th step attempt of each epoch segment it stores a checkpoint
- * (34 doubles: t, h, failures, x, v, a and the Radau b) in `checkpoints`
- * (n x ckpt_capacity x 34 doubles); ckpt_count (n) receives how many were taken and
+ * (KETE_B200_CHECKPOINT_DOUBLES doubles: t, h, failures, x, v, a, the Radau b and the
+ * predictor's previous step) in `checkpoints` (n x ckpt_capacity x
+ * KETE_B200_CHECKPOINT_DOUBLES doubles); ckpt_count (n) receives how many were taken and
  * ckpt_segment (n_epochs x n) the first checkpoint of each segment.  An object that needs
  * more than ckpt_capacity gets status KETE_B200_CHECKPOINT_FULL (its states are still
  * valid): call again with ckpt_capacity >= max(ckpt_count).  Non-gravitational models must
@@ -145,6 +149,8 @@ int kete_b200_propagate_n_body_stm(int64_t n, const double* pos, const double* v
  * block from the checkpoints.  Objects whose forward status is not OK get NaN; grad_status
  * (n, may be NULL) reports failures of the adjoint pass itself.  epochs, frame,
  * include_asteroids and nongrav must be those of the forward pass. */
+/* KETE_B200_CHECKPOINT_DOUBLES, for callers that cannot read the macro. */
+int kete_b200_checkpoint_doubles(void);
 int kete_b200_propagate_n_body_checkpointed(int64_t n, const double* pos, const double* vel,
                                             const double* jd0, int n_epochs, const double* epochs,
                                             int frame, int64_t center, int include_asteroids,

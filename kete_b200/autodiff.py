@@ -26,8 +26,12 @@ from .state import Frames
 
 
 CHECKPOINT_FULL = 8
-SENS_STRIDE = 34
 SENS_CK_ATTEMPTS = 16
+
+
+def checkpoint_doubles() -> int:
+    """Doubles per checkpoint, as the library lays them out."""
+    return int(_lib.lib().kete_b200_checkpoint_doubles())
 
 
 def _bind():
@@ -111,16 +115,17 @@ def propagate_n_body_checkpointed(pos, vel, jd0, epochs, frame=Frames.Ecliptic, 
         epochs = np.ascontiguousarray(np.atleast_1d(np.asarray(epochs, np.float64)))
         K = int(epochs.size)
     cap = int(capacity or _default_capacity(jd0, epochs))
+    stride = checkpoint_doubles()
     for _ in range(2):
         if dev:
             states = torch.empty((K, 6, n), dtype=torch.float64, device=pos.device)
             st = torch.empty(n, dtype=torch.int32, device=pos.device)
-            ck = torch.empty((n, cap, SENS_STRIDE), dtype=torch.float64, device=pos.device)
+            ck = torch.empty((n, cap, stride), dtype=torch.float64, device=pos.device)
             cnt = torch.empty(n, dtype=torch.int32, device=pos.device)
             seg = torch.empty((K, n), dtype=torch.int32, device=pos.device)
         else:
             states, st = np.empty((K, 6, n)), np.empty(n, dtype=np.int32)
-            ck = np.empty((n, cap, SENS_STRIDE))
+            ck = np.empty((n, cap, stride))
             cnt, seg = np.empty(n, dtype=np.int32), np.empty((K, n), dtype=np.int32)
         a = _lib.Args()
         args = [a.ptr(pos), a.ptr(vel), a.ptr(jd0), K, a.ptr(epochs), int(frame), int(center),
@@ -141,6 +146,14 @@ def propagate_n_body_adjoint(ck: Checkpoints, seed):
     L = _bind()
     n = ck.n
     K = int(ck.epochs.shape[0])
+    # the library reads these extents through raw pointers: check them here
+    if tuple(ck.ckpt.shape) != (n, ck.capacity, checkpoint_doubles()):
+        raise ValueError("checkpoint array does not match its capacity")
+    if tuple(seed.shape) != (K, 6, n):
+        raise ValueError(f"seed must have shape ({K}, 6, {n})")
+    if (tuple(ck.count.shape) != (n,) or tuple(ck.segment.shape) != (K, n)
+            or tuple(ck.status.shape) != (n,)):
+        raise ValueError("checkpoint bookkeeping arrays do not match")
     if _lib._is_torch_cuda(ck.ckpt):
         import torch
 

@@ -6,8 +6,9 @@
 // at the updated state in a round of its own, radau.rs:331-338) through n_epochs epochs.
 // Each epoch is a fresh integration from the previous one, as consecutive
 // propagate_n_body_spk calls are (kete_core/propagation/mod.rs:70-118).  Before every 16th
-// step attempt of an epoch segment the group stores a checkpoint: t, h, failures, x, v, a
-// and the b carried into the attempt (radau.rs:231-344 carries b unscaled between steps).
+// step attempt of an epoch segment the group stores a checkpoint: t, h, failures, x, v, a,
+// the b carried into the attempt and, after an accepted step, the step size the predicted
+// b is scaled from (predict_b_row, radau.cuh).
 //
 // Backward (nbody_sens_backward_kernel): the segments and their checkpoint blocks are taken
 // in reverse.  A block is re-run from its checkpoint with the same step code, recording for
@@ -16,6 +17,8 @@
 // with M iterations (step size and iteration count held fixed):
 //   x' = x + h v + h^2 (a/2 + W.b^M),  v' = v + h (a + U.b^M),  a' = F(x', v')
 //   b^m = P (E^m - a),  E^m_j = F(X_j(b^(m-1)), V_j(b^(m-1))),  P = C_MAT . (divided differences)
+//   b^0 = S(q) b^M of the previous attempt (the predictor, q = h / h_prev; identity after a
+//   failed attempt, zero at the start of a segment)
 //   X_j = x + f_j h v + f_j^2 h^2 (a/2 + W_j.b),  V_j = v + f_j h (a + U_j.b)
 // The adjoint runs the M iterations backwards with each node's Jacobian taken at the points
 // of the attempt's last iteration (the corrector has converged there to 1e-14 of |a| in
@@ -38,12 +41,15 @@ enum SensPhase : int { SP_BEGIN = 0, SP_EXACT_INIT = 1, SP_ITER = 2, SP_EXACT_ST
 // Checkpoint and attempt-record layout (SENS_STRIDE doubles each):
 //   [0] t  [1] h (checkpoint: proposed; record: used)  [2] failures / iterations
 //   [3] record: 1 if the attempt converged  [4..6] x  [7..9] v  [10..12] a  [13..33] b
-static_assert(SENS_STRIDE == 34, "checkpoint layout");
+//   [34] checkpoint: the previous step's h when b is to be predicted, else 0;
+//        record: the predictor's scale q used at the attempt's start, else 0
+static_assert(SENS_STRIDE == 36, "checkpoint layout");
 
 struct SensGroup {  // one object's integration state, identical in every lane of its group
-    double t, tf, h, next_h;
+    double t, tf, h, next_h, h_prev;
     double x[3], v[3], acc[3];
     int iter, failures, phase, att, rc;
+    bool predict;  // the next attempt starts from the predicted b
 };
 
 __device__ __forceinline__ double group_sum(double v, unsigned gmask) {
@@ -60,6 +66,7 @@ __device__ __forceinline__ void sens_store_state(double* dst, const SensGroup& G
         dst[0] = G.t;
         dst[1] = G.h;
         dst[2] = w2;
+        dst[34] = G.predict ? G.h_prev : 0.0;
     } else if (lane == 1) {
         dst[4] = G.x[0]; dst[5] = G.x[1]; dst[6] = G.x[2];
     } else if (lane == 2) {
@@ -91,6 +98,13 @@ __device__ __forceinline__ void sens_rounds(SensGroup& G, SpkForce& F, Policy& P
             }
             if (fabs(G.h) < 0.005) G.h = copysign(0.005, G.h);
             if (fabs(G.t - G.tf) <= fabs(G.h)) G.h = G.tf - G.t;
+            double q = 0.0;
+            if (G.predict) {
+                q = G.h / G.h_prev;
+                if (lane < 3) predict_b_row(sb + 7 * lane, q);
+                __syncwarp(gmask);
+            }
+            P.attempt_predict(q);
             G.iter = 0;
             G.att++;
             G.phase = SP_ITER;
@@ -149,8 +163,11 @@ __device__ __forceinline__ void sens_rounds(SensGroup& G, SpkForce& F, Policy& P
                 G.h = copysign(0.1, G.tf - G.t);
                 G.failures = 0;
                 G.att = 0;
+                G.predict = false;
             } else {
                 P.end_attempt(G, true);
+                G.h_prev = G.h;
+                G.predict = true;
                 G.h = G.next_h;
                 if (fabs(G.t - G.tf) < 1e-12) {
                     P.segment_end(G);
@@ -219,6 +236,7 @@ __device__ __forceinline__ void sens_rounds(SensGroup& G, SpkForce& F, Policy& P
         __syncwarp(gmask);
         if (G.iter >= 10) {  // not converged: retry with a smaller step (radau.rs:199-210)
             P.end_attempt(G, false);
+            G.predict = false;
             G.failures += 1;
             G.h *= 0.7;
             if (G.failures > 10) {
@@ -278,6 +296,7 @@ struct SensForwardPolicy {
         }
         return true;
     }
+    __device__ void attempt_predict(double) {}
     __device__ void iter_round(SensGroup&, double*, int) {}
     __device__ void end_attempt(SensGroup&, bool) {}
     __device__ void segment_end(SensGroup& G) {
@@ -338,7 +357,8 @@ __global__ void __launch_bounds__(SENS_BLOCK, MINB) nbody_sens_forward_kernel(Se
     G.tf = a.epochs[0];
     G.x[0] = a.pos[obj]; G.x[1] = a.pos[n + obj]; G.x[2] = a.pos[2 * n + obj];
     G.v[0] = a.vel[obj]; G.v[1] = a.vel[n + obj]; G.v[2] = a.vel[2 * n + obj];
-    G.h = G.next_h = 0.0;
+    G.h = G.next_h = G.h_prev = 0.0;
+    G.predict = false;
     G.acc[0] = G.acc[1] = G.acc[2] = 0.0;
     G.iter = G.failures = G.att = 0;
     G.rc = ST_OK;
@@ -395,6 +415,9 @@ struct SensReplayPolicy {
         if (na == SENS_CK_ATTEMPTS) return false;  // the block's end state is stored
         na++;
         return true;
+    }
+    __device__ void attempt_predict(double q) {
+        if (lane == 0) rec[(size_t)(na - 1) * SENS_STRIDE + 34] = q;
     }
     __device__ void iter_round(SensGroup&, double* b, int ln) {  // b of the previous iterate
         double* d = rec + (size_t)(na - 1) * SENS_STRIDE;
@@ -521,6 +544,8 @@ __global__ void __launch_bounds__(SENS_BLOCK, MINB) nbody_sens_backward_kernel(S
             G.failures = (int)c[2];
             G.tf = tf;
             G.next_h = 0.0;
+            G.h_prev = c[34];
+            G.predict = c[34] != 0.0;
 #pragma unroll
             for (int q = 0; q < 3; ++q) {
                 G.x[q] = c[4 + q];
@@ -679,6 +704,12 @@ __global__ void __launch_bounds__(SENS_BLOCK, MINB) nbody_sens_backward_kernel(S
                     lx[q] += group_sum(sx[q], gmask);
                     lv[q] += group_sum(sv[q], gmask);
                     la[q] += group_sum(sa[q], gmask);
+                }
+                // b^0 = S(q) b^M of the previous attempt when it was predicted
+                const double qs = r0[34];
+                if (qs != 0.0) {
+                    if (lane < 3) predict_b_row_transposed(slb + 7 * lane, qs);
+                    __syncwarp(gmask);
                 }
             }
         }

@@ -191,7 +191,6 @@ static void build_fast_plan(int n_force, FastPlan& P) {
     std::memset(&P, 0, sizeof P);
     if (n_force <= 0) return;
     int n = 0;
-    int current_parent = -1;
     double lo = -1e300, hi = 1e300;
     bool ok = true;
     auto add = [&](int slot, int role) {
@@ -208,7 +207,21 @@ static void build_fast_plan(int n_force, FastPlan& P) {
         P.role[n] = role;
         ++n;
     };
+    auto needs_velocity = [&](int b) {
+        const int k = g_eph.force[b].kind;
+        return k == FK_SUN || k == FK_JUPITER;
+    };
+    // bodies whose velocity enters the force, evaluated first (two at a time)
     for (int b = 0; b < n_force && ok; ++b) {
+        if (!needs_velocity(b)) continue;
+        if (g_eph.slot[g_eph.force[b].slot].parent_slot >= 0) ok = false;  // kept simple
+        add(g_eph.force[b].slot, b);
+    }
+    P.n_vel = n;
+    // the others in the reference's order, each centre before the first body chained to it
+    int current_parent = -1;
+    for (int b = 0; b < n_force && ok; ++b) {
+        if (needs_velocity(b)) continue;
         const int slot = g_eph.force[b].slot;
         const int parent = g_eph.slot[slot].parent_slot;
         if (parent >= 0 && parent != current_parent) {
@@ -217,6 +230,7 @@ static void build_fast_plan(int n_force, FastPlan& P) {
         }
         add(slot, b);
     }
+    while (ok && n > P.n_vel && (n - P.n_vel) % 3 != 0) add(g_eph.force[0].slot, -2);
     P.n_items = n;
     P.lo = lo;
     P.hi = hi;
@@ -390,6 +404,17 @@ static int ensure_tables(DevState& ds) {
             t.adj_p[jj][col] = s2;
         }
     }
+    // a(tau) = a0 + sum_k b_k tau^(k+1) over the previous step, re-expanded about its end
+    // with the new step's scale q: b'_m = q^(m+1) sum_{k>=m} C(k+1, m+1) b_k
+    for (int m = 0; m < 7; ++m)
+        for (int k = 0; k < 7; ++k) {
+            double cnk = 0.0;
+            if (k >= m) {
+                cnk = 1.0;
+                for (int i = 0; i < m + 1; ++i) cnk = cnk * (double)(k + 1 - i) / (double)(i + 1);
+            }
+            t.shift_c[m][k] = cnk;
+        }
     int rc = upload_tables(t);
     if (rc) return rc;
     // DEFAULT_SHAPE: 2048-facet Fibonacci lattice, total area 1 (flux/shapes.rs:9, 42-66)
@@ -877,6 +902,9 @@ int kete_b200_propagate_n_body_stm(int64_t n, const double* pos, const double* v
     if ((rc = launch_nbody_stm(a, st))) return rc;
     return S.finish();
 }
+
+static_assert(SENS_STRIDE == KETE_B200_CHECKPOINT_DOUBLES, "checkpoint size");
+int kete_b200_checkpoint_doubles(void) { return KETE_B200_CHECKPOINT_DOUBLES; }
 
 int kete_b200_propagate_n_body_checkpointed(int64_t n, const double* pos, const double* vel,
                                              const double* jd0, int n_epochs, const double* epochs,

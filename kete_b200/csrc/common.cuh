@@ -47,6 +47,7 @@ struct Tables {
     double inv_frac[8];     // 1 / spacing
     double inv_diff[8][8];  // 1 / (spacing[j] - spacing[z])
     double adj_p[7][7];     // b = adj_p (E - a): divided differences, then C_MAT
+    double shift_c[7][7];   // binomial C(k+1, m+1) at [m][k], k >= m: b carried to a new step
 };
 
 // LLVM's constant-exponent powi: repeated squaring, reciprocal for negative exponents.

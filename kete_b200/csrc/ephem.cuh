@@ -63,9 +63,15 @@ struct CenterChain {
 // it (role = -1).
 constexpr int FAST_NC = 14;
 constexpr int MAX_ITEMS = 24;
+// The first n_vel items are the bodies whose velocity enters the force (relativistic
+// correction of the Sun and Jupiter, non-gravitational term relative to the Sun): they are
+// evaluated two at a time with velocities.  The others (bodies whose position alone enters,
+// and centres) follow in the reference's order, three at a time, positions only; role -2
+// pads their count to a multiple of three.
 struct FastPlan {
     double lo, hi;
     int32_t n_items, ok;
+    int32_t n_vel, pad_;
     int32_t seg[MAX_ITEMS];
     int32_t role[MAX_ITEMS];
 };
@@ -201,6 +207,59 @@ __device__ __forceinline__ void cheb_pair(const double* __restrict__ ra, const d
     pb[0] = bvx * INV_AU_KM; pb[1] = bvy * INV_AU_KM; pb[2] = bvz * INV_AU_KM;
     va[0] = adx * ha1.y; va[1] = ady * ha1.y; va[2] = adz * ha1.y;
     vb[0] = bdx * hb1.y; vb[1] = bdy * hb1.y; vb[2] = bdz * hb1.y;
+}
+
+// Positions of three records evaluated in lockstep (value recurrence only), NC coefficients.
+template <int NC>
+__device__ __forceinline__ void cheb_pos3(const double* __restrict__ ra, const double* __restrict__ rb,
+                                          const double* __restrict__ rc, double jds, double pa[3],
+                                          double pb[3], double pc[3]) {
+    constexpr int NP = (NC + 1) & ~1;
+    const double* r[3] = {ra, rb, rc};
+    double xx[3], x2[3], t1[3], t2[3], acc[3][3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        const double2 h0 = __ldg(reinterpret_cast<const double2*>(r[q]));
+        const double2 h1 = __ldg(reinterpret_cast<const double2*>(r[q] + 2));
+        xx[q] = (jds - h0.x) * h1.x;
+        x2[q] = 2.0 * xx[q];
+        t2[q] = 1.0;
+        t1[q] = xx[q];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const double2 a = __ldg(reinterpret_cast<const double2*>(r[q] + 4 + c * NP));
+            acc[q][c] = a.x + a.y * xx[q];
+        }
+    }
+#pragma unroll
+    for (int k = 1; 2 * k < NC; ++k) {
+        double2 co[3][3];
+#pragma unroll
+        for (int q = 0; q < 3; ++q)
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+                co[q][c] = __ldg(reinterpret_cast<const double2*>(r[q] + 4 + c * NP) + k);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            if (2 * k + h < NC) {
+#pragma unroll
+                for (int q = 0; q < 3; ++q) {
+                    const double nt = x2[q] * t1[q] - t2[q];
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) acc[q][c] += (h ? co[q][c].y : co[q][c].x) * nt;
+                    t2[q] = t1[q];
+                    t1[q] = nt;
+                }
+            }
+        }
+    }
+    constexpr double INV_AU_KM = 1.0 / AU_KM;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        pa[c] = acc[0][c] * INV_AU_KM;
+        pb[c] = acc[1][c] * INV_AU_KM;
+        pc[c] = acc[2][c] * INV_AU_KM;
+    }
 }
 
 // Record of segment `seg` holding TDB seconds `jds` (index clamped to the segment).

@@ -185,12 +185,20 @@ struct SpkForce {
     int32_t min_id;
 
     // One body's contribution (GravParams::add_acceleration, gravity.rs:171-216, plus the
-    // non-gravitational term relative to the Sun, acceleration.rs:161-165).
+    // non-gravitational term relative to the Sun, acceleration.rs:161-165).  VEL = false
+    // serves the bodies whose velocity does not enter the force (no relativistic or
+    // non-gravitational term): bv is then not read.
+    template <bool VEL = true>
     __device__ __forceinline__ int body(const ForceEntry& fe, bool exact, const double x[3],
                                         const double v[3], const double bp[3], const double bv[3],
                                         double& acc0, double& acc1, double& acc2) {
         const double rp[3] = {x[0] - bp[0], x[1] - bp[1], x[2] - bp[2]};
-        const double rv[3] = {v[0] - bv[0], v[1] - bv[1], v[2] - bv[2]};
+        double rv[3] = {0.0, 0.0, 0.0};
+        if (VEL) {
+            rv[0] = v[0] - bv[0];
+            rv[1] = v[1] - bv[1];
+            rv[2] = v[2] - bv[2];
+        }
         const double r2 = rp[0] * rp[0] + rp[1] * rp[1] + rp[2] * rp[2];
         const double ir = rsqrt(r2);
         const double r = r2 * ir;
@@ -210,7 +218,7 @@ struct SpkForce {
         acc0 -= rp[0] * kk;
         acc1 -= rp[1] * kk;
         acc2 -= rp[2] * kk;
-        if (fe.kind == FK_SUN || fe.kind == FK_JUPITER) {
+        if (VEL && (fe.kind == FK_SUN || fe.kind == FK_JUPITER)) {
             // apply_gr_correction (gravity.rs:239-253)
             const double r_v = 4.0 * (rp[0] * rv[0] + rp[1] * rv[1] + rp[2] * rv[2]);
             const double rel_v2 = rv[0] * rv[0] + rv[1] * rv[1] + rv[2] * rv[2];
@@ -254,16 +262,19 @@ struct SpkForce {
     }
 
     // Fast path: the host-verified window where every body's first segment covers t and all
-    // records have FAST_NC coefficients.  Two records are evaluated per step.
+    // records have FAST_NC coefficients.  The Sun and Jupiter, whose velocities enter the
+    // force, are evaluated first, two records at a time with velocities; the other bodies
+    // (and the Earth-Moon barycentre they are chained through) follow in the reference's
+    // order, three records at a time, positions only.  The accelerations are therefore
+    // summed Sun, Jupiter, Mercury, Venus, Earth, Moon, Mars, Saturn, Uranus, Neptune.
     __device__ __forceinline__ int eval_fast(const FastPlan& P, bool exact, double t,
                                              const double x[3], const double v[3], double out[3]) {
         const double jds = __dmul_rn(t - 2451545.0, 86400.0);
         double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
-        double cp[3] = {0.0, 0.0, 0.0}, cv[3] = {0.0, 0.0, 0.0};
-        const int n_items = P.n_items;
+        const int n_vel = P.n_vel;
 #pragma unroll 1
-        for (int it = 0; it < n_items; it += 2) {
-            const bool has_b = it + 1 < n_items;
+        for (int it = 0; it < n_vel; it += 2) {
+            const bool has_b = it + 1 < n_vel;
             const int sa = P.seg[it];
             const int sb = has_b ? P.seg[it + 1] : sa;
             const double* ra = eph_record(c_eph, sa, jds);
@@ -273,20 +284,35 @@ struct SpkForce {
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 if (h == 1 && !has_b) break;
+                const ForceEntry fe = c_eph.force[P.role[it + h]];
+                const int rc = body<true>(fe, exact, x, v, h ? pb : pa, h ? vb : va, acc0, acc1, acc2);
+                if (rc != ST_OK) return rc;
+            }
+        }
+        double cp[3] = {0.0, 0.0, 0.0};
+        const double zero[3] = {0.0, 0.0, 0.0};
+        const int n_items = P.n_items;
+#pragma unroll 1
+        for (int it = n_vel; it < n_items; it += 3) {
+            const double* r0 = eph_record(c_eph, P.seg[it], jds);
+            const double* r1 = eph_record(c_eph, P.seg[it + 1], jds);
+            const double* r2 = eph_record(c_eph, P.seg[it + 2], jds);
+            double p3[3][3];
+            cheb_pos3<FAST_NC>(r0, r1, r2, jds, p3[0], p3[1], p3[2]);
+#pragma unroll
+            for (int h = 0; h < 3; ++h) {
                 const int role = P.role[it + h];
-                double* bp = h ? pb : pa;
-                double* bv = h ? vb : va;
-                if (role < 0) {
+                double* bp = p3[h];
+                if (role == -2) continue;  // padding
+                if (role < 0) {            // a centre kept for the bodies after it
                     cp[0] = bp[0]; cp[1] = bp[1]; cp[2] = bp[2];
-                    cv[0] = bv[0]; cv[1] = bv[1]; cv[2] = bv[2];
                     continue;
                 }
                 const ForceEntry fe = c_eph.force[role];
                 if (c_eph.slot[fe.slot].parent_slot >= 0) {
                     bp[0] += cp[0]; bp[1] += cp[1]; bp[2] += cp[2];
-                    bv[0] += cv[0]; bv[1] += cv[1]; bv[2] += cv[2];
                 }
-                const int rc = body(fe, exact, x, v, bp, bv, acc0, acc1, acc2);
+                const int rc = body<false>(fe, exact, x, v, bp, zero, acc0, acc1, acc2);
                 if (rc != ST_OK) return rc;
             }
         }

@@ -88,7 +88,7 @@ struct StmArgs {
 int launch_nbody_stm(const StmArgs& a, cudaStream_t stream);
 
 // reverse-mode gradients: checkpointed forward pass and adjoint pass (adjoint.cuh)
-constexpr int SENS_STRIDE = 34;       // doubles per checkpoint / attempt record
+constexpr int SENS_STRIDE = 36;       // doubles per checkpoint / attempt record
 constexpr int SENS_CK_ATTEMPTS = 16;  // step attempts between checkpoints
 struct SensArgs {
     int64_t n;

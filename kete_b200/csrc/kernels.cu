@@ -549,9 +549,23 @@ __device__ void radau_tangent_segment(TangentForce& F, double& t, double tf, dou
         return;
     }
     double h = copysign(0.1, tf - t);
+    double h_prev = 0.0;
+    bool predict = false;
     int failures = 0;
     for (int loop = 0; loop < max_loops; ++loop) {
         if (fabs(t - tf) <= fabs(h)) h = tf - t;
+        if (predict) {  // the predicted b (predict_b_row) and its tangent
+            const double q = h / h_prev;
+            for (int c = 0; c < 3; ++c) {
+                predict_b_row(b[c], q);
+                for (int p = 0; p < TAN_DIRS; ++p) {
+                    double row[7];
+                    for (int k = 0; k < 7; ++k) row[k] = db[c][k][p];
+                    predict_b_row(row, q);
+                    for (int k = 0; k < 7; ++k) db[c][k][p] = row[k];
+                }
+            }
+        }
         // ---- one step (radau.rs:225-346) with its tangent ----
         double g[3][7], dg[3][7][TAN_DIRS];
         double ev[3] = {a[0], a[1], a[2]};
@@ -646,6 +660,8 @@ __device__ void radau_tangent_segment(TangentForce& F, double& t, double tf, dou
             return;
         }
         if (converged) {
+            h_prev = h;
+            predict = true;
             h = next_h;
             if (fabs(t - tf) < 1e-12) {
                 rc_out = ST_OK;
@@ -654,6 +670,7 @@ __device__ void radau_tangent_segment(TangentForce& F, double& t, double tf, dou
             failures = 0;
         } else {
             rc = ST_OK;
+            predict = false;
             failures += 1;
             h *= 0.7;
             if (failures > 10) {

@@ -154,10 +154,16 @@ __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_nodes_kernel(NBodyArg
         phase = PH_DONE;
     };
 
-    // step start: |h| >= MIN_STEP, then truncate to the final time (radau.rs:187-190,214-216)
-    auto start_step = [&]() {
+    // step start: |h| >= MIN_STEP, then truncate to the final time (radau.rs:187-190,214-216);
+    // after an accepted step the corrector starts from the predicted b (predict_b_row)
+    double h_prev = 0.0;
+    auto start_step = [&](bool predict) {
         if (fabs(h) < 0.005) h = copysign(0.005, h);
         if (fabs(t - tf) <= fabs(h)) h = tf - t;
+        if (predict) {
+            if (lane < 3) predict_b_row(sb + 7 * lane, h / h_prev);
+            __syncwarp(gmask);
+        }
         iter = 0;
         phase = PH_ITER;
     };
@@ -234,16 +240,18 @@ __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_nodes_kernel(NBodyArg
                 }
                 h = copysign(0.1, tf - t);
                 failures = 0;
-            } else {
-                cnt.steps++;
-                h = next_h;
-                if (fabs(t - tf) < 1e-12) {
-                    finish(ST_OK);
-                    continue;
-                }
-                failures = 0;
+                start_step(false);
+                continue;
             }
-            start_step();
+            cnt.steps++;
+            h_prev = h;
+            h = next_h;
+            if (fabs(t - tf) < 1e-12) {
+                finish(ST_OK);
+                continue;
+            }
+            failures = 0;
+            start_step(true);
             continue;
         }
         // ---- corrector iteration: exchange the 7 node evaluations, form g and b ----
@@ -320,13 +328,14 @@ __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_nodes_kernel(NBodyArg
                 continue;
             }
             cnt.steps++;
+            h_prev = h;
             h = next_h;
             if (fabs(t - tf) < 1e-12) {
                 finish(ST_OK);
                 continue;
             }
             failures = 0;
-            start_step();
+            start_step(true);
             continue;
         }
         if (se_lane) {  // iteration not converged: forget the step-end lane's record
@@ -341,7 +350,7 @@ __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_nodes_kernel(NBodyArg
                 finish(ST_CONVERGENCE);
                 continue;
             }
-            start_step();
+            start_step(false);
         }
     }
 }
