@@ -65,8 +65,15 @@ WORKLOADS = {
     "nbody_mixed_1m": "batched uneven N-body, {n} states (90% main belt, 10% NEO, 5% JPL comet "
                       "non-grav A1~N(0,1e-8) A2~N(0,1e-9)), per-object target epochs U(+-5 yr)",
     "kepler_100k": "two-body Kepler, {n} main-belt states, per-object target epochs U(+-1000 d)",
+    "survey_10m": "survey chain, {n} states (90% main belt, 10% NEO, 5% comet non-grav), {f} "
+                  "rectangular 1.8x1.8 deg fields at ecliptic latitude U(-30,30) deg over one year, "
+                  "observer on a 1 AU e=0.0167 orbit; fov_state_check schedule (dt_limit 3 d) then "
+                  "H-G V and NEATM NEOS-band magnitudes per detection (H U(12,22), G 0.15, p_V "
+                  "lognormal median 0.14 sigma_ln 0.6, beaming 1.0, emissivity 0.9)",
 }
-DEFAULT_N = {"nbody_mba_10k": 10_000, "nbody_mixed_1m": 1_000_000, "kepler_100k": 100_000}
+DEFAULT_N = {"nbody_mba_10k": 10_000, "nbody_mixed_1m": 1_000_000, "kepler_100k": 100_000,
+             "survey_10m": 10_000_000}
+SURVEY_FIELDS, SURVEY_DT_LIMIT = 2000, 3.0
 
 
 def workload(n, seed=21, kind="nbody_mba_10k"):
@@ -217,11 +224,53 @@ def units_of(kind, jd0, jd1):
     return float(np.sum(np.abs(jd1 - jd0)) / 365.25), UNIT, METRIC
 
 
+def run_reference_survey(args):
+    """The survey chain on the CPU oracle, on the bounded seeded sample of the population."""
+    from kete_b200 import synthetic
+
+    n = args.n or DEFAULT_N["survey_10m"]
+    F = args.fields
+    pos, vel, ng, h, pv, table = survey_inputs(n, F, seed=41)
+    rng = np.random.default_rng(7)
+    idx = np.sort(rng.choice(n, size=min(n, args.cpu_sample), replace=False))
+    with tempfile.TemporaryDirectory() as td:
+        spk = synthetic.write_synthetic_spk(os.path.join(td, "syn.bsp"))
+        spk_bytes = open(spk, "rb").read()
+    w = idx[: min(200, len(idx))]
+    for _ in range(args.warmup):
+        survey_oracle(pos[:, w], vel[:, w], ng[:, w], table, spk_bytes, SURVEY_DT_LIMIT)
+    times = []
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        survey_oracle(pos[:, idx], vel[:, idx], ng[:, idx], table, spk_bytes, SURVEY_DT_LIMIT)
+        times.append(time.perf_counter() - t)
+    total = float(np.sum(times))
+    value = len(idx) * F * args.steps / total
+    line = {
+        "impl": "reference", "metric": "survey object-fields/s (fov_state_check + magnitudes)",
+        "value": value, "unit": "object-fields/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": WORKLOADS["survey_10m"].format(n=n, f=F), "n_objects": n},
+        "cpu_baseline": {"value": value, "unit": "object-fields/s", "cores": os.cpu_count(),
+                         "kind": "port",
+                         "sample": f"seeded {len(idx)}-object subsample per step (schedule and "
+                                   "field checks; magnitudes not included), oracle on all host "
+                                   "cores; the reference Rust/rayon path cannot be built"},
+        "e2e": {"value": value, "unit": "object-fields/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return
     from kete_b200 import synthetic
 
+    if args.workload == "survey_10m":
+        return run_reference_survey(args)
     kind = args.workload
     n = args.n or DEFAULT_N[kind]
     pos, vel, jd0, jd1, ng = workload(n, kind=kind)
@@ -509,6 +558,225 @@ def adjoint_section(dev, warmup, steps):
     }
 
 
+def survey_inputs(n, n_fields, seed=41):
+    """Population with H/G/albedo, and the time-sorted field table (19, F)."""
+    from kete_b200 import fov as fovmod
+    from kete_b200 import synthetic
+    from kete_b200.state import Frames, State
+
+    pos, vel, ng = synthetic.mixed(n, seed=seed)
+    rng = np.random.default_rng(seed + 1)
+    h = rng.uniform(12.0, 22.0, n)
+    pv = np.exp(np.log(0.14) + 0.6 * rng.normal(size=n))
+    frng = np.random.default_rng(seed + 2)
+    jds = np.sort(EPOCH + frng.uniform(0.0, 365.25, n_fields))
+    lat = np.radians(frng.uniform(-30.0, 30.0, n_fields))
+    lon = frng.uniform(0.0, 2 * np.pi, n_fields)
+    op, ov = synthetic.kepler_state(1.0, 0.0167, 0.0, 0.0, 1.7967, 0.0, EPOCH, jds)
+    cols = []
+    for k in range(n_fields):
+        pointing = [np.cos(lat[k]) * np.cos(lon[k]), np.cos(lat[k]) * np.sin(lon[k]), np.sin(lat[k])]
+        obs = State("observer", jds[k], op[:, k], ov[:, k], Frames.Ecliptic, 10)
+        cols.append(fovmod.RectangleFOV(pointing, 0.0, obs, 1.8, 1.8).ecliptic_column())
+    return pos, vel, ng, h, pv, np.ascontiguousarray(np.stack(cols, axis=1))
+
+
+def survey_magnitudes(ff, oo, ss, table, h, pv):
+    """H-G V magnitude and NEATM NEOS-band magnitudes of every detection (GPU kernels)."""
+    from kete_b200 import flux
+
+    m = len(oo)
+    if m == 0:
+        return np.empty(0), np.empty((2, 0))
+    sun2obj = np.ascontiguousarray(ss[1:4])
+    sun2obs = np.ascontiguousarray(table[1:4, ff])
+    hh, alb = h[oo], pv[oo]
+    v = flux.hg_apparent_mag_arrays(sun2obj, sun2obs, hh, np.full(m, 0.15))
+    diam = flux.C_V / np.sqrt(alb) * 10.0 ** (-0.2 * hh)
+    res = flux.neatm_arrays(sun2obj, sun2obs, hh, np.full(m, 0.15), diam, alb, np.ones(m),
+                            np.full(m, 0.9), np.array(flux.NEOS_BANDS), np.stack([alb, alb]),
+                            zero_mags=np.array(flux.NEOS_ZERO_MAG))
+    return v, res["magnitudes"]
+
+
+def survey_oracle(pos, vel, ng, table, spk_bytes, dt_limit):
+    """The fov_state_check schedule on the CPU oracle (all host cores): set of (field, obj)
+    and the oracle's state per pair."""
+    from kete_b200.fov import chunk_bounds
+    from oracle import oracle as O
+
+    O.spk_reset()
+    O.spk_load_bytes(spk_bytes)
+    n = pos.shape[1]
+    jds = table[0]
+
+    def prop(p, target):
+        op, ov, st, _, _ = O.propagate_n_body(p[0], p[1], np.full(n, p[3]), np.full(n, target),
+                                              ng=ng)
+        return [op, ov, p[2] & (st == 0), target]
+
+    cur_jd = big_jd = EPOCH
+    cur = [pos.copy(), vel.copy(), np.ones(n, bool), EPOCH]
+    big = [pos.copy(), vel.copy(), np.ones(n, bool), EPOCH]
+    found = {}
+    bounds = chunk_bounds(jds, dt_limit)
+    for k0, k1 in zip(bounds[:-1], bounds[1:]):
+        jd_mean = (jds[k1 - 1] + jds[k0]) / 2.0
+        if abs(jd_mean - big_jd) >= dt_limit * 50:
+            big_jd = jd_mean
+            big = prop(big, cur_jd)
+        if abs(jd_mean - cur_jd) >= dt_limit:
+            if abs(cur_jd - big_jd) >= dt_limit * 25:
+                cur = [big[0].copy(), big[1].copy(), big[2].copy(), big[3]]
+            cur_jd = jd_mean
+            cur = prop(cur, cur_jd)
+        idx = np.nonzero(cur[2])[0]
+        for k in range(k0, k1):
+            col = table[:, k]
+            flags, out7 = O.fov_check_visible(col[:7], col[7:19].reshape(4, 3), cur[0][:, idx],
+                                              cur[1][:, idx], np.full(idx.size, cur[3]), dt_limit)
+            for j in np.nonzero(flags)[0]:
+                found[(k, int(idx[j]))] = out7[:, j]
+    return found
+
+
+def run_survey(args, world, rank, local):
+    import torch
+
+    import kete_b200
+    from kete_b200 import build, synthetic
+    from kete_b200.fov import fov_state_check_arrays
+
+    build.build()
+    torch.cuda.set_device(local)
+    kete_b200.init(local)
+    td = tempfile.mkdtemp(prefix="kete_b200_bench_")
+    spk = synthetic.write_synthetic_spk(os.path.join(td, "syn.bsp"))
+    spk_bytes = open(spk, "rb").read()
+    kete_b200.spice.kernel_reload([spk])
+    n = args.n or DEFAULT_N["survey_10m"]
+    F = args.fields
+    pos, vel, ng, h, pv, table = survey_inputs(n, F, seed=41 + rank)
+    dev = torch.device("cuda", local)
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    P, V, G, TB = T(pos), T(vel), T(ng), T(table)
+    n_chunks = [0]
+
+    def chain(P_, V_):
+        n_chunks[0] = 0
+        ff, oo, ss = fov_state_check_arrays(P_, V_, EPOCH, TB, SURVEY_DT_LIMIT, False, G,
+                                            on_chunk=lambda a, b: n_chunks.__setitem__(0, n_chunks[0] + 1))
+        v, mags = survey_magnitudes(ff, oo, ss, table, h, pv)
+        return ff, oo, ss, v, mags
+
+    for _ in range(args.warmup):
+        chain(P, V)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        barrier(world)
+        t = time.perf_counter()
+        for _ in range(args.steps):
+            ff, oo, ss, vmag, bmag = chain(P, V)
+        torch.cuda.synchronize()
+        chain_s = reduce_max((time.perf_counter() - t) / args.steps, world)
+        barrier(world)
+    value = world * n * F / chain_s
+    # end to end: the population starts in pinned host memory
+    hp = {k: torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for k, a in
+          (("pos", pos), ("vel", vel), ("ng", ng), ("table", table))}
+    t = time.perf_counter()
+    P2, V2 = hp["pos"].to(dev, non_blocking=True), hp["vel"].to(dev, non_blocking=True)
+    G2, TB2 = hp["ng"].to(dev, non_blocking=True), hp["table"].to(dev, non_blocking=True)
+    G, TB = G2, TB2
+    chain(P2, V2)
+    torch.cuda.synchronize()
+    e2e_s = reduce_max(time.perf_counter() - t, world)
+
+    # FOV prefilter roofline on one chunk: algorithmic bytes = the population's states,
+    # epochs and flags read once (57 B per object) plus the field columns
+    from kete_b200.fov import chunk_bounds, fov_check_visible_arrays
+    b = chunk_bounds(table[0], SURVEY_DT_LIMIT)
+    sub = TB[:, b[0]:b[1]].contiguous()
+    # the schedule checks each chunk with the population at the chunk's mean epoch
+    jd_mean = 0.5 * (float(table[0, b[0]]) + float(table[0, b[1] - 1]))
+    jdv = torch.full((n,), jd_mean, dtype=torch.float64, device=dev)
+    okv = torch.ones(n, dtype=torch.uint8, device=dev)
+    fov_check_visible_arrays(P, V, jdv, okv, sub, SURVEY_DT_LIMIT)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    reps = 3
+    for _ in range(reps):
+        fov_check_visible_arrays(P, V, jdv, okv, sub, SURVEY_DT_LIMIT)
+    e1.record()
+    torch.cuda.synchronize()
+    fov_ms = e0.elapsed_time(e1) / reps
+    fov_bytes = n * 57 + sub.numel() * 8
+    peaks = measured_peaks()
+    if rank != 0:
+        return
+
+    # CPU oracle on a bounded seeded sample: its per-field lists must match the GPU's
+    rng = np.random.default_rng(7)
+    idx = np.sort(rng.choice(n, size=min(n, args.cpu_sample), replace=False))
+    t = time.perf_counter()
+    ref = survey_oracle(pos[:, idx], vel[:, idx], ng[:, idx], table, spk_bytes, SURVEY_DT_LIMIT)
+    cpu_s = time.perf_counter() - t
+    pos_of = {int(o): j for j, o in enumerate(idx)}
+    got = {}
+    for j in range(len(oo)):
+        o = int(oo[j])
+        if o in pos_of:
+            got[(int(ff[j]), pos_of[o])] = ss[:, j]
+    mism, edge_ok, max_err = 0, 0, 0.0
+    for key in set(ref) ^ set(got):
+        st = ref[key] if key in ref else got[key]
+        col = table[:, key[0]]
+        rel = st[1:4] - col[1:4]
+        rel = rel / np.linalg.norm(rel)
+        if np.min(np.abs(col[7:19].reshape(4, 3) @ rel)) < 1e-10:
+            edge_ok += 1
+        else:
+            mism += 1
+    for key in set(ref) & set(got):
+        max_err = max(max_err, float(np.abs(ref[key][1:4] - got[key][1:4]).max()))
+    line = {
+        "metric": "survey object-fields/s (fov_state_check + magnitudes)", "value": value,
+        "unit": "object-fields/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": chain_s * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOADS["survey_10m"].format(n=n, f=F), "n_objects_per_gpu": n,
+                   "n_fields": F, "chunks": n_chunks[0], "detections": int(len(oo)),
+                   "l2": "inputs (the population's states) larger than L2",
+                   "parallelism": f"replicas x{world} (objects independent)"},
+        "roofline": {"bound": "hbm", "kernel": "fov_prefilter_kernel (one chunk)",
+                     "achieved": fov_bytes / (fov_ms * 1e-3) / 1e9, "peak": peaks.get("hbm_gbs"),
+                     "unit": "GB/s",
+                     "frac": (fov_bytes / (fov_ms * 1e-3) / 1e9) / peaks["hbm_gbs"]
+                     if peaks.get("hbm_gbs") else None, "traffic": None,
+                     "chunk_ms": fov_ms, "bytes_algorithmic": fov_bytes,
+                     "note": "time of one chunk's fov_check_visible call (prefilter, n-body "
+                             "branch if any, result copy-back)"},
+        "cpu_baseline": {"value": len(idx) * F / cpu_s, "unit": "object-fields/s",
+                         "cores": os.cpu_count(), "kind": "port",
+                         "sample": f"seeded {len(idx)}-object subsample of the population, full "
+                                   "field list and schedule, oracle on all host cores"},
+        "e2e": {"value": world * n * F / e2e_s, "unit": "object-fields/s",
+                "h2d_bytes_per_step": int(pos.nbytes + vel.nbytes + ng.nbytes + table.nbytes),
+                "d2h_bytes_per_step": int(len(oo) * (4 + 4 + 56 + 8 + 16))},
+        "gpu_launches": None,
+        "clocks": clk.summary(),
+        "parity": {"sample_objects": int(len(idx)), "oracle_pairs": len(ref),
+                   "gpu_pairs_in_sample": len(got), "mismatches_off_edge": mism,
+                   "mismatches_within_1e-10_rad_of_edge": edge_ok,
+                   "max_state_err_au": max_err},
+        "magnitudes": {"v_median": float(np.nanmedian(vmag)) if len(vmag) else None,
+                       "neatm_band_mag_median": [float(np.nanmedian(x)) for x in bmag]
+                       if len(vmag) else None},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def ctypes_probe(_lib):
     import ctypes
 
@@ -531,6 +799,9 @@ def main():
     ap.add_argument("--mode", type=int, default=0, help="0 = autotune, 1 = thread, 2 = nodes")
     ap.add_argument("--variant", type=int, default=0)
     ap.add_argument("--refill", type=int, default=0)
+    ap.add_argument("--fields", type=int, default=SURVEY_FIELDS, help="survey workload: fields")
+    ap.add_argument("--cpu-sample", type=int, default=20000,
+                    help="survey workload: objects in the CPU oracle's sample")
     ap.add_argument("--no-adjoint", action="store_true",
                     help="skip the gradient-cost measurement on the differentiation workload")
     args = ap.parse_args()
@@ -538,6 +809,8 @@ def main():
         int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0)
     if args.impl == "reference":
         run_reference(args, world, rank)
+    elif args.workload == "survey_10m":
+        run_survey(args, world, rank, local)
     else:
         run_gpu(args, world, rank, local)
         if world > 1:

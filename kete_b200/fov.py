@@ -136,22 +136,82 @@ def fov_check_visible_arrays(pos, vel, jd, valid, fov_table, dt_limit=3.0,
     return out_f[order], out_o[order], out_s[:, order]
 
 
-def _chunks(fovs, dt_limit):
-    """Group fields (sorted by jd) into chunks spanning less than 2*dt_limit
-    (src/kete/rust/fovs/checks.rs:37-57)."""
-    chunks, chunk = [], []
-    for f in fovs:
-        if not chunk:
-            chunk.append(f)
-            continue
-        if abs(f.jd - chunk[0].jd) >= 2.0 * dt_limit:
-            chunks.append(chunk)
-            chunk = [f]
-        else:
-            chunk.append(f)
-    if chunk:
-        chunks.append(chunk)
-    return chunks
+def chunk_bounds(jds, dt_limit):
+    """Start indices of the chunks of time-sorted field epochs (checks.rs:37-57): a chunk
+    closes when the next field is 2*dt_limit or more after the chunk's first field."""
+    starts = []
+    first = None
+    for k, jd in enumerate(jds):
+        if first is None or abs(jd - first) >= 2.0 * dt_limit:
+            starts.append(k)
+            first = jd
+    return starts + [len(jds)]
+
+
+def fov_state_check_arrays(pos, vel, jd, fov_table, dt_limit=3.0, include_asteroids=False,
+                           nongrav=None, on_chunk=None):
+    """The fov_state_check schedule (src/kete/rust/fovs/checks.rs:24-110) on device arrays.
+
+    pos/vel (3, n) heliocentric ecliptic torch CUDA tensors at the common epoch ``jd``;
+    fov_table (19, F) columns sorted by observer epoch (row 0).  Chunks of fields shorter
+    than 2*dt_limit are checked against the population re-propagated (N-body) to the
+    chunk's mean epoch, re-seeded from a big-step copy every 25-50 dt_limit as the
+    reference does; objects whose propagation fails are dropped from then on.  Returns
+    (fov_index, obj_index, state7) numpy arrays over all fields, sorted by field then
+    object.  ``on_chunk(k0, k1)``, when given, is called after each chunk."""
+    import torch
+
+    n = int(pos.shape[1])
+    dev = pos.device
+    table = fov_table if _lib._is_torch_cuda(fov_table) else torch.as_tensor(
+        np.ascontiguousarray(fov_table), device=dev)
+    jds = table[0].cpu().numpy()
+    if np.any(np.diff(jds) < 0):
+        raise ValueError("fields must be sorted by epoch")
+
+    class Pop:
+        def __init__(self, P, V, ok, t):
+            self.P, self.V, self.ok, self.t = P, V, ok, t
+
+        def copy(self):
+            return Pop(self.P.clone(), self.V.clone(), self.ok.clone(), self.t)
+
+        def propagate(self, target):
+            jd0 = torch.full((n,), self.t, dtype=torch.float64, device=dev)
+            jd1 = torch.full((n,), target, dtype=torch.float64, device=dev)
+            P, V, st = propagate_n_body_arrays(self.P, self.V, jd0, jd1, Frames.Ecliptic, 10,
+                                               include_asteroids, nongrav)
+            self.P, self.V, self.t = P, V, target
+            self.ok = self.ok & (st == 0)
+
+    cur_jd = float(jd)
+    big_jd = cur_jd
+    cur = Pop(pos, vel, torch.ones(n, dtype=torch.bool, device=dev), cur_jd)
+    big = cur.copy()
+    out_f, out_o, out_s = [], [], []
+    bounds = chunk_bounds(jds, dt_limit)
+    for k0, k1 in zip(bounds[:-1], bounds[1:]):
+        jd_mean = (jds[k1 - 1] + jds[k0]) / 2.0
+        if abs(jd_mean - big_jd) >= dt_limit * 50.0:
+            big_jd = jd_mean
+            big.propagate(cur_jd)  # the reference propagates the big step to the current jd
+        if abs(jd_mean - cur_jd) >= dt_limit:
+            if abs(cur_jd - big_jd) >= dt_limit * 25.0:
+                cur = big.copy()
+            cur_jd = jd_mean
+            cur.propagate(cur_jd)
+        epochs = torch.full((n,), cur.t, dtype=torch.float64, device=dev)
+        ff, oo, ss = fov_check_visible_arrays(cur.P, cur.V, epochs, cur.ok.to(torch.uint8),
+                                              table[:, k0:k1].contiguous(), dt_limit,
+                                              include_asteroids)
+        out_f.append(ff + k0)
+        out_o.append(oo)
+        out_s.append(ss)
+        if on_chunk is not None:
+            on_chunk(k0, k1)
+    if not out_f:
+        return np.empty(0, np.int32), np.empty(0, np.int32), np.empty((7, 0))
+    return np.concatenate(out_f), np.concatenate(out_o), np.concatenate(out_s, axis=1)
 
 
 def fov_state_check(obj_state, fovs, dt_limit=3.0, include_asteroids=False):
@@ -175,46 +235,15 @@ def fov_state_check(obj_state, fovs, dt_limit=3.0, include_asteroids=False):
     desig = [s.desig for s in states]
     dev = torch.device("cuda", torch.cuda.current_device())
     T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
-
-    class Pop:
-        def __init__(self, P, V, ok, jd):
-            self.P, self.V, self.ok, self.jd = P, V, ok, jd
-
-        def copy(self):
-            return Pop(self.P.clone(), self.V.clone(), self.ok.clone(), self.jd)
-
-        def propagate(self, target):
-            jd0 = torch.full((n,), self.jd, dtype=torch.float64, device=dev)
-            jd1 = torch.full((n,), target, dtype=torch.float64, device=dev)
-            P, V, st = propagate_n_body_arrays(self.P, self.V, jd0, jd1, Frames.Ecliptic, 10,
-                                               include_asteroids)
-            self.P, self.V, self.jd = P, V, target
-            self.ok = self.ok & (st == 0)
-
-    jd = states[0].jd
-    big_jd = jd
-    cur = Pop(T(pos), T(vel), torch.ones(n, dtype=torch.bool, device=dev), jd)
-    big = cur.copy()
+    table = np.stack([f.ecliptic_column() for f in fovs], axis=1)
+    ff, oo, ss = fov_state_check_arrays(T(pos), T(vel), states[0].jd, table, dt_limit,
+                                        include_asteroids)
     results = []
-    for chunk in _chunks(fovs, dt_limit):
-        jd_mean = (chunk[-1].jd + chunk[0].jd) / 2.0
-        if abs(jd_mean - big_jd) >= dt_limit * 50.0:
-            big_jd = jd_mean
-            big.propagate(jd)  # the reference propagates the big step to the current jd
-        if abs(jd_mean - jd) >= dt_limit:
-            if abs(jd - big_jd) >= dt_limit * 25.0:
-                cur = big.copy()
-            jd = jd_mean
-            cur.propagate(jd)
-        table = T(np.stack([f.ecliptic_column() for f in chunk], axis=1))
-        jds = torch.full((n,), cur.jd, dtype=torch.float64, device=dev)
-        ff, oo, ss = fov_check_visible_arrays(cur.P, cur.V, jds, cur.ok.to(torch.uint8), table,
-                                              dt_limit, include_asteroids)
-        for k, f in enumerate(chunk):
-            sel = np.nonzero(ff == k)[0]
-            if sel.size == 0:
-                continue
-            vis = [State(desig[oo[j]], ss[0, j], ss[1:4, j], ss[4:7, j], Frames.Ecliptic, 10)
-                   for j in sel]
-            results.append(SimultaneousStates(vis, f))
+    for k, f in enumerate(fovs):
+        sel = np.nonzero(ff == k)[0]
+        if sel.size == 0:
+            continue
+        vis = [State(desig[oo[j]], ss[0, j], ss[1:4, j], ss[4:7, j], Frames.Ecliptic, 10)
+               for j in sel]
+        results.append(SimultaneousStates(vis, f))
     return results

@@ -55,3 +55,32 @@ def test_host_arrays_must_be_float64():
     # non-contiguous float64 inputs are copied, not rejected
     m = np.zeros((3, 8))[:, ::2]
     assert a.ptr(m) != 0 and a.keep[-1].flags.c_contiguous
+
+
+def test_fov_chunk_bounds():
+    """Chunks of time-sorted fields (src/kete/rust/fovs/checks.rs:37-57): a chunk closes when
+    a field is 2*dt_limit or more after the chunk's first field."""
+    from kete_b200.fov import chunk_bounds
+
+    assert chunk_bounds([], 3.0) == [0]
+    assert chunk_bounds([0.0], 3.0) == [0, 1]
+    assert chunk_bounds([0.0, 5.9, 6.0, 6.1, 11.99, 12.0], 3.0) == [0, 2, 5, 6]
+    jds = np.sort(np.random.default_rng(1).uniform(0, 365.25, 500))
+    b = chunk_bounds(jds, 3.0)
+    for k0, k1 in zip(b[:-1], b[1:]):
+        assert jds[k1 - 1] - jds[k0] < 6.0
+        if k1 < len(jds):
+            assert jds[k1] - jds[k0] >= 6.0
+
+
+def test_adjoint_wrapper_checks_shapes():
+    """The adjoint call refuses checkpoint or seed arrays whose extents do not match, before
+    any pointer reaches the library."""
+    import pytest
+
+    from kete_b200 import autodiff as A
+
+    ck = A.Checkpoints(4, np.zeros(3), 2, False, None, 5, np.zeros((4, 5, 7)),
+                       np.zeros(4, np.int32), np.zeros((3, 4), np.int32), np.zeros(4, np.int32))
+    with pytest.raises(ValueError):
+        A.propagate_n_body_adjoint(ck, np.zeros((3, 6, 4)))
