@@ -203,8 +203,21 @@ static void build_fast_plan(int n_force, FastPlan& P) {
         if (d.n_pad != FAST_NC) ok = false;
         lo = std::max(lo, d.jd_start);
         hi = std::min(hi, d.jd_end);
-        P.seg[n] = seg;
-        P.role[n] = role;
+        FastItem& I = P.item[n];
+        I.offset = d.offset;
+        I.start_s = d.start_s;
+        I.inv_intlen = d.inv_intlen;
+        I.n_rec = (double)d.n_rec;
+        I.rsize = d.rsize;
+        I.role = role;
+        if (role >= 0) {
+            const ForceEntry& fe = g_eph.force[role];
+            I.mass = fe.mass;
+            I.radius = fe.radius;
+            I.kind = fe.kind;
+            I.naif_id = fe.naif_id;
+            I.chained = g_eph.slot[slot].parent_slot >= 0 ? 1 : 0;
+        }
         ++n;
     };
     auto needs_velocity = [&](int b) {

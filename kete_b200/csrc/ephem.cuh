@@ -63,6 +63,21 @@ struct CenterChain {
 // it (role = -1).
 constexpr int FAST_NC = 14;
 constexpr int MAX_ITEMS = 24;
+// One item of the fast plan, holding everything its evaluation reads (its segment's record
+// table and, for a force body, the body's gravity parameters), so the force loop makes no
+// dependent table lookups.
+struct FastItem {
+    int64_t offset;                     // pool offset of the segment's record 0
+    double start_s, inv_intlen, n_rec;  // record = clamp(floor((t - start_s) * inv_intlen))
+    double mass, radius;
+    int32_t rsize;    // doubles per record
+    int32_t role;     // -2 padding, -1 a centre kept for later bodies, else the force index
+    int32_t kind;     // ForceKind of a force body
+    int32_t naif_id;
+    int32_t chained;  // 1: the body is centred on the kept centre (add its position)
+    int32_t pad_;
+};
+
 // The first n_vel items are the bodies whose velocity enters the force (relativistic
 // correction of the Sun and Jupiter, non-gravitational term relative to the Sun): they are
 // evaluated two at a time with velocities.  The others (bodies whose position alone enters,
@@ -72,8 +87,7 @@ struct FastPlan {
     double lo, hi;
     int32_t n_items, ok;
     int32_t n_vel, pad_;
-    int32_t seg[MAX_ITEMS];
-    int32_t role[MAX_ITEMS];
+    FastItem item[MAX_ITEMS];
 };
 
 struct EphemConst {
@@ -151,8 +165,10 @@ __device__ __forceinline__ void cheb_record(const double* __restrict__ rec, int 
 }
 
 // Position/velocity of two records evaluated in lockstep (two independent recurrence chains),
-// NC coefficients per coordinate, fully unrolled.
-template <int NC>
+// NC coefficients per coordinate.  KU: coefficient pairs per unrolled loop body (a small
+// body keeps the lane-parallel kernels' code in the instruction cache; the one-object-per-
+// thread kernel prefers the loop fully unrolled).
+template <int NC, int KU = NC>
 __device__ __forceinline__ void cheb_pair(const double* __restrict__ ra, const double* __restrict__ rb,
                                           double jds, double pa[3], double va[3], double pb[3],
                                           double vb[3]) {
@@ -177,7 +193,7 @@ __device__ __forceinline__ void cheb_pair(const double* __restrict__ ra, const d
     double bdx = bx.y, bdy = by.y, bdz = bz.y;
     double at2 = 1.0, at1 = xa, au2 = 1.0, au1 = xa2;
     double bt2 = 1.0, bt1 = xb, bu2 = 1.0, bu1 = xb2;
-#pragma unroll
+#pragma unroll KU
     for (int k = 1; 2 * k < NC; ++k) {
         ax = __ldg(cxa + k); ay = __ldg(cya + k); az = __ldg(cza + k);
         bx = __ldg(cxb + k); by = __ldg(cyb + k); bz = __ldg(czb + k);
@@ -209,8 +225,9 @@ __device__ __forceinline__ void cheb_pair(const double* __restrict__ ra, const d
     vb[0] = bdx * hb1.y; vb[1] = bdy * hb1.y; vb[2] = bdz * hb1.y;
 }
 
-// Positions of three records evaluated in lockstep (value recurrence only), NC coefficients.
-template <int NC>
+// Positions of three records evaluated in lockstep (value recurrence only), NC coefficients;
+// KU as for cheb_pair.
+template <int NC, int KU = NC>
 __device__ __forceinline__ void cheb_pos3(const double* __restrict__ ra, const double* __restrict__ rb,
                                           const double* __restrict__ rc, double jds, double pa[3],
                                           double pb[3], double pc[3]) {
@@ -231,7 +248,7 @@ __device__ __forceinline__ void cheb_pos3(const double* __restrict__ ra, const d
             acc[q][c] = a.x + a.y * xx[q];
         }
     }
-#pragma unroll
+#pragma unroll KU
     for (int k = 1; 2 * k < NC; ++k) {
         double2 co[3][3];
 #pragma unroll
@@ -260,6 +277,14 @@ __device__ __forceinline__ void cheb_pos3(const double* __restrict__ ra, const d
         pb[c] = acc[1][c] * INV_AU_KM;
         pc[c] = acc[2][c] * INV_AU_KM;
     }
+}
+
+// Record of a fast-plan item holding TDB seconds `jds` (index clamped to the segment).
+__device__ __forceinline__ const double* fast_record(const double* pool, const FastItem& I,
+                                                     double jds) {
+    const double fidx = floor((jds - I.start_s) * I.inv_intlen);
+    const int idx = fidx < 0.0 ? 0 : (fidx >= I.n_rec ? (int)I.n_rec - 1 : (int)fidx);
+    return pool + I.offset + (int64_t)idx * I.rsize;
 }
 
 // Record of segment `seg` holding TDB seconds `jds` (index clamped to the segment).

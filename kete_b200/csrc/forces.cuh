@@ -175,8 +175,10 @@ __device__ __forceinline__ int from_ssb_equatorial(double t, int frame, const Ce
     return ST_OK;
 }
 
-// Acceleration from the SPK perturbers (spk_accel, acceleration.rs:121-168).
-struct SpkForce {
+// Acceleration from the SPK perturbers (spk_accel, acceleration.rs:121-168).  KU: the
+// Chebyshev loops' unrolling (cheb_pair); SpkForce is the lane-parallel kernels' compact form.
+template <int KU>
+struct SpkForceT {
     int n_force;
     NonGrav ng;
     // outputs of exact evaluations
@@ -270,22 +272,26 @@ struct SpkForce {
     __device__ __forceinline__ int eval_fast(const FastPlan& P, bool exact, double t,
                                              const double x[3], const double v[3], double out[3]) {
         const double jds = __dmul_rn(t - 2451545.0, 86400.0);
+        const double* pool = c_eph.pool;
         double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
         const int n_vel = P.n_vel;
 #pragma unroll 1
         for (int it = 0; it < n_vel; it += 2) {
             const bool has_b = it + 1 < n_vel;
-            const int sa = P.seg[it];
-            const int sb = has_b ? P.seg[it + 1] : sa;
-            const double* ra = eph_record(c_eph, sa, jds);
-            const double* rb = eph_record(c_eph, sb, jds);
+            const FastItem& A = P.item[it];
+            const FastItem& B = P.item[has_b ? it + 1 : it];
+            const double* ra = fast_record(pool, A, jds);
+            const double* rb = fast_record(pool, B, jds);
             double pa[3], va[3], pb[3], vb[3];
-            cheb_pair<FAST_NC>(ra, rb, jds, pa, va, pb, vb);
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                if (h == 1 && !has_b) break;
-                const ForceEntry fe = c_eph.force[P.role[it + h]];
-                const int rc = body<true>(fe, exact, x, v, h ? pb : pa, h ? vb : va, acc0, acc1, acc2);
+            cheb_pair<FAST_NC, KU>(ra, rb, jds, pa, va, pb, vb);
+            {
+                const ForceEntry fe{A.mass, A.radius, 0, A.kind, A.naif_id, 0};
+                const int rc = body<true>(fe, exact, x, v, pa, va, acc0, acc1, acc2);
+                if (rc != ST_OK) return rc;
+            }
+            if (has_b) {
+                const ForceEntry fe{B.mass, B.radius, 0, B.kind, B.naif_id, 0};
+                const int rc = body<true>(fe, exact, x, v, pb, vb, acc0, acc1, acc2);
                 if (rc != ST_OK) return rc;
             }
         }
@@ -294,24 +300,24 @@ struct SpkForce {
         const int n_items = P.n_items;
 #pragma unroll 1
         for (int it = n_vel; it < n_items; it += 3) {
-            const double* r0 = eph_record(c_eph, P.seg[it], jds);
-            const double* r1 = eph_record(c_eph, P.seg[it + 1], jds);
-            const double* r2 = eph_record(c_eph, P.seg[it + 2], jds);
+            const double* r0 = fast_record(pool, P.item[it], jds);
+            const double* r1 = fast_record(pool, P.item[it + 1], jds);
+            const double* r2 = fast_record(pool, P.item[it + 2], jds);
             double p3[3][3];
-            cheb_pos3<FAST_NC>(r0, r1, r2, jds, p3[0], p3[1], p3[2]);
+            cheb_pos3<FAST_NC, KU>(r0, r1, r2, jds, p3[0], p3[1], p3[2]);
 #pragma unroll
             for (int h = 0; h < 3; ++h) {
-                const int role = P.role[it + h];
+                const FastItem& I = P.item[it + h];
                 double* bp = p3[h];
-                if (role == -2) continue;  // padding
-                if (role < 0) {            // a centre kept for the bodies after it
+                if (I.role == -2) continue;  // padding
+                if (I.role < 0) {            // a centre kept for the bodies after it
                     cp[0] = bp[0]; cp[1] = bp[1]; cp[2] = bp[2];
                     continue;
                 }
-                const ForceEntry fe = c_eph.force[role];
-                if (c_eph.slot[fe.slot].parent_slot >= 0) {
+                if (I.chained) {
                     bp[0] += cp[0]; bp[1] += cp[1]; bp[2] += cp[2];
                 }
+                const ForceEntry fe{I.mass, I.radius, 0, I.kind, I.naif_id, 0};
                 const int rc = body<false>(fe, exact, x, v, bp, zero, acc0, acc1, acc2);
                 if (rc != ST_OK) return rc;
             }
@@ -358,6 +364,9 @@ struct SpkForce {
         return ST_OK;
     }
 };
+
+using SpkForce = SpkForceT<1>;         // lane-parallel kernels: compact loops
+using SpkForceUnrolled = SpkForceT<FAST_NC>;  // one object per thread
 
 // central_accel (acceleration.rs:66-80): the Sun at the origin only.
 struct CentralForce {

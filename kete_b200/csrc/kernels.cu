@@ -81,7 +81,7 @@ __global__ void __launch_bounds__(128) nbody_thread_kernel(NBodyArgs a) {
     const double tf = a.jd1[i];
     s.x[0] = a.pos[i]; s.x[1] = a.pos[n + i]; s.x[2] = a.pos[2 * n + i];
     s.v[0] = a.vel[i]; s.v[1] = a.vel[n + i]; s.v[2] = a.vel[2 * n + i];
-    SpkForce F;
+    SpkForceUnrolled F;  // one object per thread: fully unrolled Chebyshev loops
     F.n_force = a.n_force;
     F.ng.base = a.nongrav ? a.nongrav + i : nullptr;
     F.ng.stride = n;
