@@ -43,6 +43,9 @@ SPAN = 365.25
 # Earth/Moon + barycentre (6), 10 Newtonian terms (10 x 19) with 2 relative velocities (6),
 # relativistic terms (2 x 34), solar/Jovian J2 (2 x 42), Earth J2 (30).
 FLOPS_PER_EVAL = 1802
+# ncu dram__bytes_read.sum + dram__bytes_write.sum of one node-kernel launch on the default
+# workload (profiles/nbody_nodes_kernel_10k.md)
+NODES_10K_DRAM_BYTES = 860_672 + 4_864
 FLOPS_PER_ITER = 7 * FLOPS_PER_EVAL + 1201  # 7 node evaluations + predictor/g/b/test
 FLOPS_PER_STEP = 120       # state update + step-size control
 
@@ -367,6 +370,28 @@ def run_gpu(args, world, rank, local):
     for _ in range(args.warmup):
         step(d)
     torch.cuda.synchronize()
+    # the timed steps replay a captured CUDA graph of one step (the library allocates nothing
+    # once its buffers have grown to the workload, so the step captures as it runs)
+    graph = None
+    if not args.no_graph:
+        try:
+            side = torch.cuda.Stream(dev)
+            side.wait_stream(torch.cuda.current_stream(dev))
+            with torch.cuda.stream(side):
+                step(d)
+            torch.cuda.current_stream(dev).wait_stream(side)
+            torch.cuda.synchronize()
+            graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(graph):
+                step(d)
+            torch.cuda.synchronize()
+            for _ in range(2):
+                graph.replay()
+            torch.cuda.synchronize()
+        except Exception as e:  # capture refused: time direct launches instead
+            log("CUDA graph capture failed, timing direct launches:", repr(e))
+            graph = None
+    run_step = graph.replay if graph is not None else (lambda: step(d))
     stream = torch.cuda.current_stream(dev)
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
            for _ in range(args.steps)]
@@ -376,7 +401,7 @@ def run_gpu(args, world, rank, local):
         for k in range(args.steps):
             flush.zero_()  # write > L2 (126 MB) between steps, outside the timed pair
             evs[k][0].record(stream)
-            step(d)
+            run_step()
             evs[k][1].record(stream)
         torch.cuda.synchronize()
         barrier(world)
@@ -407,8 +432,12 @@ def run_gpu(args, world, rank, local):
     hbm_bytes = int(h2d + d2h)
     if nbody:
         achieved = flops / (ms_step * 1e-3) / 1e12
+        # DRAM bytes per launch of the node kernel from one ncu capture of this workload
+        # (profiles/nbody_nodes_kernel_10k.md); other workloads have none recorded
+        traffic = NODES_10K_DRAM_BYTES if (kind == "nbody_mba_10k" and best.get("mode") == 2) else None
         roof = {"bound": "fp64", "achieved": achieved, "peak": tflops_probe, "unit": "TFLOP/s",
-                "frac": achieved / tflops_probe if tflops_probe else None, "traffic": None,
+                "frac": achieved / tflops_probe if tflops_probe else None, "traffic": traffic,
+                "traffic_unit": "bytes per launch (DRAM read + write)",
                 "peak_source": "measured DFMA probe (kete_b200_fp64_probe) in this run",
                 "flops_per_launch": flops, "hbm_bytes_algorithmic": hbm_bytes}
     else:
@@ -434,6 +463,7 @@ def run_gpu(args, world, rank, local):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOADS[kind].format(n=n), "n_objects_per_gpu": n,
                    "launch": best, "autotune_sweep_ms": sweep,
+                   "cuda_graph": graph is not None,
                    "l2": "flushed (256 MB write) between timed steps",
                    "parallelism": f"replicas x{world} (objects independent)"},
         "roofline": roof,
@@ -802,6 +832,8 @@ def main():
     ap.add_argument("--fields", type=int, default=SURVEY_FIELDS, help="survey workload: fields")
     ap.add_argument("--cpu-sample", type=int, default=20000,
                     help="survey workload: objects in the CPU oracle's sample")
+    ap.add_argument("--no-graph", action="store_true",
+                    help="time direct launches instead of a captured CUDA graph")
     ap.add_argument("--no-adjoint", action="store_true",
                     help="skip the gradient-cost measurement on the differentiation workload")
     args = ap.parse_args()
