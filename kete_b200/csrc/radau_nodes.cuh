@@ -11,8 +11,10 @@
 //
 // The loop is organised in rounds with a single force-evaluation call site, so groups of a
 // warp that are in different phases (corrector iteration / exact evaluation) still share the
-// expensive instruction stream.  The arithmetic of each step is the reference's; only the
-// division by node spacings uses tabulated reciprocals and multiply-adds are fused.
+// expensive instruction stream.  The arithmetic of each step is the reference's, except
+// that divisions by node spacings use tabulated reciprocals, multiply-adds are fused, each
+// corrector starts from the predicted b (predict_b_row) and the state updates are summed
+// with compensation (Kahan), which the reference does not do.
 #pragma once
 #include "common.cuh"
 #include "forces.cuh"
@@ -71,6 +73,8 @@ __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_nodes_kernel(NBodyArg
     // evaluations (3 doubles each), exchanged after each corrector iteration
     __shared__ double s_b[NODES_BLOCK / NODE_G][21];
     __shared__ double s_e[NODES_BLOCK / NODE_G][NODE_G * 3];
+    // per group: the running compensations of x and v (compensated summation of the updates)
+    __shared__ double s_cmp[NODES_BLOCK / NODE_G][6];
     for (int i = threadIdx.x; i < 9 * NODE_ROW; i += blockDim.x) {
         const int j = i / NODE_ROW, k = i % NODE_ROW;
         double val = 0.0;
@@ -94,6 +98,7 @@ __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_nodes_kernel(NBodyArg
     const int64_t group = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / NODE_G;
     double* sb = s_b[threadIdx.x / NODE_G];
     double* se = s_e[threadIdx.x / NODE_G];
+    double* scmp = s_cmp[threadIdx.x / NODE_G];
     const int comp = lane % 3;  // component this lane forms g and b for (lanes 0-2 publish)
     const double* nrow = s_node + (lane < 7 ? lane + 1 : (SE ? 8 : 7)) * NODE_ROW;
     const bool se_lane = SE && lane == 7;
@@ -129,6 +134,7 @@ __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_nodes_kernel(NBodyArg
             sb[7 + lane] = 0.0;
             sb[14 + lane] = 0.0;
         }
+        if (lane < 6) scmp[lane] = 0.0;
         F.ng.base = a.nongrav ? a.nongrav + obj : nullptr;
         F.ng.stride = n;
         F.ng.kind = a.nongrav ? (int)a.nongrav[obj] : 0;
@@ -292,6 +298,10 @@ __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_nodes_kernel(NBodyArg
         ++iter;
         if (ratio < 1e-14) {
             const double h2 = h * h;
+            // x += dx, v += dv with compensated (Kahan) summation: the rounding error of each
+            // addition is carried into the next step's, so the many small increments of a long
+            // integration do not accumulate rounding in x and v
+            double ncx[3], ncv[3];
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
                 double dw = 0.0, du = 0.0;
@@ -301,8 +311,19 @@ __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_nodes_kernel(NBodyArg
                     dw += bck * c_tab.w[k];
                     du += bck * c_tab.u[k];
                 }
-                x[c] += v[c] * h + h2 * (acc[c] * 0.5 + dw);
-                v[c] += h * (acc[c] + du);
+                const double dx = v[c] * h + h2 * (acc[c] * 0.5 + dw);
+                const double dv = h * (acc[c] + du);
+                const double yx = dx - scmp[c], yv = dv - scmp[3 + c];
+                const double tx = x[c] + yx, tv = v[c] + yv;
+                ncx[c] = (tx - x[c]) - yx;
+                ncv[c] = (tv - v[c]) - yv;
+                x[c] = tx;
+                v[c] = tv;
+            }
+            __syncwarp(gmask);  // every lane has read the old compensations
+            if (lane < 3) {
+                scmp[lane] = lane == 0 ? ncx[0] : (lane == 1 ? ncx[1] : ncx[2]);
+                scmp[3 + lane] = lane == 0 ? ncv[0] : (lane == 1 ? ncv[1] : ncv[2]);
             }
             t += h;
             const double mb6 = fmax(fmax(fabs(b60), fabs(b61)), fabs(b62));
