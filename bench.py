@@ -74,8 +74,13 @@ WORKLOADS = {
                   "H-G V and NEATM NEOS-band magnitudes per detection (H U(12,22), G 0.15, p_V "
                   "lognormal median 0.14 sigma_ln 0.6, beaming 1.0, emissivity 0.9)",
 }
+WORKLOADS["spk_type21_1m"] = ("SPK state queries, {n} epochs of a type-21 (modified difference "
+                              "array) asteroid segment (a 48-record slice of a JPL file), relative "
+                              "to the solar-system barycentre through the Sun's type-2 segment")
 DEFAULT_N = {"nbody_mba_10k": 10_000, "nbody_mixed_1m": 1_000_000, "kepler_100k": 100_000,
-             "survey_10m": 10_000_000}
+             "survey_10m": 10_000_000, "spk_type21_1m": 1_000_000}
+SPK21_SUBSET = os.path.join(ROOT, "tests", "golden", "spk_type21_subset.bsp")
+SPK21_ID = 20000042
 SURVEY_FIELDS, SURVEY_DT_LIMIT = 2000, 3.0
 
 
@@ -267,6 +272,41 @@ def run_reference_survey(args):
     print(json.dumps(line), flush=True)
 
 
+def run_reference_spk(args):
+    """SPK type-21 state queries on the CPU oracle, all host cores."""
+    from kete_b200 import synthetic
+    from oracle import oracle as O
+
+    n = args.n or DEFAULT_N["spk_type21_1m"]
+    jd, _ = spk21_queries(n)
+    with tempfile.TemporaryDirectory() as td:
+        spk = synthetic.write_synthetic_spk(os.path.join(td, "syn.bsp"))
+        O.spk_reset()
+        for p in (spk, SPK21_SUBSET):
+            with open(p, "rb") as f:
+                O.spk_load_bytes(f.read())
+    for _ in range(args.warmup):
+        O.spk_get_states(SPK21_ID, jd[:10000], 0, 1)
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        O.spk_get_states(SPK21_ID, jd, 0, 1)
+    total = time.perf_counter() - t
+    value = n * args.steps / total
+    line = {
+        "impl": "reference", "metric": "SPK type-21 states/s", "value": value, "unit": "states/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic planets + type-21 slice",
+        "config": {"workload": WORKLOADS["spk_type21_1m"].format(n=n), "n_queries": n},
+        "cpu_baseline": {"value": value, "unit": "states/s", "cores": os.cpu_count(),
+                         "kind": "port", "sample": "the full workload per step; the reference "
+                                                   "Rust path cannot be built"},
+        "e2e": {"value": value, "unit": "states/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return
@@ -274,6 +314,8 @@ def run_reference(args, world, rank):
 
     if args.workload == "survey_10m":
         return run_reference_survey(args)
+    if args.workload == "spk_type21_1m":
+        return run_reference_spk(args)
     kind = args.workload
     n = args.n or DEFAULT_N[kind]
     pos, vel, jd0, jd1, ng = workload(n, kind=kind)
@@ -807,6 +849,114 @@ def run_survey(args, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
+def spk21_queries(n, seed=51):
+    """Seeded query epochs inside the type-21 slice's coverage, and the FP64 flops each
+    needs: the modified-difference interpolation at its record's orders plus the Sun's
+    type-2 record (223) and the chain sums (6)."""
+    from kete_b200 import synthetic
+
+    (_, _, _, _, s0, s1, data), = synthetic.read_daf_segments(SPK21_SUBSET)
+    nr, md = int(data[-1]), int(data[-2])
+    rl = 4 * md + 11
+    ep = data[nr * rl:nr * rl + nr]
+    rng = np.random.default_rng(seed)
+    jds = rng.uniform(s0 + 1.0, s1 - 1.0, n)
+    rec = np.minimum(np.searchsorted(ep, jds, side="left"), nr - 1)
+    m = data[rec * rl + 4 * md + 7]
+    kq = sum(data[rec * rl + 4 * md + 8 + c] for c in range(3))
+    flops = (3 * (m - 2) + m + 1.5 * (m - 2) * (m - 1) + 3 * (m - 2) + 4 * kq + 27 + 2 + 223 + 6)
+    return jds / 86400.0 + 2451545.0, float(flops.sum())
+
+
+def run_spk(args, world, rank, local):
+    import ctypes
+
+    import torch
+
+    import kete_b200
+    from kete_b200 import _lib, build, synthetic
+    from oracle import oracle as O
+
+    build.build()
+    torch.cuda.set_device(local)
+    kete_b200.init(local)
+    td = tempfile.mkdtemp(prefix="kete_b200_bench_")
+    spk = synthetic.write_synthetic_spk(os.path.join(td, "syn.bsp"))
+    kete_b200.spice.kernel_reload([spk, SPK21_SUBSET])
+    n = args.n or DEFAULT_N["spk_type21_1m"]
+    jd, flops = spk21_queries(n, seed=51 + rank)
+    dev = torch.device("cuda", local)
+    L = _lib.lib()
+    d_jd = torch.from_numpy(jd).to(dev)
+    d_out = torch.empty((6, n), dtype=torch.float64, device=dev)
+    d_st = torch.empty(n, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        _lib.check(L.kete_b200_spk_get_states(n, SPK21_ID, d_jd.data_ptr(), 0, 1, d_out.data_ptr(),
+                                              d_st.data_ptr(), 1, ctypes.c_void_p(stream.cuda_stream)))
+
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    with ClockSampler(local) as clk:
+        barrier(world)
+        for k in range(args.steps):
+            flush.zero_()
+            evs[k][0].record(stream)
+            step()
+            evs[k][1].record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+    t_total = reduce_max(sum(a.elapsed_time(b) for a, b in evs) * 1e-3, world)
+    ms_step = 1e3 * t_total / args.steps
+    value = world * n * args.steps / t_total
+    # end to end from host arrays (copies inside)
+    hj = torch.from_numpy(jd).pin_memory().numpy()
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        out6, st = kete_b200.spice.get_states_arrays(SPK21_ID, hj, 0, 1)
+    e2e_s = reduce_max((time.perf_counter() - t) / args.steps, world)
+    if rank != 0:
+        return
+    tflops_probe = ctypes_probe(_lib)
+    achieved = flops / (ms_step * 1e-3) / 1e12
+    O.spk_reset()
+    for p in (spk, SPK21_SUBSET):
+        with open(p, "rb") as f:
+            O.spk_load_bytes(f.read())
+    t = time.perf_counter()
+    ref, rst = O.spk_get_states(SPK21_ID, jd, 0, 1)
+    cpu_s = time.perf_counter() - t
+    ok = (st == 0) & (rst == 0)
+    rel = np.abs(out6 - ref).max(axis=0) / np.abs(ref).max(axis=0)
+    line = {
+        "metric": "SPK type-21 states/s", "value": value, "unit": "states/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic planets + a slice of a JPL type-21 asteroid segment",
+        "config": {"workload": WORKLOADS["spk_type21_1m"].format(n=n), "n_queries_per_gpu": n,
+                   "l2": "flushed (256 MB write) between timed steps"},
+        "roofline": {"bound": "fp64", "achieved": achieved, "peak": tflops_probe,
+                     "unit": "TFLOP/s", "frac": achieved / tflops_probe, "traffic": None,
+                     "flops_per_launch": flops,
+                     "peak_source": "measured DFMA probe (kete_b200_fp64_probe) in this run"},
+        "cpu_baseline": {"value": n / cpu_s, "unit": "states/s", "cores": os.cpu_count(),
+                         "kind": "port", "sample": "the full workload, oracle on all host cores"},
+        "e2e": {"value": world * n / e2e_s, "unit": "states/s", "h2d_bytes_per_step": 8 * n,
+                "d2h_bytes_per_step": 52 * n},
+        "gpu_launches": args.steps,
+        "clocks": clk.summary(),
+        "parity": {"max_rel_err": float(rel[ok].max()) if ok.any() else None,
+                   "objects_compared": int(ok.sum()),
+                   "status_mismatches": int((st != rst).sum()), "tolerance_rel": 5e-14},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def ctypes_probe(_lib):
     import ctypes
 
@@ -843,6 +993,8 @@ def main():
         run_reference(args, world, rank)
     elif args.workload == "survey_10m":
         run_survey(args, world, rank, local)
+    elif args.workload == "spk_type21_1m":
+        run_spk(args, world, rank, local)
     else:
         run_gpu(args, world, rank, local)
         if world > 1:

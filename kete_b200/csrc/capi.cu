@@ -69,12 +69,36 @@ constexpr int N_MASSES = 15;
 struct HostSeg {
     int64_t obj_id, center_id;
     int frame_code;
+    int type;                 // 2, 3 (Chebyshev) or 1, 21 (modified difference arrays)
     double jd_start, jd_end;  // JD
     double start_s;           // jd_to_spice_jd(jd_start)
-    double intlen;
-    int64_t n_coef, rsize, n_rec;
+    double intlen;            // types 2, 3
+    int64_t n_coef, rsize, n_rec;  // types 1, 21: n_coef = MAXDIM, rsize = 4 MAXDIM + 11
     std::vector<double> data;  // the DAF array
 };
+
+// Every record of a type 1 / 21 segment must keep the interpolation inside its arrays: the
+// device kernels index by these orders without further checks (SPKE21 reads the same).
+static bool mda_records_valid(const HostSeg& seg) {
+    const int64_t md = seg.n_coef, rl = seg.rsize;
+    const double* ep = seg.data.data() + seg.n_rec * rl;
+    for (int64_t r = 0; r < seg.n_rec; ++r) {
+        const double* rec = seg.data.data() + r * rl;
+        for (int64_t q = 0; q < rl; ++q)
+            if (!std::isfinite(rec[q])) return false;
+        const double kqm = rec[4 * md + 7];
+        if (kqm != std::floor(kqm) || kqm < 2.0 || kqm > (double)std::min<int64_t>(md + 1, 26)) return false;
+        const int64_t kqmax1 = (int64_t)kqm;
+        for (int c = 0; c < 3; ++c) {
+            const double kq = rec[4 * md + 8 + c];
+            if (kq != std::floor(kq) || kq < 0.0 || kq > (double)(kqmax1 - 1)) return false;
+        }
+        for (int64_t j = 0; j < kqmax1 - 2; ++j)
+            if (rec[1 + j] == 0.0) return false;
+        if (!std::isfinite(ep[r]) || (r > 0 && ep[r] < ep[r - 1])) return false;
+    }
+    return true;
+}
 
 struct DevState {
     int version = -1;       // ephemeris version resident on this device
@@ -154,7 +178,8 @@ static int parse_daf(const uint8_t* buf, int64_t n, std::vector<HostSeg>& out, i
             const int64_t nf = a1 - a0 + 1;
             if (a0 < 1 || nf <= 4 || 8 * (a0 - 1) + 8 * nf > n)
                 return set_error(KETE_B200_E_IO, "SPK array outside the file");
-            if (iv[3] != 2) {
+            const int type = iv[3];
+            if (type != 2 && type != 3 && type != 1 && type != 21) {
                 ++skipped;
                 continue;
             }
@@ -162,21 +187,42 @@ static int parse_daf(const uint8_t* buf, int64_t n, std::vector<HostSeg>& out, i
             seg.obj_id = iv[0];
             seg.center_id = iv[1];
             seg.frame_code = iv[2];
+            seg.type = type;
             seg.jd_start = spice_jds_to_jd(f0);
             seg.jd_end = spice_jds_to_jd(f1);
             seg.start_s = jd_to_spice_jd(seg.jd_start);
             seg.data.resize((size_t)nf);
             for (int64_t q = 0; q < nf; ++q) seg.data[q] = rd_f64(buf + 8 * (a0 - 1) + 8 * q, le);
-            seg.rsize = (int64_t)seg.data[nf - 2];
-            seg.intlen = seg.data[nf - 3];
-            seg.n_coef = (seg.rsize - 2) / 3;
-            if (seg.rsize < 5 || 3 * seg.n_coef + 2 != seg.rsize)
-                return set_error(KETE_B200_E_IO,
-                                 "File incorrectly formatted, found number of Chebyshev coefficients "
-                                 "doesn't match expected");
-            seg.n_rec = (nf - 4) / seg.rsize;
-            if (seg.n_rec < 1 || !(seg.intlen > 0.0))
-                return set_error(KETE_B200_E_IO, "type-2 segment without records");
+            if (type == 2 || type == 3) {
+                // From<DafArray> for SpkSegmentType2 / 3 (spk_segments.rs:379-397, 482-498)
+                const int per = type == 2 ? 3 : 6;
+                seg.rsize = (int64_t)seg.data[nf - 2];
+                seg.intlen = seg.data[nf - 3];
+                seg.n_coef = (seg.rsize - 2) / per;
+                if (seg.rsize < 2 + 2 * per || per * seg.n_coef + 2 != seg.rsize)
+                    return set_error(KETE_B200_E_IO,
+                                     "File incorrectly formatted, found number of Chebyshev "
+                                     "coefficients doesn't match expected");
+                seg.n_rec = (nf - 4) / seg.rsize;
+                if (seg.n_rec < 1 || !(seg.intlen > 0.0))
+                    return set_error(KETE_B200_E_IO, "Chebyshev segment without records");
+            } else {
+                // From<DafArray> for SpkSegmentType1 / 21 (spk_segments.rs:302-308, 971-984)
+                const double nr = seg.data[nf - 1];
+                const double md = type == 1 ? 15.0 : seg.data[nf - 2];
+                if (!(nr >= 1.0 && nr < 1e9) || !(md >= 1.0 && md <= 25.0) || md != std::floor(md))
+                    return set_error(KETE_B200_E_IO, "SPK File contains segments of type " +
+                                                         std::to_string(type) +
+                                                         " has invalid contents.");
+                seg.n_rec = (int64_t)nr;
+                seg.n_coef = (int64_t)md;
+                seg.rsize = 4 * seg.n_coef + 11;
+                seg.intlen = 0.0;
+                if (seg.n_rec * (seg.rsize + 1) > nf || !mda_records_valid(seg))
+                    return set_error(KETE_B200_E_IO, "SPK File contains segments of type " +
+                                                         std::to_string(type) +
+                                                         " has invalid contents.");
+            }
             out.push_back(std::move(seg));
         }
     }
@@ -200,7 +246,7 @@ static void build_fast_plan(int n_force, FastPlan& P) {
         }
         const int seg = g_eph.slot[slot].first;
         const SegDesc& d = g_eph.seg[seg];
-        if (d.n_pad != FAST_NC) ok = false;
+        if (d.type != 2 || d.n_pad != FAST_NC) ok = false;
         lo = std::max(lo, d.jd_start);
         hi = std::min(hi, d.jd_end);
         FastItem& I = P.item[n];
@@ -268,7 +314,8 @@ static int rebuild_tables() {
     // FAST_NC, so mixed coefficient counts (as in DE440s) still take it: the extra zero
     // coefficients add exactly nothing to the sums
     int64_t max_coef = 0;
-    for (const auto& sg : g_segs) max_coef = std::max<int64_t>(max_coef, sg.n_coef);
+    for (const auto& sg : g_segs)
+        if (sg.type == 2) max_coef = std::max<int64_t>(max_coef, sg.n_coef);
     const bool common_pad = max_coef <= FAST_NC;
     int nseg = 0;
     for (size_t si = 0; si < ids.size(); ++si) {
@@ -291,12 +338,44 @@ static int rebuild_tables() {
             d.jd_end = s.jd_end;
             d.start_s = s.start_s;
             d.intlen = s.intlen;
-            d.inv_intlen = 1.0 / s.intlen;
+            d.inv_intlen = s.intlen > 0.0 ? 1.0 / s.intlen : 0.0;
             d.n_coef = (int32_t)s.n_coef;
-            d.n_pad = common_pad ? FAST_NC : (int32_t)((s.n_coef + 1) & ~1LL);
             d.n_rec = (int32_t)s.n_rec;
-            d.rsize = 4 + 3 * d.n_pad;
+            d.type = s.type;
             d.offset = (int64_t)g_pool_host.size();
+            d.epoch_offset = 0;
+            if (s.type == 1 || s.type == 21) {
+                // records as stored, then the final epochs
+                d.n_pad = 0;
+                d.rsize = (int32_t)s.rsize;
+                g_pool_host.insert(g_pool_host.end(), s.data.begin(),
+                                   s.data.begin() + s.n_rec * (s.rsize + 1));
+                d.epoch_offset = d.offset + s.n_rec * s.rsize;
+                ++sl.count;
+                ++nseg;
+                continue;
+            }
+            if (s.type == 3) {
+                d.n_pad = (int32_t)((s.n_coef + 1) & ~1LL);
+                d.rsize = 4 + 6 * d.n_pad;
+                for (int64_t r = 0; r < s.n_rec; ++r) {
+                    const double* rec = s.data.data() + r * s.rsize;
+                    const double mid = rec[0], rad = rec[1];
+                    g_pool_host.push_back(mid);
+                    g_pool_host.push_back(rad);
+                    g_pool_host.push_back(1.0 / rad);
+                    g_pool_host.push_back(86400.0 / AU_KM);  // spk_segments.rs:472
+                    for (int c = 0; c < 6; ++c) {
+                        for (int64_t q = 0; q < s.n_coef; ++q) g_pool_host.push_back(rec[2 + c * s.n_coef + q]);
+                        for (int64_t q = s.n_coef; q < d.n_pad; ++q) g_pool_host.push_back(0.0);
+                    }
+                }
+                ++sl.count;
+                ++nseg;
+                continue;
+            }
+            d.n_pad = common_pad ? FAST_NC : (int32_t)((s.n_coef + 1) & ~1LL);
+            d.rsize = 4 + 3 * d.n_pad;
             for (int64_t r = 0; r < s.n_rec; ++r) {
                 const double* rec = s.data.data() + r * s.rsize;
                 const double mid = rec[0], rad = rec[1];
@@ -666,18 +745,13 @@ int kete_b200_spk_get_states(int64_t n, int64_t id, const double* jd, int64_t ce
     if ((rc = ensure_device(ds))) return rc;
     if (n == 0) return 0;
     cudaStream_t st = (cudaStream_t)stream;
-    std::vector<int32_t> slots((size_t)n, it->second);
-    Stager S{*ds, st, 0};
-    int32_t* d_slot = S.in(slots.data(), (size_t)n);
-    S.on_device = on_device;
+    Stager S{*ds, st, on_device};
     const double* d_jd = S.in(jd, (size_t)n);
     double* d_out = S.out(out6, (size_t)n * 6);
     int32_t* d_st = S.out(status, (size_t)n);
     if (S.rc) return S.rc;
-    if ((rc = launch_spk_states(n, d_slot, d_jd, ch, frame, d_out, d_st, st))) return rc;
-    rc = S.finish();
-    if (!rc && on_device) rc = cuda_check(cudaStreamSynchronize(st), "stream synchronize");
-    return rc;
+    if ((rc = launch_spk_states(n, it->second, d_jd, ch, frame, d_out, d_st, st))) return rc;
+    return S.finish();
 }
 
 int kete_b200_propagate_two_body(int64_t n, const double* pos, const double* vel,

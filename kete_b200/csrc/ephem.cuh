@@ -24,13 +24,18 @@ constexpr int MAX_CHAIN = 3;
 constexpr int ORDER_BUCKETS = 64;
 constexpr int ORDER_SCRATCH_HEADER = 256;
 
+// Segment types held on the device: 2 and 3 (Chebyshev position / position and velocity),
+// 1 and 21 (modified difference arrays).
 struct SegDesc {
     double jd_start, jd_end;  // JD, as spice_jds_to_jd(summary) (spice/mod.rs:25-28)
     double start_s;           // jd_to_spice_jd(jd_start), what the reference indexes from
-    double intlen;            // record length in seconds (INTLEN)
+    double intlen;            // types 2, 3: record length in seconds (INTLEN)
     double inv_intlen;        // 1 / intlen
     int64_t offset;           // doubles into the pool of record 0
-    int32_t n_coef, n_pad, n_rec, rsize;
+    int64_t epoch_offset;     // types 1, 21: doubles into the pool of the final-epoch list
+    int32_t n_coef;           // types 2, 3: coefficients per coordinate; 1, 21: MAXDIM
+    int32_t n_pad, n_rec, rsize;
+    int32_t type, pad_;
 };
 
 // One body id with its segments [first, first+count) and the slot of its centre body
@@ -295,6 +300,86 @@ __device__ __forceinline__ const double* eph_record(const EphemConst& E, int seg
     return E.pool + d.offset + (int64_t)idx * d.rsize;
 }
 
+// Type 3 record (SpkSegmentType3::try_get_pos_vel, spk_segments.rs:446-480): position and
+// velocity from their own Chebyshev series, values only.  Device layout:
+//   [mid_s, radius_s, 1/radius_s, 86400/AU_KM, x, y, z, vx, vy, vz] (n_pad each)
+__device__ __forceinline__ void cheb_record3(const double* __restrict__ rec, int n_coef, int n_pad,
+                                             double tau_num, double p[3], double v[3]) {
+    const double x = (tau_num - rec[0]) * rec[2];
+    const double x2 = 2.0 * x;
+    double acc[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) acc[c] = rec[4 + c * n_pad] + rec[4 + c * n_pad + 1] * x;
+    double second_t = 1.0, last_t = x;
+    for (int k = 2; k < n_coef; ++k) {
+        const double next_t = x2 * last_t - second_t;
+#pragma unroll
+        for (int c = 0; c < 6; ++c) acc[c] += rec[4 + c * n_pad + k] * next_t;
+        second_t = last_t;
+        last_t = next_t;
+    }
+    constexpr double INV_AU_KM = 1.0 / AU_KM;
+    const double vs = rec[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        p[c] = acc[c] * INV_AU_KM;
+        v[c] = acc[3 + c] * vs;
+    }
+}
+
+// Types 1 and 21 (SpkSegmentType1 / 21::try_get_pos_vel, spk_segments.rs:207-290,
+// 1008-1090; SPICE's SPKE21): the modified difference array of the first record whose final
+// epoch is at or after t.  Records are kept as the DAF stores them (4*MAXDIM + 11 doubles);
+// the host has checked every record's orders and step sizes, so the indices below stay in
+// bounds (KQMAX1 <= MAXDIM + 1 <= 26, KQ <= KQMAX1 - 1, no zero step).
+__device__ __forceinline__ void mda_record(const double* __restrict__ pool, const SegDesc& d,
+                                           double jds, double p[3], double v[3]) {
+    const double* epochs = pool + d.epoch_offset;
+    int lo = 0, hi = d.n_rec;
+    while (lo < hi) {  // first record whose final epoch is >= jds
+        const int mid = (lo + hi) >> 1;
+        if (epochs[mid] < jds) lo = mid + 1;
+        else hi = mid;
+    }
+    if (lo >= d.n_rec) lo = d.n_rec - 1;
+    const int md = d.n_coef;
+    const double* rec = pool + d.offset + (int64_t)lo * d.rsize;
+    const double* g = rec + 1;
+    const double* ref = rec + 1 + md;
+    const double* dt_arr = rec + 7 + md;
+    const int kqmax1 = (int)rec[4 * md + 7];
+    const double delta = jds - rec[0];
+    double fc[25], wc[25], w[26];
+    double tp = delta;
+    for (int j = 0; j < kqmax1 - 2; ++j) {
+        fc[j] = tp / g[j];
+        wc[j] = delta / g[j];
+        tp = delta + g[j];
+    }
+    for (int j = 0; j < kqmax1; ++j) w[j] = 1.0 / (double)(j + 1);
+    int ks = kqmax1 - 1, ks1 = ks - 1, jx = 0;
+    while (ks >= 2) {
+        jx += 1;
+        for (int j = 0; j < jx; ++j) w[j + ks] = fc[j] * w[j + ks1] - wc[j] * w[j + ks];
+        ks = ks1;
+        ks1 -= 1;
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        double sum = 0.0;
+        for (int j = (int)rec[4 * md + 8 + c]; j >= 1; --j) sum += dt_arr[c * md + j - 1] * w[j + ks - 1];
+        p[c] = (ref[2 * c] + delta * (sum * delta + ref[2 * c + 1])) / AU_KM;
+    }
+    for (int j = 0; j < jx; ++j) w[j + ks] = fc[j] * w[j + ks1] - wc[j] * w[j + ks];
+    ks -= 1;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        double sum = 0.0;
+        for (int j = (int)rec[4 * md + 8 + c]; j >= 1; --j) sum += dt_arr[c * md + j - 1] * w[j + ks - 1];
+        v[c] = (ref[2 * c + 1] + delta * sum) / AU_KM * 86400.0;
+    }
+}
+
 // try_get_raw_state for the body in `slot`: first segment (scan order) whose
 // [jd_start, jd_end] contains jd.
 __device__ __forceinline__ int eph_raw(const EphemConst& E, int slot, double jd, double p[3],
@@ -306,12 +391,17 @@ __device__ __forceinline__ int eph_raw(const EphemConst& E, int slot, double jd,
             // jd_to_spice_jd (spice/mod.rs:31-34), rounded as the reference rounds it: an
             // explicit multiply so the compiler cannot fuse it into the subtraction below
             const double jds = __dmul_rn(jd - 2451545.0, 86400.0);
+            if (d.type == 1 || d.type == 21) {
+                mda_record(E.pool, d, jds, p, v);
+                return ST_OK;
+            }
             // record index floor((t - start) / intlen) (spk_segments.rs:358); the quotient
             // is formed with the tabulated reciprocal
             double fidx = floor((jds - d.start_s) * d.inv_intlen);
             int idx = fidx < 0.0 ? 0 : (fidx >= (double)d.n_rec ? d.n_rec - 1 : (int)fidx);
             const double* rec = E.pool + d.offset + (int64_t)idx * d.rsize;
-            cheb_record(rec, d.n_coef, d.n_pad, jds, p, v);
+            if (d.type == 3) cheb_record3(rec, d.n_coef, d.n_pad, jds, p, v);
+            else cheb_record(rec, d.n_coef, d.n_pad, jds, p, v);
             return ST_OK;
         }
     }

@@ -63,7 +63,7 @@ int noalloc_snapshot(int include_asteroids, int64_t center, NBodyArgs& a, Launch
 int launch_radau_central(int64_t n, const double* pos, const double* vel, const double* t0,
                          const double* t1, double* out_pos, double* out_vel, int32_t* status,
                          cudaStream_t stream);
-int launch_spk_states(int64_t n, const int32_t* slot, const double* jd,
+int launch_spk_states(int64_t n, int32_t slot, const double* jd,
                       const CenterChain& center_chain, int frame, double* out6, int32_t* status,
                       cudaStream_t stream);
 

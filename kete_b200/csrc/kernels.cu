@@ -160,7 +160,7 @@ int launch_radau_central(int64_t n, const double* pos, const double* vel, const 
 // batched SpkCollection::try_get_state (spk.rs:87-96): state of body `slot` (chained to the
 // barycentre) minus the centre chain, in `frame`.
 // -------------------------------------------------------------------------------------------
-__global__ void spk_states_kernel(int64_t n, const int32_t* slot, const double* jd,
+__global__ void spk_states_kernel(int64_t n, int32_t slot, const double* jd,
                                   CenterChain center_chain, int frame, double* out6,
                                   int32_t* status) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -169,7 +169,7 @@ __global__ void spk_states_kernel(int64_t n, const int32_t* slot, const double* 
     double p[3] = {0, 0, 0}, v[3] = {0, 0, 0};
     int rc = ST_OK;
     // the body's own chain: raw(body) + raw(parent) ...
-    int s = slot[i];
+    int s = slot;
     for (int k = 0; k < 3 && s >= 0 && rc == ST_OK; ++k) {
         double sp[3], sv[3];
         rc = eph_raw(c_eph, s, t, sp, sv);
@@ -188,7 +188,7 @@ __global__ void spk_states_kernel(int64_t n, const int32_t* slot, const double* 
     status[i] = rc;
 }
 
-int launch_spk_states(int64_t n, const int32_t* slot, const double* jd,
+int launch_spk_states(int64_t n, int32_t slot, const double* jd,
                       const CenterChain& center_chain, int frame, double* out6, int32_t* status,
                       cudaStream_t stream) {
     if (n <= 0) return 0;

@@ -249,6 +249,49 @@ def fit_type2_segment(body, jd_start, jd_end, record_days, n_coef=14, seed=2024)
     return np.concatenate([recs.ravel(), tail]), center
 
 
+def fit_type3_segment(body, jd_start, jd_end, record_days, n_coef=12, seed=2024):
+    """Type-3 records (Chebyshev position and velocity series fitted separately) of one body.
+
+    Returns (DAF array data, center id)."""
+    n_rec = int(np.ceil((jd_end - jd_start) / record_days))
+    nodes = _cheb_nodes(3 * n_coef)
+    mids = jd_start + (np.arange(n_rec) + 0.5) * record_days
+    rad = record_days / 2.0
+    tj = (mids[:, None] + rad * nodes[None, :]).ravel()
+    p, v, center = synthetic_bodies(tj, seed)[body]
+    pinv = np.linalg.pinv(np.polynomial.chebyshev.chebvander(nodes, n_coef - 1))
+    recs = np.empty((n_rec, 2 + 6 * n_coef))
+    recs[:, 0] = (mids - J2000) * 86400.0
+    recs[:, 1] = rad * 86400.0
+    for c, arr in enumerate((p[0], p[1], p[2], v[0], v[1], v[2])):
+        vals = arr.reshape(n_rec, nodes.size)
+        recs[:, 2 + c * n_coef:2 + (c + 1) * n_coef] = vals @ pinv.T
+    tail = np.array([(jd_start - J2000) * 86400.0, record_days * 86400.0, 2 + 6 * n_coef, n_rec])
+    return np.concatenate([recs.ravel(), tail]), center
+
+
+def read_daf_segments(path):
+    """The segments of a DAF/SPK file: list of (target, center, frame, type, start_s, end_s,
+    data array), in the file's summary order."""
+    buf = open(path, "rb").read()
+    e = "<" if buf[88:96] == b"LTL-IEEE" else ">"
+    nd, ni = struct.unpack(e + "2i", buf[8:16])
+    ss = nd + (ni + 1) // 2
+    nxt = struct.unpack(e + "i", buf[76:80])[0]
+    out = []
+    while nxt:
+        off = 1024 * (nxt - 1)
+        nxt_d, _, nsum = struct.unpack(e + "3d", buf[off:off + 24])
+        for k in range(int(nsum)):
+            o = off + 24 + k * ss * 8
+            s0, s1 = struct.unpack(e + "2d", buf[o:o + 16])
+            tgt, ctr, frm, typ, a0, a1 = struct.unpack(e + "6i", buf[o + 16:o + 40])
+            data = np.frombuffer(buf[8 * (a0 - 1):8 * a1], dtype=e + "f8").astype(np.float64)
+            out.append((tgt, ctr, frm, typ, s0, s1, data))
+        nxt = int(nxt_d)
+    return out
+
+
 def write_daf_spk(path, segments, internal_name="kete_b200 synthetic ephemeris"):
     """Write a little-endian DAF/SPK.  segments: list of (target, center, frame, type,
     start_s, end_s, data)."""
@@ -295,6 +338,19 @@ def write_daf_spk(path, segments, internal_name="kete_b200 synthetic ephemeris")
 
 SPK_BODIES = (10, 1, 2, 3, 399, 301, 4, 5, 6, 7, 8)
 ASTEROIDS = (20000001, 20000002, 20000004, 20000010, 20000704)
+
+
+def write_type3_spk(path, bodies=ASTEROIDS[:2], jd_start=2459000.5, jd_end=2461000.5,
+                    record_days=16.0, n_coef=12, seed=2024):
+    """An SPK of type-3 segments for some of the synthetic asteroids (centre: the Sun)."""
+    segs = []
+    for body in bodies:
+        data, center = fit_type3_segment(body, jd_start, jd_end, record_days, n_coef, seed)
+        n_rec = int(data[-1])
+        s0 = (jd_start - J2000) * 86400.0
+        segs.append((body, center, 1, 3, s0, s0 + n_rec * record_days * 86400.0, data))
+    write_daf_spk(path, segs)
+    return path
 
 
 def write_synthetic_spk(path, jd_start=2457000.5, jd_end=2463000.5, record_days=32.0,

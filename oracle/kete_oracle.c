@@ -612,8 +612,9 @@ int ko_radau_central(const double pos[3], const double vel[3], double t0, double
 }
 
 /* ------------------------------------------------------------------------------------------
- * DAF / SPK type 2 (kete_core/spice/daf.rs:148-351, spk.rs:37-126,210-329,
- * spk_segments.rs:105-177,316-397, interpolation.rs:25-77, spice/mod.rs:25-34)
+ * DAF / SPK types 2, 3, 1 and 21 (kete_core/spice/daf.rs:148-351, spk.rs:37-126,210-329,
+ * spk_segments.rs:105-177,185-310 (type 1),316-397 (type 2),404-480 (type 3),
+ * 964-1105 (type 21), interpolation.rs:25-130, spice/mod.rs:25-34)
  * ---------------------------------------------------------------------------------------- */
 typedef struct {
     int64_t obj_id, center_id;
@@ -622,8 +623,9 @@ typedef struct {
     double jd_start, jd_end;
     double *data;
     int64_t n_data;
-    double jd_step;
-    int64_t n_coef, record_len;
+    double jd_step;              /* types 2, 3 */
+    int64_t n_coef, record_len;  /* types 2, 3: coefficients per coordinate; 1, 21: MAXDIM */
+    int64_t n_rec;               /* types 1, 21 */
 } spk_segment;
 
 static spk_segment *g_planet = NULL, *g_other = NULL;
@@ -717,14 +719,25 @@ int ko_spk_load_buffer(const uint8_t *buf, int64_t n_bytes) {
             seg.n_data = nf;
             seg.data = (double *)malloc((size_t)nf * sizeof(double));
             for (int64_t q = 0; q < nf; ++q) seg.data[q] = rd_f64(buf + 8 * (a0 - 1) + 8 * q, le);
-            if (seg.seg_type != 2) {
-                free(seg.data);
-                return KO_IO_ERROR; /* only type 2 is restated */
+            int bad = 0;
+            if (seg.seg_type == 2 || seg.seg_type == 3) {
+                /* From<DafArray> for SpkSegmentType2 / 3 (spk_segments.rs:379-397, 482-498) */
+                const int per = seg.seg_type == 2 ? 3 : 6;
+                seg.record_len = (int64_t)seg.data[nf - 2];
+                seg.jd_step = seg.data[nf - 3];
+                seg.n_coef = (seg.record_len - 2) / per;
+                bad = nf < 4 || per * seg.n_coef + 2 != seg.record_len || seg.n_coef < 2;
+            } else if (seg.seg_type == 1 || seg.seg_type == 21) {
+                /* From<DafArray> for SpkSegmentType1 / 21 (spk_segments.rs:302-308, 971-984) */
+                seg.n_rec = (int64_t)seg.data[nf - 1];
+                seg.n_coef = seg.seg_type == 1 ? 15 : (int64_t)seg.data[nf - 2];
+                seg.record_len = 4 * seg.n_coef + 11;
+                bad = seg.n_rec < 1 || seg.n_coef < 1 || seg.n_coef > 25 ||
+                      seg.n_rec * (seg.record_len + 1) > nf;
+            } else {
+                bad = 1; /* types 2, 3, 1 and 21 are restated */
             }
-            seg.record_len = (int64_t)seg.data[nf - 2];
-            seg.jd_step = seg.data[nf - 3];
-            seg.n_coef = (seg.record_len - 2) / 3;
-            if (3 * seg.n_coef + 2 != seg.record_len) {
+            if (bad) {
                 free(seg.data);
                 return KO_IO_ERROR;
             }
@@ -768,9 +781,119 @@ typedef struct {
     double pos[3], vel[3];
 } ko_state;
 
+/* chebyshev_evaluate (interpolation.rs:96-130): values only */
+static void cheb_val(double x, const double *cx, const double *cy, const double *cz, int64_t n,
+                     double val[3]) {
+    double x2 = 2.0 * x;
+    val[0] = cx[0] + cx[1] * x;
+    val[1] = cy[0] + cy[1] * x;
+    val[2] = cz[0] + cz[1] * x;
+    double second_t = 1.0, last_t = x, next_t;
+    for (int64_t idx = 2; idx < n; ++idx) {
+        next_t = x2 * last_t - second_t;
+        val[0] += cx[idx] * next_t;
+        val[1] += cy[idx] * next_t;
+        val[2] += cz[idx] * next_t;
+        second_t = last_t;
+        last_t = next_t;
+    }
+}
+
+/* SpkSegmentType3::try_get_pos_vel (spk_segments.rs:446-480): Chebyshev position and
+ * velocity polynomials, values only.  The record index is clamped to the segment. */
+static void type3_state(const spk_segment *s, double jds, double p[3], double v[3]) {
+    double start = jd_to_spice_jd(s->jd_start);
+    double fidx = floor((jds - start) / s->jd_step);
+    int64_t idx = fidx < 0 ? 0 : (int64_t)fidx;
+    int64_t n_rec = (s->n_data - 4) / s->record_len;
+    if (idx >= n_rec) idx = n_rec - 1;
+    const double *rec = s->data + idx * s->record_len;
+    const int64_t n = s->n_coef;
+    double t = (jds - rec[0]) / rec[1];
+    double pp[3], vv[3];
+    cheb_val(t, rec + 2, rec + 2 + n, rec + 2 + 2 * n, n, pp);
+    cheb_val(t, rec + 2 + 3 * n, rec + 2 + 4 * n, rec + 2 + 5 * n, n, vv);
+    double t_scaled = 86400.0 / AU_KM;
+    for (int c = 0; c < 3; ++c) {
+        p[c] = pp[c] / AU_KM;
+        v[c] = vv[c] * t_scaled;
+    }
+}
+
+/* SpkSegmentType1 / 21::try_get_pos_vel (spk_segments.rs:207-290, 1008-1090): the modified
+ * difference array of the first record whose final epoch is at or after t (SPICE's
+ * SPKE21 interpolation).  Returns KO_IO_ERROR for a zero step-size entry. */
+static int mda_state(const spk_segment *s, double jds, double p[3], double v[3]) {
+    const int64_t nr = s->n_rec, md = s->n_coef, rl = s->record_len;
+    const double *epochs = s->data + nr * rl;
+    int64_t lo = 0, hi = nr; /* first index with epochs[idx] >= jds */
+    while (lo < hi) {
+        int64_t mid = lo + (hi - lo) / 2;
+        if (epochs[mid] < jds) lo = mid + 1;
+        else hi = mid;
+    }
+    if (lo >= nr) lo = nr - 1; /* the reference reads past the records here */
+    const double *rec = s->data + lo * rl;
+    const double tl = rec[0];
+    const double *g = rec + 1, *ref = rec + 1 + md, *dt_arr = rec + 7 + md;
+    const int64_t kqmax1 = (int64_t)rec[4 * md + 7];
+    const double *kq = rec + 4 * md + 8;
+    if (kqmax1 < 2 || kqmax1 > md + 1 || kqmax1 > 26) return KO_IO_ERROR;
+    for (int c = 0; c < 3; ++c)
+        if (kq[c] < 0 || kq[c] > (double)(kqmax1 - 1)) return KO_IO_ERROR;
+    const double delta = jds - tl;
+    double fc[25], wc[25], w[27];
+    double tp = delta;
+    const int64_t mq2 = kqmax1 - 2;
+    for (int64_t j = 0; j < mq2; ++j) {
+        if (g[j] == 0.0) return KO_IO_ERROR;
+        fc[j] = tp / g[j];
+        wc[j] = delta / g[j];
+        tp = delta + g[j];
+    }
+    for (int64_t j = 0; j < kqmax1; ++j) w[j] = 1.0 / (double)(j + 1);
+    int64_t ks = kqmax1 - 1, ks1 = ks - 1, jx = 0;
+    while (ks >= 2) {
+        jx += 1;
+        for (int64_t j = 0; j < jx; ++j) w[j + ks] = fc[j] * w[j + ks1] - wc[j] * w[j + ks];
+        ks = ks1;
+        ks1 -= 1;
+    }
+    for (int c = 0; c < 3; ++c) {
+        double sum = 0.0;
+        for (int64_t j = (int64_t)kq[c]; j >= 1; --j) sum += dt_arr[c * md + j - 1] * w[j + ks - 1];
+        p[c] = (ref[2 * c] + delta * (sum * delta + ref[2 * c + 1])) / AU_KM;
+    }
+    for (int64_t j = 0; j < jx; ++j) w[j + ks] = fc[j] * w[j + ks1] - wc[j] * w[j + ks];
+    ks -= 1;
+    for (int c = 0; c < 3; ++c) {
+        double sum = 0.0;
+        for (int64_t j = (int64_t)kq[c]; j >= 1; --j) sum += dt_arr[c * md + j - 1] * w[j + ks - 1];
+        v[c] = (ref[2 * c + 1] + delta * sum) / AU_KM * 86400.0;
+    }
+    return KO_OK;
+}
+
 /* SpkSegment::try_get_state + SpkSegmentType2::try_get_pos_vel */
 static int seg_state(const spk_segment *s, double jd, ko_state *out) {
     if (jd < s->jd_start || jd > s->jd_end) return KO_DAF_LIMITS;
+    if (s->seg_type != 2) {
+        double jds3 = jd_to_spice_jd(jd), p[3], v[3];
+        if (s->seg_type == 3) {
+            type3_state(s, jds3, p, v);
+        } else {
+            int rc = mda_state(s, jds3, p, v);
+            if (rc != KO_OK) return rc;
+        }
+        out->id = s->obj_id;
+        out->center = s->center_id;
+        out->frame = s->frame;
+        for (int c = 0; c < 3; ++c) {
+            out->pos[c] = p[c];
+            out->vel[c] = v[c];
+        }
+        return KO_OK;
+    }
     double jds = jd_to_spice_jd(jd);
     double start = jd_to_spice_jd(s->jd_start);
     double fidx = floor((jds - start) / s->jd_step);
@@ -947,6 +1070,20 @@ int ko_spk_get_state(int64_t id, double jd, int64_t center, int frame, double ou
     if (rc) return rc;
     memcpy(out6, s.pos, 3 * sizeof(double));
     memcpy(out6 + 3, s.vel, 3 * sizeof(double));
+    return KO_OK;
+}
+
+/* SpkCollection::try_get_state for many epochs (the batch form of the call above), OpenMP
+ * over the epochs; out6 is 6 x n (SoA). */
+int ko_spk_get_states(int64_t n, int64_t id, const double *jd, int64_t center, int frame,
+                      double *out6, int32_t *status, int threads) {
+#pragma omp parallel for schedule(static) num_threads(threads > 0 ? threads : omp_get_max_threads())
+    for (int64_t i = 0; i < n; ++i) {
+        double o[6] = {0, 0, 0, 0, 0, 0};
+        int rc = ko_spk_get_state(id, jd[i], center, frame, o);
+        status[i] = rc;
+        for (int c = 0; c < 6; ++c) out6[c * n + i] = rc == KO_OK ? o[c] : NAN;
+    }
     return KO_OK;
 }
 

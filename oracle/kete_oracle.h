@@ -54,6 +54,8 @@ int ko_spk_reset(void);
 int ko_spk_load_buffer(const uint8_t *bytes, int64_t n_bytes);
 /* state of `id` wrt `center` in frame (KO_FRAME_*), like SpkCollection::try_get_state */
 int ko_spk_get_state(int64_t id, double jd, int64_t center, int frame, double out6[6]);
+int ko_spk_get_states(int64_t n, int64_t id, const double *jd, int64_t center, int frame,
+                      double *out6, int32_t *status, int threads);
 
 /* ---- N-body -------------------------------------------------------------------------- */
 /* non-grav row layout (11 doubles): kind, then

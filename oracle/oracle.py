@@ -49,6 +49,8 @@ def lib():
         L.ko_radau_central.argtypes = [_dp, _dp, C.c_double, C.c_double, _dp, _dp]
         L.ko_spk_load_buffer.argtypes = [C.c_char_p, C.c_int64]
         L.ko_spk_get_state.argtypes = [C.c_int64, C.c_double, C.c_int64, C.c_int, _dp]
+        L.ko_spk_get_states.argtypes = [C.c_int64, C.c_int64, _dp, C.c_int64, C.c_int, _dp,
+                                        C.POINTER(C.c_int32), C.c_int]
         L.ko_spk_accel.argtypes = [C.c_double, _dp, _dp, C.c_int, _dp, C.c_int, _dp, _i64p]
         L.ko_propagate_n_body_spk.argtypes = [_dp, _dp, C.c_double, C.c_int, C.c_int64,
                                               C.c_double, C.c_int, _dp, _dp, _dp, _i64p, _dp,
@@ -147,6 +149,17 @@ def spk_get_state(naif_id, jd, center=0, frame=FRAME_EQUATORIAL):
     out = np.zeros(6)
     rc = lib().ko_spk_get_state(naif_id, jd, center, frame, _p(out))
     return rc, out
+
+
+def spk_get_states(naif_id, jd, center=0, frame=FRAME_EQUATORIAL, threads=0):
+    """Batch form: jd (n,) -> out6 (6, n), status (n,) (OpenMP over the epochs)."""
+    jd = np.ascontiguousarray(jd, dtype=np.float64)
+    n = jd.size
+    out = np.zeros((6, n))
+    st = np.zeros(n, dtype=np.int32)
+    lib().ko_spk_get_states(n, naif_id, _p(jd), center, frame, _p(out), st.ctypes.data_as(_i32p),
+                            threads)
+    return out, st
 
 
 def spk_accel(t, pos, vel, include_extended=False, ng=None, exact=False):
