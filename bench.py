@@ -631,7 +631,7 @@ def adjoint_section(dev, warmup, steps):
 
 
 def survey_inputs(n, n_fields, seed=41):
-    """Population with H/G/albedo, and the time-sorted field table (19, F)."""
+    """Population with H/G/albedo, and the time-sorted field table (20, F)."""
     from kete_b200 import fov as fovmod
     from kete_b200 import synthetic
     from kete_b200.state import Frames, State

@@ -47,6 +47,12 @@ extern "C" {
 #define KETE_B200_E_IO (-4)
 #define KETE_B200_E_UNSUPPORTED (-5)
 
+/* field-of-view table: rows per patch column, and the patch kinds of its last row */
+#define KETE_B200_FOV_ROWS 20
+#define KETE_B200_PATCH_RECTANGLE 0
+#define KETE_B200_PATCH_CONE 1
+#define KETE_B200_PATCH_OMNIDIRECTIONAL 2
+
 #define KETE_B200_FRAME_EQUATORIAL 1
 #define KETE_B200_FRAME_ECLIPTIC 2
 
@@ -175,9 +181,13 @@ int kete_b200_radau_central(int64_t n, const double* pos, const double* vel, con
 /* --- fields of view ----------------------------------------------------------------------
  * FovLike::check_visible (src/kete_core/src/fov/fov_like.rs:134-192) of n_obj heliocentric
  * ecliptic states (each at its own epoch jd[i]; valid: NULL or n_obj flags, 0 = skip) in
- * n_fov rectangular fields at once.  fov is 19 x n_fov: observer jd, observer position[3]
- * and velocity[3] (heliocentric ecliptic), then the 4 edge normals (12 values) of
- * OnSkyRectangle (fov/patches.rs:122-155).  Objects within dt_limit days of a field are
+ * n_fov fields at once.  fov is KETE_B200_FOV_ROWS x n_fov, one column per sky patch:
+ * observer jd, observer position[3] and velocity[3] (heliocentric ecliptic), 12 patch
+ * parameters, then the patch kind: KETE_B200_PATCH_RECTANGLE (the 4 edge normals of
+ * OnSkyRectangle, fov/patches.rs:122-155), KETE_B200_PATCH_CONE (unit pointing[3] and the
+ * half-angle in radians of SphericalCone, patches.rs:277-337) or
+ * KETE_B200_PATCH_OMNIDIRECTIONAL (always inside, fov/generic.rs:97-135).  A multi-patch
+ * field (NeosVisit, ZtfField) is one column per patch.  Objects within dt_limit days of a field are
  * pre-filtered by linear motion and confirmed by two-body propagation with light delay;
  * the others by two-body then N-body propagation (include_asteroids as for
  * propagate_n_body).  Each visible (field, object) pair writes out_fov, out_obj and the
@@ -190,6 +200,15 @@ int kete_b200_fov_check_visible(int64_t n_obj, const double* pos, const double* 
                                 int64_t capacity, int32_t* out_fov, int32_t* out_obj,
                                 double* out_state, int64_t* n_visible, int on_device,
                                 void* stream);
+
+/* FovLike::check_statics (src/kete_core/src/fov/fov_like.rs:228-250): which of the n_fov
+ * patches (fov as for kete_b200_fov_check_visible) contain each of n_vec fixed directions
+ * (vec: 3 x n_vec, observer to target, ecliptic).  Each contained (patch, direction) pair
+ * writes out_fov / out_idx; *n_found is the total, which may exceed capacity (the excess
+ * is not written).  Order of the pairs is unspecified. */
+int kete_b200_fov_contains(int64_t n_vec, const double* vec, int64_t n_fov, const double* fov,
+                           int64_t capacity, int32_t* out_fov, int32_t* out_idx,
+                           int64_t* n_found, int on_device, void* stream);
 
 /* --- magnitudes ---------------------------------------------------------------------------
  * hg_apparent_mag (src/kete/rust/flux/reflected.rs:120-132, HGParams::apparent_mag

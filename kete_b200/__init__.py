@@ -5,7 +5,8 @@ Drop-in GPU versions of kete's ``propagate_two_body``, ``propagate_n_body``,
 by hand-written sm_100a CUDA kernels in ``libketeb200.so`` (C ABI: include/kete_b200.h).
 """
 from . import autodiff, flux, fov, spice
-from .fov import RectangleFOV, fov_state_check
+from .fov import (ConeFOV, NeosCmos, NeosVisit, OmniDirectionalFOV, RectangleFOV, WiseCmos,
+                  ZtfCcdQuad, ZtfField, fov_spk_check, fov_state_check, fov_static_check)
 from ._lib import KeteB200Error, init
 from .propagation import (
     NonGravModel,
@@ -22,7 +23,16 @@ __all__ = [
     "flux",
     "fov",
     "RectangleFOV",
+    "ConeFOV",
+    "OmniDirectionalFOV",
+    "WiseCmos",
+    "NeosCmos",
+    "NeosVisit",
+    "ZtfCcdQuad",
+    "ZtfField",
     "fov_state_check",
+    "fov_spk_check",
+    "fov_static_check",
     "spice",
     "init",
     "KeteB200Error",

@@ -991,6 +991,7 @@ int kete_b200_propagate_n_body_stm(int64_t n, const double* pos, const double* v
 }
 
 static_assert(SENS_STRIDE == KETE_B200_CHECKPOINT_DOUBLES, "checkpoint size");
+static_assert(FOV_STRIDE == KETE_B200_FOV_ROWS, "field table rows");
 int kete_b200_checkpoint_doubles(void) { return KETE_B200_CHECKPOINT_DOUBLES; }
 
 int kete_b200_propagate_n_body_checkpointed(int64_t n, const double* pos, const double* vel,
@@ -1087,6 +1088,45 @@ int kete_b200_propagate_n_body_adjoint(int64_t n, int n_epochs, const double* ep
     a.rec = (double*)rec;
     if ((rc = launch_sens_backward(a, st))) return rc;
     return S.finish();
+}
+
+int kete_b200_fov_contains(int64_t n_vec, const double* vec, int64_t n_fov, const double* fov,
+                           int64_t capacity, int32_t* out_fov, int32_t* out_idx,
+                           int64_t* n_found, int on_device, void* stream) {
+    if (n_vec < 0 || n_fov < 0 || capacity < 0 || !n_found)
+        return set_error(KETE_B200_E_ARGUMENT, "negative size or null count");
+    if (n_vec > 0 && !vec) return set_error(KETE_B200_E_ARGUMENT, "null direction array");
+    if (n_fov > 0 && !fov) return set_error(KETE_B200_E_ARGUMENT, "null field table");
+    if (capacity > 0 && (!out_fov || !out_idx)) return set_error(KETE_B200_E_ARGUMENT, "null output");
+    if (n_vec > INT32_MAX || n_fov > INT32_MAX)
+        return set_error(KETE_B200_E_ARGUMENT, "more than 2^31 directions or fields");
+    std::lock_guard<std::mutex> lk(g_mu);
+    DevState* ds;
+    int rc = ensure_device(ds);
+    if (rc) return rc;
+    *n_found = 0;
+    if (n_vec == 0 || n_fov == 0) return 0;
+    cudaStream_t st = (cudaStream_t)stream;
+    Stager S{*ds, st, on_device};
+    const double* d_vec = S.in(vec, 3 * (size_t)n_vec);
+    const double* d_fov = S.in(fov, (size_t)FOV_STRIDE * n_fov);
+    int32_t* d_f = S.out(out_fov, (size_t)capacity);
+    int32_t* d_i = S.out(out_idx, (size_t)capacity);
+    if (S.rc) return S.rc;
+    void* cnt = nullptr;
+    if ((rc = staging(*ds, 35, sizeof(unsigned long long), &cnt))) return rc;
+    if ((rc = cuda_check(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), st), "clear counter")))
+        return rc;
+    if ((rc = launch_fov_contains(n_vec, d_vec, n_fov, d_fov, capacity, (unsigned long long*)cnt, d_f,
+                                  d_i, st)))
+        return rc;
+    unsigned long long h = 0;
+    if ((rc = cuda_check(cudaMemcpyAsync(&h, cnt, sizeof h, cudaMemcpyDeviceToHost, st), "read counter")))
+        return rc;
+    if ((rc = S.finish())) return rc;
+    if ((rc = cuda_check(cudaStreamSynchronize(st), "stream synchronize"))) return rc;
+    *n_found = (int64_t)h;
+    return 0;
 }
 
 int kete_b200_fov_check_visible(int64_t n_obj, const double* pos, const double* vel,

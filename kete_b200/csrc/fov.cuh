@@ -34,6 +34,34 @@ __device__ __forceinline__ bool rect_contains(const double* __restrict__ nrm, co
     return true;
 }
 
+// SphericalCone::contains (fov/patches.rs:300-337): the angle between the unit pointing and
+// the normalised direction; outside, the distance to move into the cone.
+__device__ __forceinline__ bool cone_contains(const double* __restrict__ prm, const double v[3],
+                                              double& dist) {
+    const double r = norm3(v[0], v[1], v[2]);
+    const double d = fabs(acos(prm[0] * (v[0] / r) + prm[1] * (v[1] / r) + prm[2] * (v[2] / r)));
+    if (d <= prm[3]) {
+        dist = 0.0;
+        return true;
+    }
+    const double min_angle = fabs(d - prm[3]);
+    dist = min_angle > 1.5707963267948966 ? r : sin(min_angle) * r;
+    return false;
+}
+
+// The containment test of one field row by its patch kind (OmniDirectional::contains,
+// fov/generic.rs:123-125, is always inside).
+__device__ __forceinline__ bool patch_contains(const double* __restrict__ f, const double v[3],
+                                               double& dist) {
+    const int kind = (int)f[FOV_KIND_ROW];
+    if (kind == 1) return cone_contains(f + 7, v, dist);
+    if (kind == 2) {
+        dist = 0.0;
+        return true;
+    }
+    return rect_contains(f + 7, v, dist);
+}
+
 // check_two_body: Kepler to the observer epoch, back by the light time, Kepler again.
 __device__ __forceinline__ int fov_two_body(const double* __restrict__ f, double jd,
                                             const double pos[3], const double vel[3], bool& inside,
@@ -47,7 +75,7 @@ __device__ __forceinline__ int fov_two_body(const double* __restrict__ f, double
     rc = analytic_2_body(t2 - ojd, p, v);
     if (rc != ST_OK) return rc;
     const double rel[3] = {p[0] - f[1], p[1] - f[2], p[2] - f[3]};
-    inside = rect_contains(f + 7, rel, dist);
+    inside = patch_contains(f, rel, dist);
     fin[0] = t2;
     fin[1] = p[0]; fin[2] = p[1]; fin[3] = p[2];
     fin[4] = v[0]; fin[5] = v[1]; fin[6] = v[2];
@@ -97,7 +125,7 @@ __global__ void __launch_bounds__(128) fov_prefilter_kernel(FovArgs a) {
                 const double dt = f[0] - jd - norm3(rel0, rel1, rel2) * C_AU_PER_DAY_INV;
                 const double nrel[3] = {pos[0] + vel[0] * dt - f[1], pos[1] + vel[1] * dt - f[2],
                                         pos[2] + vel[2] * dt - f[3]};
-                if (!rect_contains(f + 7, nrel, dist) && dist > max_dist) continue;
+                if (!patch_contains(f, nrel, dist) && dist > max_dist) continue;
                 if (fov_two_body(f, jd, pos, vel, inside, dist, fin) == ST_OK && inside)
                     fov_emit(a, (int)(base + t), i, fin);
             } else {
@@ -148,9 +176,50 @@ __global__ void fov_nbody_finish_kernel(FovArgs a, int64_t m, const double* __re
     if (analytic_2_body(t2 - ojd, p, v) != ST_OK) return;
     const double rel[3] = {p[0] - fcol[1], p[1] - fcol[2], p[2] - fcol[3]};
     double dist;
-    if (!rect_contains(fcol + 7, rel, dist)) return;
+    if (!patch_contains(fcol, rel, dist)) return;
     const double fin[7] = {t2, p[0], p[1], p[2], v[0], v[1], v[2]};
     fov_emit(a, f, a.cand_obj[k], fin);
+}
+
+// FovLike::check_static (fov/fov_like.rs:228-250 through contains): which fields contain
+// each fixed direction (observer to target, heliocentric ecliptic).  One thread per
+// direction, looping over tiles of fields staged in shared memory; every (field, direction)
+// pair inside is appended at an atomic counter (pairs beyond `capacity` are counted, not
+// written).
+__global__ void __launch_bounds__(128) fov_contains_kernel(int64_t n_vec, const double* __restrict__ vec,
+                                                           int64_t n_fov, const double* __restrict__ fov,
+                                                           int64_t capacity,
+                                                           unsigned long long* __restrict__ counter,
+                                                           int32_t* __restrict__ out_fov,
+                                                           int32_t* __restrict__ out_idx) {
+    __shared__ double s_f[FOV_TILE * FOV_STRIDE];
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool active = i < n_vec;
+    double v[3] = {0.0, 0.0, 0.0};
+    if (active) {
+        v[0] = vec[i];
+        v[1] = vec[n_vec + i];
+        v[2] = vec[2 * n_vec + i];
+    }
+    for (int64_t base = 0; base < n_fov; base += FOV_TILE) {
+        const int nt = (int)((n_fov - base) < FOV_TILE ? (n_fov - base) : FOV_TILE);
+        __syncthreads();
+        for (int q = threadIdx.x; q < nt * FOV_STRIDE; q += blockDim.x) {
+            const int f = q / FOV_STRIDE, c = q % FOV_STRIDE;
+            s_f[q] = fov[(int64_t)c * n_fov + base + f];
+        }
+        __syncthreads();
+        if (!active) continue;
+        for (int t = 0; t < nt; ++t) {
+            double dist;
+            if (!patch_contains(s_f + t * FOV_STRIDE, v, dist)) continue;
+            const unsigned long long k = atomicAdd(counter, 1ULL);
+            if ((int64_t)k < capacity) {
+                out_fov[k] = (int32_t)(base + t);
+                out_idx[k] = (int32_t)i;
+            }
+        }
+    }
 }
 
 }  // namespace kb

@@ -5,7 +5,11 @@
 namespace kb {
 
 constexpr int FOV_TILE = 128;   // fields staged in shared memory per pass
-constexpr int FOV_STRIDE = 19;  // doubles per field: jd, pos[3], vel[3], normals[12]
+// doubles per field (patch): observer jd, pos[3], vel[3], then 12 patch parameters and the
+// patch kind: 0 rectangle (4 edge normals), 1 cone (unit pointing[3], half-angle),
+// 2 omnidirectional (no parameters)
+constexpr int FOV_STRIDE = 20;
+constexpr int FOV_KIND_ROW = 19;
 
 struct FovArgs {
     int64_t n_obj;

@@ -121,6 +121,9 @@ struct FovArgs;
 int launch_fov_prefilter(const FovArgs& a, cudaStream_t stream);
 int launch_fov_gather(const FovArgs& a, int64_t m, double* gpos, double* gvel, double* gjd0,
                       double* gjd1, cudaStream_t stream);
+int launch_fov_contains(int64_t n_vec, const double* vec, int64_t n_fov, const double* fov,
+                        int64_t capacity, unsigned long long* counter, int32_t* out_fov,
+                        int32_t* out_idx, cudaStream_t stream);
 int launch_fov_finish(const FovArgs& a, int64_t m, const double* npos, const double* nvel,
                       const int32_t* nst, cudaStream_t stream);
 int launch_hg_mag(int64_t n, const double* s2obj, const double* s2obs, const double* h,

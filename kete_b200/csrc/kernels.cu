@@ -498,6 +498,15 @@ int launch_fov_gather(const FovArgs& a, int64_t m, double* gpos, double* gvel, d
     return cuda_check(cudaGetLastError(), "fov_gather_kernel launch");
 }
 
+int launch_fov_contains(int64_t n_vec, const double* vec, int64_t n_fov, const double* fov,
+                        int64_t capacity, unsigned long long* counter, int32_t* out_fov,
+                        int32_t* out_idx, cudaStream_t stream) {
+    if (n_vec <= 0 || n_fov <= 0) return 0;
+    fov_contains_kernel<<<(unsigned)((n_vec + 127) / 128), 128, 0, stream>>>(
+        n_vec, vec, n_fov, fov, capacity, counter, out_fov, out_idx);
+    return cuda_check(cudaGetLastError(), "fov_contains_kernel launch");
+}
+
 int launch_fov_finish(const FovArgs& a, int64_t m, const double* npos, const double* nvel,
                       const int32_t* nst, cudaStream_t stream) {
     if (m <= 0) return 0;

@@ -1351,12 +1351,37 @@ int ko_rect_contains(const double nrm[12], const double v[3], double *dist) {
     return 1;
 }
 
+/* SphericalCone::contains (fov/patches.rs:300-337): prm = unit pointing (3), half-angle */
+int ko_cone_contains(const double prm[4], const double v[3], double *dist) {
+    double r = norm3(v);
+    double u[3] = {v[0] / r, v[1] / r, v[2] / r};
+    double d = fabs(acos(dot3(prm, u)));
+    if (d <= prm[3]) {
+        *dist = 0.0;
+        return 1;
+    }
+    double min_angle = fabs(d - prm[3]);
+    *dist = min_angle > 1.5707963267948966 ? r : sin(min_angle) * r;
+    return 0;
+}
+
+/* One patch of a field: kind 0 rectangle (4 edge normals), 1 cone (pointing, half-angle),
+ * 2 omnidirectional (OmniDirectional::contains, fov/generic.rs:123-125: always inside). */
+int ko_patch_contains(const double prm[12], int kind, const double v[3], double *dist) {
+    if (kind == 1) return ko_cone_contains(prm, v, dist);
+    if (kind == 2) {
+        *dist = 0.0;
+        return 1;
+    }
+    return ko_rect_contains(prm, v, dist);
+}
+
 typedef struct {
     double jd, pos[3], vel[3];
 } fstate;
 
-static int check_two_body_fov(const double obs7[7], const double nrm[12], const fstate *s,
-                              int *inside, double *dist, fstate *fin) {
+static int check_two_body_fov(const double obs7[7], const double nrm[12], int kind,
+                              const fstate *s, int *inside, double *dist, fstate *fin) {
     double op[3], ov[3];
     int rc = analytic_2_body_d(obs7[0] - s->jd, s->pos, s->vel, 0, op, ov);
     if (rc) return rc;
@@ -1367,15 +1392,16 @@ static int check_two_body_fov(const double obs7[7], const double nrm[12], const 
     rc = analytic_2_body_d(t2 - obs7[0], op, ov, 0, p2, v2);
     if (rc) return rc;
     double rel[3] = {p2[0] - obs7[1], p2[1] - obs7[2], p2[2] - obs7[3]};
-    *inside = ko_rect_contains(nrm, rel, dist);
+    *inside = ko_patch_contains(nrm, kind, rel, dist);
     fin->jd = t2;
     memcpy(fin->pos, p2, sizeof p2);
     memcpy(fin->vel, v2, sizeof v2);
     return KO_OK;
 }
 
-static int check_n_body_fov(const double obs7[7], const double nrm[12], const fstate *s,
-                            int include_extended, int *inside, double *dist, fstate *fin) {
+static int check_n_body_fov(const double obs7[7], const double nrm[12], int kind,
+                            const fstate *s, int include_extended, int *inside, double *dist,
+                            fstate *fin) {
     double op[3], ov[3];
     /* states here are heliocentric ecliptic (center 10, frame Ecliptic) */
     int rc = ko_propagate_n_body_spk(s->pos, s->vel, s->jd, KO_FRAME_ECLIPTIC, 10, obs7[0],
@@ -1388,7 +1414,7 @@ static int check_n_body_fov(const double obs7[7], const double nrm[12], const fs
     rc = analytic_2_body_d(t2 - obs7[0], op, ov, 0, p2, v2);
     if (rc) return rc;
     double rel[3] = {p2[0] - obs7[1], p2[1] - obs7[2], p2[2] - obs7[3]};
-    *inside = ko_rect_contains(nrm, rel, dist);
+    *inside = ko_patch_contains(nrm, kind, rel, dist);
     fin->jd = t2;
     memcpy(fin->pos, p2, sizeof p2);
     memcpy(fin->vel, v2, sizeof v2);
@@ -1398,6 +1424,15 @@ static int check_n_body_fov(const double obs7[7], const double nrm[12], const fs
 void ko_fov_check_visible(const double obs7[7], const double nrm[12], int64_t n,
                           const double *pos, const double *vel, const double *jd,
                           double dt_limit, int include_extended, int32_t *flags, double *out7) {
+    ko_fov_check_visible_kind(obs7, nrm, 0, n, pos, vel, jd, dt_limit, include_extended, flags,
+                              out7);
+}
+
+/* check_visible for a patch of any kind (ko_patch_contains) */
+void ko_fov_check_visible_kind(const double obs7[7], const double nrm[12], int kind, int64_t n,
+                               const double *pos, const double *vel, const double *jd,
+                               double dt_limit, int include_extended, int32_t *flags,
+                               double *out7) {
 #pragma omp parallel for schedule(dynamic, 1000)
     for (int64_t i = 0; i < n; ++i) {
         fstate s;
@@ -1419,14 +1454,14 @@ void ko_fov_check_visible(const double obs7[7], const double nrm[12], int64_t n,
             double np[3], nrel[3];
             for (int c = 0; c < 3; ++c) np[c] = s.pos[c] + s.vel[c] * dt;
             for (int c = 0; c < 3; ++c) nrel[c] = np[c] - obs7[1 + c];
-            int lin_in = ko_rect_contains(nrm, nrel, &dist);
+            int lin_in = ko_patch_contains(nrm, kind, nrel, &dist);
             if (!(!lin_in && dist > max_dist)) {
-                if (check_two_body_fov(obs7, nrm, &s, &inside, &dist, &fin) == KO_OK && inside) vis = 1;
+                if (check_two_body_fov(obs7, nrm, kind, &s, &inside, &dist, &fin) == KO_OK && inside) vis = 1;
             }
         } else {
-            if (check_two_body_fov(obs7, nrm, &s, &inside, &dist, &fin) == KO_OK) {
+            if (check_two_body_fov(obs7, nrm, kind, &s, &inside, &dist, &fin) == KO_OK) {
                 if (!(!inside && dist > max_dist)) {
-                    if (check_n_body_fov(obs7, nrm, &s, include_extended, &inside, &dist, &fin) == KO_OK &&
+                    if (check_n_body_fov(obs7, nrm, kind, &s, include_extended, &inside, &dist, &fin) == KO_OK &&
                         inside)
                         vis = 1;
                 }

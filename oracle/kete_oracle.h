@@ -80,6 +80,12 @@ void ko_propagate_n_body_batch(int64_t n, const double *pos, const double *vel,
 void ko_rect_from_pointing(const double pointing[3], double rotation, double lon_width,
                            double lat_width, double normals12[12]);
 /* returns 1 inside, 0 outside; *dist is Contains::Outside distance */
+int ko_cone_contains(const double prm[4], const double v[3], double *dist);
+int ko_patch_contains(const double prm[12], int kind, const double v[3], double *dist);
+void ko_fov_check_visible_kind(const double obs7[7], const double prm[12], int kind, int64_t n,
+                               const double *pos, const double *vel, const double *jd,
+                               double dt_limit, int include_extended, int32_t *flags,
+                               double *out7);
 int ko_rect_contains(const double normals12[12], const double v[3], double *dist);
 /* check_visible of one rectangle FOV for n heliocentric-ecliptic states at epoch jd[i].
  * obs7 = (jd, pos[3], vel[3]).  Writes flags[i] = 1 if visible and the light-time

@@ -62,6 +62,9 @@ def lib():
         L.ko_rect_contains.argtypes = [_dp, _dp, _dp]
         L.ko_fov_check_visible.argtypes = [_dp, _dp, C.c_int64, _dp, _dp, _dp, C.c_double,
                                            C.c_int, _i32p, _dp]
+        L.ko_fov_check_visible_kind.argtypes = [_dp, _dp, C.c_int, C.c_int64, _dp, _dp, _dp,
+                                                C.c_double, C.c_int, _i32p, _dp]
+        L.ko_patch_contains.argtypes = [_dp, C.c_int, _dp, _dp]
         L.ko_hg_phase_curve_correction.argtypes = [C.c_double, C.c_double]
         L.ko_hg_phase_curve_correction.restype = C.c_double
         L.ko_hg_apparent_mag.argtypes = [_dp, _dp, C.c_double, C.c_double]
@@ -205,17 +208,31 @@ def rect_contains(normals, v):
     return bool(inside), d.value
 
 
-def fov_check_visible(obs7, normals, pos, vel, jd, dt_limit=3.0, include_extended=False):
+def patch_contains(params, kind, v):
+    """One patch: kind 0 rectangle (params = 4 normals), 1 cone (pointing, half-angle),
+    2 omnidirectional.  Returns (inside, distance)."""
+    prm = np.zeros(12)
+    a = np.asarray(params, dtype=np.float64).ravel()
+    prm[:a.size] = a
+    d = C.c_double()
+    inside = lib().ko_patch_contains(_p(prm), int(kind), _p(_v3(v)), C.byref(d))
+    return bool(inside), d.value
+
+
+def fov_check_visible(obs7, normals, pos, vel, jd, dt_limit=3.0, include_extended=False, kind=0):
     obs7 = np.ascontiguousarray(obs7, dtype=np.float64)
-    nrm = np.ascontiguousarray(normals, dtype=np.float64).reshape(12)
+    nrm = np.zeros(12)
+    a = np.asarray(normals, dtype=np.float64).ravel()
+    nrm[:a.size] = a
     pos = np.ascontiguousarray(pos, dtype=np.float64)
     vel = np.ascontiguousarray(vel, dtype=np.float64)
     n = pos.shape[1]
     jd = np.ascontiguousarray(np.broadcast_to(jd, (n,)), dtype=np.float64)
     flags = np.zeros(n, dtype=np.int32)
     out7 = np.zeros((7, n))
-    lib().ko_fov_check_visible(_p(obs7), _p(nrm), n, _p(pos), _p(vel), _p(jd), dt_limit,
-                               int(include_extended), flags.ctypes.data_as(_i32p), _p(out7))
+    lib().ko_fov_check_visible_kind(_p(obs7), _p(nrm), int(kind), n, _p(pos), _p(vel), _p(jd),
+                                    dt_limit, int(include_extended), flags.ctypes.data_as(_i32p),
+                                    _p(out7))
     return flags, out7
 
 
