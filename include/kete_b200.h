@@ -172,6 +172,25 @@ int kete_b200_propagate_n_body_adjoint(int64_t n, int n_epochs, const double* ep
                                        double* out_grad, int32_t* grad_status, int on_device,
                                        void* stream);
 
+/* propagate_n_body_vec (src/kete_core/src/propagation/mod.rs:142-237, kete's
+ * propagate_n_body_long, src/kete/rust/propagation.rs:203-249): n test particles
+ * (heliocentric J2000 equatorial pos / vel 3 x n, all at jd0) integrated to jd1 together
+ * with the nine massive bodies of SIMPLE_PLANETS (Sun, Mercury, Venus, Earth-Moon
+ * barycentre, Mars to Neptune), in batches of batch_size particles (1 to 55) that each
+ * share one integration with the massive bodies, as the reference's chunks do.  planets:
+ * 9 x 6 heliocentric equatorial states at jd0 (row per body, in that order), or NULL to
+ * read them from the loaded SPK.  nongrav: NULL or 10 x n rows as for
+ * kete_b200_propagate_n_body; as in the reference (acceleration.rs:239-240) the first
+ * particle of each batch gets no non-gravitational force.  Outputs are relative to the
+ * Sun's final state; out_planets (9 x 6, may be NULL) receives the massive bodies of the
+ * last batch.  status[i] is the outcome of object i's batch (an impact or a failed
+ * convergence fails the whole batch). */
+int kete_b200_propagate_n_body_long(int64_t n, const double* pos, const double* vel, double jd0,
+                                    double jd1, const double* planets, const double* nongrav,
+                                    int batch_size, double* out_pos, double* out_vel,
+                                    double* out_planets, int32_t* status, int on_device,
+                                    void* stream);
+
 /* RadauIntegrator::integrate with central_accel (propagation/mod.rs:35-46,126-138): the
  * integrator alone, for checking it against kete's closed-form two-body result. */
 int kete_b200_radau_central(int64_t n, const double* pos, const double* vel, const double* t0,

@@ -12,6 +12,8 @@ from .propagation import (
     NonGravModel,
     propagate_n_body,
     propagate_n_body_arrays,
+    propagate_n_body_long,
+    propagate_n_body_long_arrays,
     propagate_two_body,
     propagate_two_body_arrays,
     radau_central_arrays,
@@ -39,6 +41,8 @@ __all__ = [
     "NonGravModel",
     "propagate_n_body",
     "propagate_n_body_arrays",
+    "propagate_n_body_long",
+    "propagate_n_body_long_arrays",
     "propagate_two_body",
     "propagate_two_body_arrays",
     "radau_central_arrays",

@@ -496,6 +496,25 @@ static int ensure_tables(DevState& ds) {
             t.adj_p[jj][col] = s2;
         }
     }
+    // SIMPLE_PLANETS: MASSES 0, 1, 2, the Earth-Moon barycentre (EM_BARY,
+    // gravity.rs:137-142), MASSES 5-9
+    {
+        const int from_masses[9] = {0, 1, 2, -1, 5, 6, 7, 8, 9};
+        for (int k = 0; k < 9; ++k) {
+            if (from_masses[k] >= 0) {
+                const GravEntry& e = MASSES[from_masses[k]];
+                t.simple_mass[k] = e.mass_ratio == 1.0 ? GMS : e.mass_ratio * GMS;
+                t.simple_radius[k] = e.radius;
+                t.simple_kind[k] = e.kind;
+                t.simple_naif[k] = (int32_t)e.id;
+            } else {
+                t.simple_mass[k] = (3.00348961546514e-06 + 3.69430335010988e-08) * GMS;
+                t.simple_radius[k] = 385000.0 / AU_KM;
+                t.simple_kind[k] = FK_PLAIN;
+                t.simple_naif[k] = 3;
+            }
+        }
+    }
     // a(tau) = a0 + sum_k b_k tau^(k+1) over the previous step, re-expanded about its end
     // with the new step's scale q: b'_m = q^(m+1) sum_{k>=m} C(k+1, m+1) b_k
     for (int m = 0; m < 7; ++m)
@@ -1087,6 +1106,74 @@ int kete_b200_propagate_n_body_adjoint(int64_t n, int n_epochs, const double* ep
         return rc;
     a.rec = (double*)rec;
     if ((rc = launch_sens_backward(a, st))) return rc;
+    return S.finish();
+}
+
+int kete_b200_propagate_n_body_long(int64_t n, const double* pos, const double* vel, double jd0,
+                                    double jd1, const double* planets, const double* nongrav,
+                                    int batch_size, double* out_pos, double* out_vel,
+                                    double* out_planets, int32_t* status, int on_device,
+                                    void* stream) {
+    if (n < 0 || batch_size < 1 || batch_size > 55)
+        return set_error(KETE_B200_E_ARGUMENT, "need n >= 0 and a batch size of 1 to 55");
+    if (n > 0 && (!pos || !vel || !out_pos || !out_vel || !status))
+        return set_error(KETE_B200_E_ARGUMENT, "null array");
+    if (!std::isfinite(jd0) || !std::isfinite(jd1))
+        return set_error(KETE_B200_E_ARGUMENT, "epochs must be finite");
+    std::lock_guard<std::mutex> lk(g_mu);
+    DevState* ds;
+    int rc = ensure_device(ds);
+    if (rc) return rc;
+    if (n == 0) return 0;
+    cudaStream_t st = (cudaStream_t)stream;
+    Stager S{*ds, st, on_device};
+    LongArgs a;
+    std::memset(&a, 0, sizeof a);
+    a.n = n;
+    a.pos = S.in(pos, 3 * (size_t)n);
+    a.vel = S.in(vel, 3 * (size_t)n);
+    a.jd0 = jd0;
+    a.jd1 = jd1;
+    a.nongrav = S.in(nongrav, 10 * (size_t)n);
+    a.batch = batch_size;
+    a.out_pos = S.out(out_pos, 3 * (size_t)n);
+    a.out_vel = S.out(out_vel, 3 * (size_t)n);
+    a.out_planets = S.out(out_planets, 54);
+    a.status = S.out(status, (size_t)n);
+    a.max_loops = 1 << 24;
+    if (planets) {
+        a.planets = S.in(planets, 54);
+    } else {
+        // SpkCollection::try_get_state(id, jd0, 10, Equatorial) for the nine bodies
+        // (mod.rs:166-176), on the device, into library scratch
+        if (!g_eph.loaded) return set_error(KETE_B200_E_NO_EPHEMERIS, "no SPK loaded");
+        static const int64_t ids[9] = {10, 1, 2, 3, 4, 5, 6, 7, 8};
+        CenterChain ch;
+        if ((rc = center_chain(10, ch))) return rc;
+        void *pl = nullptr, *pst = nullptr, *pjd = nullptr;
+        if ((rc = staging(*ds, 36, 54 * sizeof(double), &pl)) ||
+            (rc = staging(*ds, 37, 9 * sizeof(int32_t), &pst)) ||
+            (rc = staging(*ds, 38, sizeof(double), &pjd)))
+            return rc;
+        if ((rc = cuda_check(cudaMemcpyAsync(pjd, &a.jd0, sizeof(double), cudaMemcpyHostToDevice, st),
+                             "copy epoch")))
+            return rc;
+        for (int k = 0; k < 9; ++k) {
+            auto it = g_slot_of.find(ids[k]);
+            if (it == g_slot_of.end())
+                return set_error(KETE_B200_E_NO_EPHEMERIS,
+                                 "Object (" + std::to_string(ids[k]) + ") does not have an SPK record");
+            if ((rc = launch_spk_states(1, it->second, (const double*)pjd, ch, FRAME_EQUATORIAL,
+                                        (double*)pl + 6 * k, (int32_t*)pst + k, st)))
+                return rc;
+        }
+        a.planets = (const double*)pl;
+        a.planet_status = (const int32_t*)pst;
+        // the epoch copy reads a host stack value: wait for it before returning
+        if ((rc = cuda_check(cudaStreamSynchronize(st), "stream synchronize"))) return rc;
+    }
+    if (S.rc) return S.rc;
+    if ((rc = launch_nbody_long(a, st))) return rc;
     return S.finish();
 }
 

@@ -48,6 +48,10 @@ struct Tables {
     double inv_diff[8][8];  // 1 / (spacing[j] - spacing[z])
     double adj_p[7][7];     // b = adj_p (E - a): divided differences, then C_MAT
     double shift_c[7][7];   // binomial C(k+1, m+1) at [m][k], k >= m: b carried to a new step
+    // SIMPLE_PLANETS (constants/gravity.rs:137-153) for the system integration:
+    // mass (GM, AU^3/day^2), radius (AU), ForceKind, NAIF id
+    double simple_mass[9], simple_radius[9];
+    int32_t simple_kind[9], simple_naif[9];
 };
 
 // LLVM's constant-exponent powi: repeated squaring, reciprocal for negative exponents.

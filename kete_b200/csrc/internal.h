@@ -116,6 +116,24 @@ struct SensArgs {
 int launch_sens_forward(const SensArgs& a, cudaStream_t stream);
 int launch_sens_backward(const SensArgs& a, cudaStream_t stream);
 
+// system integration (long.cuh): SIMPLE_PLANETS integrated with batches of test particles
+struct LongArgs {
+    int64_t n;
+    const double* pos;  // 3 x n heliocentric equatorial at jd0
+    const double* vel;
+    double jd0, jd1;
+    const double* planets;        // 9 x 6 heliocentric equatorial at jd0 (row per body)
+    const int32_t* planet_status; // 9 or null: the SPK lookups that produced planets
+    const double* nongrav;        // 10 x n or null
+    int batch;                    // test particles per batch (<= 55)
+    double* out_pos;
+    double* out_vel;
+    double* out_planets;          // 9 x 6 or null: the last batch's massive bodies
+    int32_t* status;
+    int max_loops;
+};
+int launch_nbody_long(const LongArgs& a, cudaStream_t stream);
+
 struct NeatmArgs;
 struct FovArgs;
 int launch_fov_prefilter(const FovArgs& a, cudaStream_t stream);

@@ -761,6 +761,7 @@ int launch_nbody_stm(const StmArgs& a, cudaStream_t stream) {
 }  // namespace kb
 
 #include "adjoint.cuh"
+#include "long.cuh"
 
 namespace kb {
 
@@ -776,6 +777,18 @@ int launch_sens_backward(const SensArgs& a, cudaStream_t stream) {
     const int64_t threads = a.n * SG;
     nbody_sens_backward_kernel<1><<<(unsigned)((threads + SENS_BLOCK - 1) / SENS_BLOCK), SENS_BLOCK, 0, stream>>>(a);
     return cuda_check(cudaGetLastError(), "nbody_sens_backward_kernel launch");
+}
+
+}  // namespace kb
+
+namespace kb {
+
+int launch_nbody_long(const LongArgs& a, cudaStream_t stream) {
+    if (a.n <= 0 || a.batch < 1 || a.batch > 64 - LONG_MASSIVE) return 0;  // checked by the caller
+    const int64_t n_batch = (a.n + a.batch - 1) / a.batch;
+    const int block = LONG_MASSIVE + a.batch <= 32 ? 32 : 64;
+    nbody_long_kernel<<<(unsigned)n_batch, block, 0, stream>>>(a);
+    return cuda_check(cudaGetLastError(), "nbody_long_kernel launch");
 }
 
 }  // namespace kb

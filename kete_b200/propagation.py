@@ -216,3 +216,89 @@ def propagate_n_body(states, jd, include_asteroids=False, non_gravs=None, suppre
                       f"at time {float(det['impact_jd'][k])}", file=sys.stderr)
             out[i] = State.new_nan(s.desig, jd, s.frame, s.center_id)
     return out
+
+
+SIMPLE_PLANET_IDS = (10, 1, 2, 3, 4, 5, 6, 7, 8)
+
+
+def propagate_n_body_long_arrays(pos, vel, jd0, jd1, planets=None, nongrav=None, batch_size=10):
+    """propagate_n_body_vec on arrays: pos/vel (3, n) heliocentric equatorial at jd0;
+    planets None (read from the loaded SPK) or (9, 6) heliocentric equatorial states of the
+    SIMPLE_PLANETS at jd0.  Returns (pos, vel, planets (9, 6), status), heliocentric
+    equatorial at jd1.  Host numpy arrays or torch CUDA tensors."""
+    _lib.init()
+    n = int(pos.shape[1])
+    out_p = _alloc_like(pos, (3, n), np.float64)
+    out_v = _alloc_like(pos, (3, n), np.float64)
+    out_pl = _alloc_like(pos, (9, 6), np.float64)
+    st = _alloc_like(pos, (n,), np.int32)
+    a = _lib.Args()
+    v = _lib.C.c_void_p
+    L = _lib.lib()
+    L.kete_b200_propagate_n_body_long.argtypes = [_lib.C.c_int64, v, v, _lib.C.c_double,
+                                                  _lib.C.c_double, v, v, _lib.C.c_int, v, v, v,
+                                                  v, _lib.C.c_int, v]
+    args = [a.ptr(pos), a.ptr(vel), float(jd0), float(jd1), a.ptr(planets), a.ptr(nongrav),
+            int(batch_size), a.ptr(out_p), a.ptr(out_v), a.ptr(out_pl), a.ptr(st, np.int32)]
+    _lib.check(L.kete_b200_propagate_n_body_long(n, *args, a.on_device, a.stream))
+    return out_p, out_v, out_pl, st
+
+
+def propagate_n_body_long(states, jd_final, planet_states=None, non_gravs=None, batch_size=10):
+    """kete.propagate_n_body_long (src/kete/rust/propagation.rs:203-249 over
+    propagate_n_body_vec, kete_core/propagation/mod.rs:142-237): the states (one common
+    epoch, centred on the Sun) integrated together with the Sun, the planets and the
+    Earth-Moon barycentre, batch_size objects per integration.  Returns (states, planets)
+    at jd_final, heliocentric J2000 equatorial."""
+    from .state import ecliptic_to_equatorial
+
+    jd1 = _jd(jd_final)
+    states = list(states)
+    if not states:
+        return [], []
+    if non_gravs is None:
+        non_gravs = [None] * len(states)
+    non_gravs = list(non_gravs)
+    if len(non_gravs) != len(states):
+        raise ValueError("Number of non-grav models doesnt match the number of provided objects.")
+    jd0 = states[0].jd
+    n = len(states)
+    pos, vel = np.empty((3, n)), np.empty((3, n))
+    for i, s in enumerate(states):
+        if s.jd != jd0:
+            raise ValueError("All input states must have the same JD")
+        if int(s.center_id) != 10:
+            raise ValueError("Center of all states must be 10 (the Sun).")
+        p, v = np.asarray(s.pos, float), np.asarray(s.vel, float)
+        if Frames(s.frame) == Frames.Ecliptic:
+            p, v = ecliptic_to_equatorial(p), ecliptic_to_equatorial(v)
+        pos[:, i], vel[:, i] = p, v
+    planets, names = None, list(SIMPLE_PLANET_IDS)
+    if planet_states is not None:
+        planet_states = list(planet_states)
+        if len(planet_states) != len(SIMPLE_PLANET_IDS):
+            raise ValueError("Input planet states must contain the correct number of states.")
+        if planet_states[0].jd != jd0:
+            raise ValueError("Planet states JD must match JD of input state.")
+        planets = np.empty((9, 6))
+        for k, ps in enumerate(planet_states):
+            p, v = np.asarray(ps.pos, float), np.asarray(ps.vel, float)
+            if Frames(ps.frame) == Frames.Ecliptic:
+                p, v = ecliptic_to_equatorial(p), ecliptic_to_equatorial(v)
+            planets[k, :3], planets[k, 3:] = p, v
+        names = [ps.desig for ps in planet_states]
+    ng = None
+    if any(m is not None for m in non_gravs):
+        ng = np.zeros((10, n))
+        for i, m in enumerate(non_gravs):
+            if m is not None:
+                ng[:, i] = m.row
+    p, v, pl, st = propagate_n_body_long_arrays(pos, vel, jd0, jd1, planets, ng, batch_size)
+    bad = np.nonzero(st != 0)[0]
+    if bad.size:
+        raise _status_error(st[bad[0]], f"propagation of {states[bad[0]].desig!r} failed")
+    out = [State(s.desig, jd1, p[:, i], v[:, i], Frames.Equatorial, 10)
+           for i, s in enumerate(states)]
+    planets_out = [State(names[k], jd1, pl[k, :3], pl[k, 3:], Frames.Equatorial, 10)
+                   for k in range(9)]
+    return out, planets_out

@@ -1479,6 +1479,232 @@ void ko_fov_check_visible_kind(const double obs7[7], const double nrm[12], int k
 }
 
 /* ------------------------------------------------------------------------------------------
+ * propagate_n_body_vec (kete_core/propagation/mod.rs:142-237) with vec_accel
+ * (acceleration.rs:197-249): the massive bodies of SIMPLE_PLANETS (constants/gravity.rs:
+ * 137-153) integrated together with a batch of test particles by one Radau integration over
+ * all their coordinates (radau.rs:160-346 on a DVector).
+ * ---------------------------------------------------------------------------------------- */
+#define N_SIMPLE 9
+static const int64_t SIMPLE_IDS[N_SIMPLE] = {10, 1, 2, 3, 4, 5, 6, 7, 8};
+
+static void simple_params(grav_params out[N_SIMPLE]) {
+    const int from_masses[N_SIMPLE] = {0, 1, 2, -1, 5, 6, 7, 8, 9};
+    for (int k = 0; k < N_SIMPLE; ++k) {
+        if (from_masses[k] >= 0) {
+            out[k] = MASSES[from_masses[k]];
+        } else { /* EM_BARY (gravity.rs:137-142) */
+            out[k].naif_id = 3;
+            out[k].mass = (3.00348961546514e-06 + 3.69430335010988e-08) * GMS;
+            out[k].radius = 385000.0 / AU_KM;
+        }
+    }
+}
+
+typedef struct {
+    int m;                     /* bodies: N_SIMPLE massive, then the test particles */
+    const double *ng;          /* 10 rows per test particle (row-major per particle) or NULL */
+    grav_params gp[N_SIMPLE];
+} vec_meta;
+
+/* vec_accel: every body feels every massive body but itself; the comet / dust model acts
+ * relative to the Sun on test particles after the first of the batch (the reference's
+ * `idx > n_massive`, acceleration.rs:239-240, skips the first one). */
+static int vec_accel(double t, const double *x, const double *v, const vec_meta *m, int exact,
+                     double *out) {
+    (void)t;
+    for (int i = 0; i < m->m; ++i) {
+        double acc[3] = {0.0, 0.0, 0.0};
+        for (int k = 0; k < N_SIMPLE; ++k) {
+            if (i == k) continue;
+            double rp[3], rv[3], w[3] = {0.0, 0.0, 0.0};
+            for (int c = 0; c < 3; ++c) {
+                rp[c] = x[3 * i + c] - x[3 * k + c];
+                rv[c] = v[3 * i + c] - v[3 * k + c];
+            }
+            if (exact && norm3(rp) <= m->gp[k].radius) return KO_IMPACT;
+            grav_add(&m->gp[k], w, rp, rv);
+            if (m->gp[k].naif_id == 10 && i > N_SIMPLE && m->ng) {
+                const double *ng = m->ng + 10 * (i - N_SIMPLE);
+                if ((int)ng[0] != 0) nongrav_add(ng, w, rp, rv);
+            }
+            for (int c = 0; c < 3; ++c) acc[c] += w[c];
+        }
+        memcpy(out + 3 * i, acc, sizeof acc);
+    }
+    return KO_OK;
+}
+
+/* RadauIntegrator::integrate / step (radau.rs:160-346) over d coordinates */
+static int radau_vec(int d, double *x, double *v, double t0, double tf, const vec_meta *m) {
+    radau_init();
+    double *a = calloc((size_t)d, sizeof(double)), *ev = calloc((size_t)d, sizeof(double));
+    double *xs = calloc((size_t)d, sizeof(double)), *vs = calloc((size_t)d, sizeof(double));
+    double *b = calloc((size_t)d * 7, sizeof(double)), *g = calloc((size_t)d * 7, sizeof(double));
+    double *b6_old = calloc((size_t)d, sizeof(double));
+    double t = t0;
+    int rc = vec_accel(t, x, v, m, 1, a);
+    if (rc) goto done;
+    if (fabs(tf - t0) < 1e-10) goto done;
+    double h = copysign(0.1, tf - t);
+    int failures = 0;
+    for (;;) {
+        if (fabs(t - tf) <= fabs(h)) h = tf - t;
+        /* one step */
+        int converged = 0;
+        double next_h = h;
+        memset(g, 0, (size_t)d * 7 * sizeof(double));
+        memcpy(ev, a, (size_t)d * sizeof(double));
+        for (int iter = 0; iter < 10 && !converged; ++iter) {
+            for (int q = 0; q < d; ++q) b6_old[q] = b[7 * q + 6];
+            for (int j = 1; j < 8; ++j) {
+                double f = GR_SPACING[j];
+                for (int q = 0; q < d; ++q) {
+                    double bw = 0.0, bu = 0.0;
+                    for (int k = 0; k < 7; ++k) bw = W_POW[j][k] * b[7 * q + k] + bw;
+                    for (int k = 0; k < 7; ++k) bu = U_POW[j][k] * b[7 * q + k] + bu;
+                    xs[q] = x[q] + f * v[q] * h + FRAC2[j] * ko_powi(h, 2) * (a[q] / 2.0 + bw);
+                    vs[q] = v[q] + f * h * (a[q] + bu);
+                }
+                rc = vec_accel(t + f * h, xs, vs, m, 0, ev);
+                if (rc) goto done;
+                for (int q = 0; q < d; ++q) {
+                    double gk = (ev[q] - a[q]) / f;
+                    for (int z = 1; z < j; ++z) gk = (gk - g[7 * q + z - 1]) / (f - GR_SPACING[z]);
+                    g[7 * q + j - 1] = gk;
+                }
+            }
+            for (int q = 0; q < d; ++q)
+                for (int jj = 0; jj < 7; ++jj) {
+                    double acc = 0.0;
+                    int first = 1;
+                    for (int k = 0; k < 7; ++k) {
+                        double tt = C_MAT[k][jj] * g[7 * q + k];
+                        if (first) {
+                            acc = tt;
+                            first = 0;
+                        } else
+                            acc = tt + acc;
+                    }
+                    b[7 * q + jj] = acc;
+                }
+            double ratio = 0.0, fem_max = 0.0, b6_max = 0.0;
+            for (int q = 0; q < d; ++q) {
+                double fem = fabs(ev[q]) + 1e-6;
+                double r = fabs(b[7 * q + 6] - b6_old[q]) / fem;
+                if (r > ratio) ratio = r;
+                if (fem > fem_max) fem_max = fem;
+                if (fabs(b[7 * q + 6]) > b6_max) b6_max = fabs(b[7 * q + 6]);
+            }
+            if (ratio < 1e-14) {
+                for (int q = 0; q < d; ++q) {
+                    double dw = 0.0, du = 0.0;
+                    for (int k = 0; k < 7; ++k) dw = dw + b[7 * q + k] * W_VEC[k];
+                    for (int k = 0; k < 7; ++k) du = du + b[7 * q + k] * U_VEC[k];
+                    x[q] += v[q] * h + ko_powi(h, 2) * (a[q] * 0.5 + dw);
+                    v[q] += h * (a[q] + du);
+                }
+                t += h;
+                rc = vec_accel(t, x, v, m, 1, a);
+                if (rc) goto done;
+                next_h = h * clampd(pow(1e-6 * fem_max / b6_max, 1.0 / 7.0), 0.25, 4.0);
+                converged = 1;
+            }
+        }
+        if (converged) {
+            h = next_h;
+            if (fabs(t - tf) < 1e-12) break;
+            failures = 0;
+        } else {
+            failures += 1;
+            h *= 0.7;
+            if (failures > 10) {
+                rc = KO_CONVERGENCE;
+                goto done;
+            }
+        }
+        if (fabs(h) < 0.005) h = copysign(0.005, h);
+    }
+    rc = KO_OK;
+done:
+    free(a);
+    free(ev);
+    free(xs);
+    free(vs);
+    free(b);
+    free(g);
+    free(b6_old);
+    return rc;
+}
+
+/* n objects (heliocentric equatorial, 3 x n SoA) at jd0 to jd1 in batches of batch_size,
+ * each with the 9 massive bodies (planets: 9 x 6 row-major heliocentric equatorial states
+ * at jd0, or NULL to read them from the loaded SPK); ng 10 x n or NULL.  out_planets
+ * (9 x 6, may be NULL) receives the massive bodies of the last batch.  status[i] is the
+ * failure of object i's batch. */
+int ko_propagate_n_body_vec(int64_t n, const double *pos, const double *vel, double jd0,
+                            double jd1, const double *planets, const double *ng, int batch_size,
+                            double *out_pos, double *out_vel, double *out_planets,
+                            int32_t *status, int n_threads) {
+    if (batch_size < 1) return KO_VALUE_ERROR;
+    double p0[N_SIMPLE * 6];
+    for (int k = 0; k < N_SIMPLE; ++k) {
+        if (planets) {
+            memcpy(p0 + 6 * k, planets + 6 * k, 6 * sizeof(double));
+        } else {
+            ko_state st;
+            int rc = get_state(SIMPLE_IDS[k], jd0, 10, KO_FRAME_EQUATORIAL, &st);
+            if (rc) return rc;
+            memcpy(p0 + 6 * k, st.pos, 3 * sizeof(double));
+            memcpy(p0 + 6 * k + 3, st.vel, 3 * sizeof(double));
+        }
+    }
+    const int64_t n_batch = (n + batch_size - 1) / batch_size;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(n_threads > 0 ? n_threads : omp_get_max_threads())
+    for (int64_t bi = 0; bi < n_batch; ++bi) {
+        const int64_t i0 = bi * batch_size;
+        const int nb = (int)((n - i0) < batch_size ? (n - i0) : batch_size);
+        const int mm = N_SIMPLE + nb, d = 3 * mm;
+        double *x = malloc((size_t)d * sizeof(double)), *v = malloc((size_t)d * sizeof(double));
+        double *ngb = ng ? malloc((size_t)10 * nb * sizeof(double)) : NULL;
+        for (int k = 0; k < N_SIMPLE; ++k)
+            for (int c = 0; c < 3; ++c) {
+                x[3 * k + c] = p0[6 * k + c];
+                v[3 * k + c] = p0[6 * k + 3 + c];
+            }
+        for (int q = 0; q < nb; ++q)
+            for (int c = 0; c < 3; ++c) {
+                x[3 * (N_SIMPLE + q) + c] = pos[c * n + i0 + q];
+                v[3 * (N_SIMPLE + q) + c] = vel[c * n + i0 + q];
+            }
+        if (ngb)
+            for (int q = 0; q < nb; ++q)
+                for (int r = 0; r < 10; ++r) ngb[10 * q + r] = ng[r * n + i0 + q];
+        vec_meta m;
+        m.m = mm;
+        m.ng = ngb;
+        simple_params(m.gp);
+        int rc = radau_vec(d, x, v, jd0, jd1, &m);
+        for (int q = 0; q < nb; ++q) {
+            status[i0 + q] = rc;
+            for (int c = 0; c < 3; ++c) {
+                out_pos[c * n + i0 + q] = rc ? NAN : x[3 * (N_SIMPLE + q) + c] - x[c];
+                out_vel[c * n + i0 + q] = rc ? NAN : v[3 * (N_SIMPLE + q) + c] - v[c];
+            }
+        }
+        if (out_planets && bi == n_batch - 1)
+            for (int k = 0; k < N_SIMPLE; ++k)
+                for (int c = 0; c < 3; ++c) {
+                    out_planets[6 * k + c] = x[3 * k + c] - x[c];
+                    out_planets[6 * k + 3 + c] = v[3 * k + c] - v[c];
+                }
+        free(x);
+        free(v);
+        free(ngb);
+    }
+    return KO_OK;
+}
+
+/* ------------------------------------------------------------------------------------------
  * flux (kete_core/flux/reflected.rs:23-34,255-326, common.rs:139-256, neatm.rs:19-185,
  * shapes.rs:42-66, sun.rs:64-75, constants/wise.rs:9-85)
  * ---------------------------------------------------------------------------------------- */

@@ -50,6 +50,10 @@ int ko_radau_central(const double pos[3], const double vel[3], double t0, double
                      double out_pos[3], double out_vel[3]);
 
 /* ---- SPK ---------------------------------------------------------------------------- */
+int ko_propagate_n_body_vec(int64_t n, const double *pos, const double *vel, double jd0,
+                            double jd1, const double *planets, const double *ng, int batch_size,
+                            double *out_pos, double *out_vel, double *out_planets,
+                            int32_t *status, int n_threads);
 int ko_spk_reset(void);
 int ko_spk_load_buffer(const uint8_t *bytes, int64_t n_bytes);
 /* state of `id` wrt `center` in frame (KO_FRAME_*), like SpkCollection::try_get_state */

@@ -65,6 +65,8 @@ def lib():
         L.ko_fov_check_visible_kind.argtypes = [_dp, _dp, C.c_int, C.c_int64, _dp, _dp, _dp,
                                                 C.c_double, C.c_int, _i32p, _dp]
         L.ko_patch_contains.argtypes = [_dp, C.c_int, _dp, _dp]
+        L.ko_propagate_n_body_vec.argtypes = [C.c_int64, _dp, _dp, C.c_double, C.c_double, _dp,
+                                              _dp, C.c_int, _dp, _dp, _dp, _i32p, C.c_int]
         L.ko_hg_phase_curve_correction.argtypes = [C.c_double, C.c_double]
         L.ko_hg_phase_curve_correction.restype = C.c_double
         L.ko_hg_apparent_mag.argtypes = [_dp, _dp, C.c_double, C.c_double]
@@ -163,6 +165,25 @@ def spk_get_states(naif_id, jd, center=0, frame=FRAME_EQUATORIAL, threads=0):
     lib().ko_spk_get_states(n, naif_id, _p(jd), center, frame, _p(out), st.ctypes.data_as(_i32p),
                             threads)
     return out, st
+
+
+def propagate_n_body_vec(pos, vel, jd0, jd1, planets=None, ng=None, batch_size=10, threads=0):
+    """propagate_n_body_vec in batches: pos/vel (3, n) heliocentric equatorial at jd0;
+    planets (9, 6) or None (from the loaded SPK).  Returns out_pos, out_vel, out_planets
+    (9, 6), status."""
+    pos = np.ascontiguousarray(pos, dtype=np.float64)
+    vel = np.ascontiguousarray(vel, dtype=np.float64)
+    n = pos.shape[1]
+    pl = None if planets is None else np.ascontiguousarray(planets, dtype=np.float64).reshape(9, 6)
+    ngp = None if ng is None else np.ascontiguousarray(ng, dtype=np.float64)
+    op, ov = np.zeros((3, n)), np.zeros((3, n))
+    opl = np.zeros((9, 6))
+    st = np.zeros(n, dtype=np.int32)
+    rc = lib().ko_propagate_n_body_vec(n, _p(pos), _p(vel), jd0, jd1, _p(pl), _p(ngp), batch_size,
+                                       _p(op), _p(ov), _p(opl), st.ctypes.data_as(_i32p), threads)
+    if rc != 0:
+        raise ValueError(f"oracle propagate_n_body_vec failed ({rc})")
+    return op, ov, opl, st
 
 
 def spk_accel(t, pos, vel, include_extended=False, ng=None, exact=False):
