@@ -253,6 +253,18 @@ int kete_b200_neatm(int64_t n, const double* sun2obj, const double* sun2obs, con
                     double* hg_fluxes, double* magnitudes, double* v_mag, double* v_flux,
                     int on_device, void* stream);
 
+/* FrmParams::apparent_total_flux (src/kete_core/src/flux/frm.rs:60-130): the fast rotating
+ * model, as kete_b200_neatm but with the beaming parameter fixed to pi and facet
+ * temperatures that depend on the facet's latitude only (frm_facet_temperature,
+ * frm.rs:15-30). */
+int kete_b200_frm(int64_t n, const double* sun2obj, const double* sun2obs, const double* h_mag,
+                  const double* g_param, const double* diam, const double* vis_albedo,
+                  const double* emissivity, int n_bands, const double* band_wavelength,
+                  const double* band_albedos, const double* sun_correction,
+                  const double* zero_mags, int wise_color_correction, double* fluxes,
+                  double* thermal_fluxes, double* hg_fluxes, double* magnitudes, double* v_mag,
+                  double* v_flux, int on_device, void* stream);
+
 /* --- allocation-free variant (no counterpart in the reference) ---------------------------
  * kete_b200_propagate_n_body on the persistent lane-group grid, for callers that must not
  * have device memory allocated or freed during the call: cudaMalloc/cudaFree synchronize

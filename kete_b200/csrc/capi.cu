@@ -103,7 +103,7 @@ static bool mda_records_valid(const HostSeg& seg) {
 struct DevState {
     int version = -1;       // ephemeris version resident on this device
     bool tables = false;
-    double* facets = nullptr;  // NEATM shape: 2048 unit normals, 3 x 2048
+    double* facets = nullptr;  // thermal-model shape: 2048 unit normals, cos/sin latitude, 5 x 2048
     double* pool = nullptr;
     size_t pool_cap = 0;
     // grow-only staging buffers for host-pointer calls
@@ -532,13 +532,18 @@ static int ensure_tables(DevState& ds) {
     {
         const double TAUD = 6.283185307179586, GOLDEN_RATIO = 1.618033988749894, EPS = 0.36;
         const double nf = (double)N_FACETS;
-        std::vector<double> f(3 * N_FACETS);
+        std::vector<double> f(5 * N_FACETS);
         for (int idx = 0; idx < N_FACETS; ++idx) {
             const double theta = TAUD * (double)idx / GOLDEN_RATIO;
             const double phi = std::acos(1.0 - 2.0 * ((double)idx + EPS) / (nf - 1.0 + 2.0 * EPS));
             f[idx] = std::cos(theta) * std::sin(phi);
             f[N_FACETS + idx] = std::sin(theta) * std::sin(phi);
             f[2 * N_FACETS + idx] = std::cos(phi);
+            // cos and sin of the facet latitude for the FRM: the host's asin, as frm.rs:26
+            // evaluates it
+            const double lat = std::asin(f[2 * N_FACETS + idx]);
+            f[3 * N_FACETS + idx] = std::cos(lat);
+            f[4 * N_FACETS + idx] = std::sin(lat);
         }
         if ((rc = cuda_check(cudaMalloc(&ds.facets, f.size() * sizeof(double)), "cudaMalloc facets")))
             return rc;
@@ -912,22 +917,27 @@ int kete_b200_hg_apparent_mag(int64_t n, const double* sun2obj, const double* su
     return S.finish();
 }
 
-int kete_b200_neatm(int64_t n, const double* sun2obj, const double* sun2obs, const double* h_mag,
-                    const double* g_param, const double* diam, const double* vis_albedo,
-                    const double* beaming, const double* emissivity, int n_bands,
-                    const double* band_wavelength, const double* band_albedos,
-                    const double* sun_correction, const double* zero_mags,
-                    int wise_color_correction, double* fluxes, double* thermal_fluxes,
-                    double* hg_fluxes, double* magnitudes, double* v_mag, double* v_flux,
-                    int on_device, void* stream) {
+}  // extern "C"
+
+namespace kb {
+
+// NEATM (model 0) and FRM (model 1) share the facet sum; FRM ignores beaming.
+static int thermal_model(int model, int64_t n, const double* sun2obj, const double* sun2obs,
+                         const double* h_mag, const double* g_param, const double* diam,
+                         const double* vis_albedo, const double* beaming,
+                         const double* emissivity, int n_bands, const double* band_wavelength,
+                         const double* band_albedos, const double* sun_correction,
+                         const double* zero_mags, int wise_color_correction, double* fluxes,
+                         double* thermal_fluxes, double* hg_fluxes, double* magnitudes,
+                         double* v_mag, double* v_flux, int on_device, void* stream) {
     if (n_bands < 1 || n_bands > MAX_BANDS)
         return set_error(KETE_B200_E_ARGUMENT, "n_bands must be 1..8");
     if (!band_wavelength || !sun_correction) return set_error(KETE_B200_E_ARGUMENT, "null band table");
     if (wise_color_correction && n_bands != 4)
         return set_error(KETE_B200_E_ARGUMENT, "WISE colour correction needs the 4 WISE bands");
     if (n < 0 || (n > 0 && (!sun2obj || !sun2obs || !h_mag || !g_param || !diam || !vis_albedo ||
-                            !beaming || !emissivity || !band_albedos || !fluxes || !thermal_fluxes ||
-                            !hg_fluxes || !v_mag || !v_flux)))
+                            (model == 0 && !beaming) || !emissivity || !band_albedos || !fluxes ||
+                            !thermal_fluxes || !hg_fluxes || !v_mag || !v_flux)))
         return set_error(KETE_B200_E_ARGUMENT, "null array");
     std::lock_guard<std::mutex> lk(g_mu);
     DevState* ds;
@@ -936,12 +946,18 @@ int kete_b200_neatm(int64_t n, const double* sun2obj, const double* sun2obs, con
     cudaStream_t st = (cudaStream_t)stream;
     NeatmArgs a;
     std::memset(&a, 0, sizeof a);
+    a.model = model;
     a.n = n;
     a.n_bands = n_bands;
     for (int b = 0; b < n_bands; ++b) {
         a.wavelength[b] = band_wavelength[b];
         a.sun_correction[b] = sun_correction[b];
         a.zero_mag[b] = zero_mags ? zero_mags[b] : 0.0;
+        // black_body_flux's per-band constants (common.rs:139-154); bands below 10 nm
+        // give no thermal flux
+        const double wl_um = band_wavelength[b] * 1e-3;
+        a.bb_k[b] = 1.43877688e4 / wl_um;
+        a.bb_coef[b] = band_wavelength[b] < 10.0 ? 0.0 : 397.289171e17 / ((wl_um * wl_um) * wl_um);
     }
     a.have_zero_mags = zero_mags ? 1 : 0;
     a.wise_cc = wise_color_correction ? 1 : 0;
@@ -954,7 +970,7 @@ int kete_b200_neatm(int64_t n, const double* sun2obj, const double* sun2obs, con
     a.g_param = S.in(g_param, (size_t)n);
     a.diam = S.in(diam, (size_t)n);
     a.vis_albedo = S.in(vis_albedo, (size_t)n);
-    a.beaming = S.in(beaming, (size_t)n);
+    a.beaming = model == 0 ? S.in(beaming, (size_t)n) : nullptr;
     a.emissivity = S.in(emissivity, (size_t)n);
     a.band_albedo = S.in(band_albedos, (size_t)n_bands * n);
     a.fluxes = S.out(fluxes, (size_t)n_bands * n);
@@ -966,6 +982,37 @@ int kete_b200_neatm(int64_t n, const double* sun2obj, const double* sun2obs, con
     if (S.rc) return S.rc;
     if ((rc = launch_neatm(a, st))) return rc;
     return S.finish();
+}
+
+}  // namespace kb
+
+extern "C" {
+
+int kete_b200_neatm(int64_t n, const double* sun2obj, const double* sun2obs, const double* h_mag,
+                    const double* g_param, const double* diam, const double* vis_albedo,
+                    const double* beaming, const double* emissivity, int n_bands,
+                    const double* band_wavelength, const double* band_albedos,
+                    const double* sun_correction, const double* zero_mags,
+                    int wise_color_correction, double* fluxes, double* thermal_fluxes,
+                    double* hg_fluxes, double* magnitudes, double* v_mag, double* v_flux,
+                    int on_device, void* stream) {
+    return kb::thermal_model(0, n, sun2obj, sun2obs, h_mag, g_param, diam, vis_albedo, beaming,
+                             emissivity, n_bands, band_wavelength, band_albedos, sun_correction,
+                             zero_mags, wise_color_correction, fluxes, thermal_fluxes, hg_fluxes,
+                             magnitudes, v_mag, v_flux, on_device, stream);
+}
+
+int kete_b200_frm(int64_t n, const double* sun2obj, const double* sun2obs, const double* h_mag,
+                  const double* g_param, const double* diam, const double* vis_albedo,
+                  const double* emissivity, int n_bands, const double* band_wavelength,
+                  const double* band_albedos, const double* sun_correction,
+                  const double* zero_mags, int wise_color_correction, double* fluxes,
+                  double* thermal_fluxes, double* hg_fluxes, double* magnitudes, double* v_mag,
+                  double* v_flux, int on_device, void* stream) {
+    return kb::thermal_model(1, n, sun2obj, sun2obs, h_mag, g_param, diam, vis_albedo, nullptr,
+                             emissivity, n_bands, band_wavelength, band_albedos, sun_correction,
+                             zero_mags, wise_color_correction, fluxes, thermal_fluxes, hg_fluxes,
+                             magnitudes, v_mag, v_flux, on_device, stream);
 }
 
 int kete_b200_propagate_n_body_stm(int64_t n, const double* pos, const double* vel,

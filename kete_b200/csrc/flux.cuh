@@ -3,7 +3,7 @@
 // Restates kete_core/flux/reflected.rs:23-34 (hg_phase_curve_correction), 255-268
 // (HGParams::apparent_mag), 295-326 (apparent_flux); flux/common.rs:139-154 (black_body_flux),
 // 192-208 (lambertian_vis_scale_factor), 220-236 (sub_solar_temperature), 254-256
-// (flux_to_mag); flux/neatm.rs:19-29, 85-185 (NEATM); flux/sun.rs:64-75
+// (flux_to_mag); flux/neatm.rs:19-29, 85-185 (NEATM); flux/frm.rs:15-130 (FRM); flux/sun.rs:64-75
 // (solar_flux_black_body); constants/wise.rs:24-78 (WISE colour corrections).
 #pragma once
 #include "common.cuh"
@@ -100,6 +100,7 @@ __device__ __forceinline__ double wise_color_correction(int band, double temp) {
 }
 
 struct NeatmArgs {
+    int model;  // 0 NEATM (neatm.rs), 1 FRM (frm.rs: beaming pi, latitude-only temperatures)
     int64_t n;
     const double* sun2obj;  // 3 x n
     const double* sun2obs;  // 3 x n
@@ -113,10 +114,13 @@ struct NeatmArgs {
     double wavelength[MAX_BANDS];
     double sun_correction[MAX_BANDS];
     double zero_mag[MAX_BANDS];
+    double bb_k[MAX_BANDS];     // black body: exponent numerator 1.43877688e4 / wavelength_um
+    double bb_coef[MAX_BANDS];  // 397.289171e17 / wavelength_um^3; 0 when wavelength < 10 nm
     int have_zero_mags;
     int wise_cc;
     const double* band_albedo;  // n_bands x n
-    const double* facets;       // 3 x N_FACETS (unit normals)
+    const double* facets;       // 5 x N_FACETS: unit normals x, y, z; cos and sin of the
+                                // latitude asin(z)
     double facet_area;
     double* fluxes;             // n_bands x n
     double* thermal;            // n_bands x n

@@ -398,63 +398,149 @@ int launch_hg_mag(int64_t n, const double* s2obj, const double* s2obs, const dou
 }
 
 // -------------------------------------------------------------------------------------------
-// NEATM total flux (NeatmParams::apparent_total_flux, flux/neatm.rs:143-185): one warp per
-// geometry, the 2048 facets strided over the lanes, band sums reduced across the warp.
+// NEATM and FRM total flux (NeatmParams / FrmParams::apparent_total_flux, flux/neatm.rs:143-185,
+// flux/frm.rs:137-185).  One warp per geometry.  A facet adds to the thermal sum only when
+// the observer sees it and its temperature is above black_body_flux's 30 K floor
+// (common.rs:139-154), and on a sphere that is a scattered half or less of the 2048 facets.
+// So the warp first tests 32 facets at a time (two dot products), appends the survivors'
+// (cos, seen) pairs to a per-warp queue in shared memory, and evaluates the black bodies
+// only in full 32-facet batches: every lane busy on the exp-heavy part.  Band sums are
+// reduced across the warp at the end.
 // -------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) neatm_kernel(NeatmArgs a) {
-    const int lane = threadIdx.x & 31;
-    const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (i >= a.n) return;
-    const int64_t n = a.n;
-    const double s2obj[3] = {a.sun2obj[i], a.sun2obj[n + i], a.sun2obj[2 * n + i]};
-    const double s2obs[3] = {a.sun2obs[i], a.sun2obs[n + i], a.sun2obs[2 * n + i]};
-    const double g = a.g_param[i], diam = a.diam[i], emis = a.emissivity[i];
-    const double obj2sun[3] = {-s2obj[0], -s2obj[1], -s2obj[2]};
-    const double obs2obj[3] = {s2obj[0] - s2obs[0], s2obj[1] - s2obs[1], s2obj[2] - s2obs[2]};
-    const double obs2obj_r = norm3(obs2obj[0], obs2obj[1], obs2obj[2]);
-    // sub_solar_temperature (common.rs:220-236)
-    const double phase_integral = 0.29 + 0.684 * g;
-    const double bond_albedo = a.vis_albedo[i] * phase_integral;
-    const double r2 = obj2sun[0] * obj2sun[0] + obj2sun[1] * obj2sun[1] + obj2sun[2] * obj2sun[2];
-    const double reflected = (1.0 - bond_albedo) * SOLAR_FLUX / r2;
-    double ss_temp = reflected / (a.beaming[i] * emis * STEFAN_BOLTZMANN);
-    ss_temp = ss_temp <= 0.0 ? 0.0 : sqrt(sqrt(ss_temp));
-    const double ns = norm3(obj2sun[0], obj2sun[1], obj2sun[2]);
-    const double o2s[3] = {obj2sun[0] / ns, obj2sun[1] / ns, obj2sun[2] / ns};
-    const double o2o[3] = {obs2obj[0] / obs2obj_r, obs2obj[1] / obs2obj_r, obs2obj[2] / obs2obj_r};
-    const double dscale = obs2obj_r * AU_KM / diam;
-    const double scale = 1.0 / (dscale * dscale);  // powi(-2), common.rs:200
-    double th[MAX_BANDS];
-#pragma unroll
-    for (int b = 0; b < MAX_BANDS; ++b) th[b] = 0.0;
-    for (int f = lane; f < N_FACETS; f += 32) {
-        const double nx = __ldg(a.facets + f), ny = __ldg(a.facets + N_FACETS + f),
-                     nz = __ldg(a.facets + 2 * N_FACETS + f);
-        const double tmp = nx * o2s[0] + ny * o2s[1] + nz * o2s[2];
-        const double temp = tmp > 0.0 ? sqrt(sqrt(tmp)) * ss_temp : 0.0;
-        const double observed = -(nx * o2o[0] + ny * o2o[1] + nz * o2o[2]);
-        const double sc = observed > 0.0 ? observed * emis * PI * scale : 0.0;
-        if (temp == 0.0 || sc == 0.0) continue;
-#pragma unroll
-        for (int b = 0; b < MAX_BANDS; ++b) {
-            if (b < a.n_bands) {
-                double ff = black_body_flux(temp, a.wavelength[b]);
-                if (a.wise_cc) ff *= wise_color_correction(b, temp);
-                ff *= a.facet_area;
-                th[b] += sc * ff;
-            }
-        }
+constexpr int THERMAL_WARPS = 4;
+
+// Black-body sum of one surviving facet into th[]: temperature from the cos term, then per
+// band coef / (exp(k / T) - 1) (common.rs:139-154) with the WISE colour correction folded
+// into the same division (constants/wise.rs:40-85).
+template <int NB, bool CC>
+__device__ __forceinline__ void thermal_facet(const NeatmArgs& a, double tmp, double seen,
+                                              double ss_temp, double (&th)[NB]) {
+    const double temp = sqrt(sqrt(tmp)) * ss_temp;
+    if (!(temp >= 30.0)) return;
+    const double inv_t = 1.0 / temp;
+    double t = 0.0, t2 = 0.0, t3 = 0.0, t4 = 0.0, w4 = 0.0;
+    if (CC) {
+        t = clampd(temp, 100.0, 400.0);
+        t2 = t * t;
+        t3 = t * t2;
+        t4 = t2 * t2;
+        const double l = log(t), l2 = l * l;
+        w4 = 2.17247804e+01 + -1.46084733e+01 * l + 3.85364000e+00 * l2 -
+             4.51512551e-01 * (l * l2) + 1.98397252e-02 * (l2 * l2);
     }
 #pragma unroll
-    for (int b = 0; b < MAX_BANDS; ++b)
+    for (int b = 0; b < NB; ++b) {
+        if (b >= a.n_bands || a.bb_coef[b] == 0.0) continue;
+        const double em1 = exp(a.bb_k[b] * inv_t) - 1.0;
+        double ff;
+        if (CC && b == 0)
+            ff = a.bb_coef[b] / (em1 * (-3.78226591e-01 + 3.50431748e-03 * t + 1.45866307e-05 * t2 -
+                                        6.67674083e-08 * t3 + 7.03651986e-11 * t4));
+        else if (CC && b == 1)
+            ff = a.bb_coef[b] / (em1 * (-8.60229377e-01 + 1.54988562e-02 * t - 5.10705456e-05 * t2 +
+                                        7.68314436e-08 * t3 - 4.32238900e-11 * t4));
+        else if (CC && b == 2)
+            ff = a.bb_coef[b] / (em1 * (-1.29814355 + 2.43268763e-02 * t - 9.05178737e-05 * t2 +
+                                        1.50095351e-07 * t3 - 9.35433316e-11 * t4));
+        else if (CC)
+            ff = a.bb_coef[b] / em1 * w4;
+        else
+            ff = a.bb_coef[b] / em1;
+        th[b] += seen * ff;
+    }
+}
+
+template <int NB, bool CC>
+__global__ void __launch_bounds__(32 * THERMAL_WARPS, 8) thermal_kernel(NeatmArgs a) {
+    __shared__ double2 queue[THERMAL_WARPS][64];
+    const int lane = threadIdx.x & 31;
+    double2* q = queue[threadIdx.x >> 5];
+    const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (i >= a.n) return;  // warp-uniform
+    const int64_t n = a.n;
+    double ss_temp, o2s[3], o2o[3], cs = 0.0, sn = 0.0;
+    {
+        const double s2obj[3] = {a.sun2obj[i], a.sun2obj[n + i], a.sun2obj[2 * n + i]};
+        const double s2obs[3] = {a.sun2obs[i], a.sun2obs[n + i], a.sun2obs[2 * n + i]};
+        const double obj2sun[3] = {-s2obj[0], -s2obj[1], -s2obj[2]};
+        const double obs2obj[3] = {s2obj[0] - s2obs[0], s2obj[1] - s2obs[1], s2obj[2] - s2obs[2]};
+        const double obs2obj_r = norm3(obs2obj[0], obs2obj[1], obs2obj[2]);
+        // sub_solar_temperature (common.rs:220-236); the FRM's beaming is pi (frm.rs:95-101)
+        const double emis = a.emissivity[i];
+        const double phase_integral = 0.29 + 0.684 * a.g_param[i];
+        const double bond_albedo = a.vis_albedo[i] * phase_integral;
+        const double r2 = obj2sun[0] * obj2sun[0] + obj2sun[1] * obj2sun[1] + obj2sun[2] * obj2sun[2];
+        const double reflected = (1.0 - bond_albedo) * SOLAR_FLUX / r2;
+        const double beam = a.model == 1 ? PI : a.beaming[i];
+        ss_temp = reflected / (beam * emis * STEFAN_BOLTZMANN);
+        ss_temp = ss_temp <= 0.0 ? 0.0 : sqrt(sqrt(ss_temp));
+        const double ns = norm3(obj2sun[0], obj2sun[1], obj2sun[2]);
+        for (int c = 0; c < 3; ++c) {
+            o2s[c] = obj2sun[c] / ns;
+            o2o[c] = obs2obj[c] / obs2obj_r;
+        }
+        // FRM: cos(lat_facet - lat_sun) (frm_facet_temperature, frm.rs:19-30) expanded with
+        // the facet's cos/sin of latitude from the table
+        if (a.model == 1) {
+            const double sun_lat = asin(o2s[2]);
+            cs = cos(sun_lat);
+            sn = sin(sun_lat);
+        }
+    }
+    double th[NB];
+#pragma unroll
+    for (int b = 0; b < NB; ++b) th[b] = 0.0;
+    const unsigned below = (1u << lane) - 1u;
+    int count = 0;  // queued facets, warp-uniform
+    for (int base = 0; base < N_FACETS; base += 32) {
+        const int f = base + lane;
+        const double nx = __ldg(a.facets + f), ny = __ldg(a.facets + N_FACETS + f),
+                     nz = __ldg(a.facets + 2 * N_FACETS + f);
+        const double seen = -(nx * o2o[0] + ny * o2o[1] + nz * o2o[2]);
+        double tmp = 0.0;
+        if (seen > 0.0)
+            tmp = a.model == 1 ? __ldg(a.facets + 3 * N_FACETS + f) * cs +
+                                     __ldg(a.facets + 4 * N_FACETS + f) * sn
+                               : nx * o2s[0] + ny * o2s[1] + nz * o2s[2];
+        const bool keep = seen > 0.0 && tmp > 0.0;
+        const unsigned m = __ballot_sync(0xffffffffu, keep);
+        if (keep) q[count + __popc(m & below)] = make_double2(tmp, seen);
+        count += __popc(m);
+        if (count >= 32) {
+            __syncwarp();
+            const double2 e = q[lane];
+            thermal_facet<NB, CC>(a, e.x, e.y, ss_temp, th);
+            __syncwarp();
+            if (lane < count - 32) q[lane] = q[lane + 32];
+            __syncwarp();
+            count -= 32;
+        }
+    }
+    __syncwarp();
+    if (lane < count) {
+        const double2 e = q[lane];
+        thermal_facet<NB, CC>(a, e.x, e.y, ss_temp, th);
+    }
+    // the geometry again, from memory rather than held in registers through the loop
+    const double s2obj[3] = {a.sun2obj[i], a.sun2obj[n + i], a.sun2obj[2 * n + i]};
+    const double s2obs[3] = {a.sun2obs[i], a.sun2obs[n + i], a.sun2obs[2 * n + i]};
+    const double g = a.g_param[i], diam = a.diam[i];
+    // Lambertian scale emissivity * pi * (r / D)^-2 (common.rs:190-205) and the facet area
+    const double obs2obj_r = norm3(s2obj[0] - s2obs[0], s2obj[1] - s2obs[1], s2obj[2] - s2obs[2]);
+    const double dscale = obs2obj_r * AU_KM / diam;
+    const double sc = a.emissivity[i] * PI * (1.0 / (dscale * dscale)) * a.facet_area;
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) th[b] += __shfl_xor_sync(0xffffffffu, th[b], o);
+        th[b] *= sc;
+    }
     if (lane < a.n_bands) {
         const int b = lane;
         double thb = 0.0;
 #pragma unroll
-        for (int q = 0; q < MAX_BANDS; ++q)
-            if (q == b) thb = th[q];
+        for (int c = 0; c < NB; ++c)
+            if (c == b) thb = th[c];
         const double refl =
             hg_apparent_flux(s2obj, s2obs, g, diam, a.wavelength[b], a.band_albedo[(int64_t)b * n + i]) *
             a.sun_correction[b];
@@ -475,8 +561,17 @@ __global__ void __launch_bounds__(128) neatm_kernel(NeatmArgs a) {
 int launch_neatm(const NeatmArgs& a, cudaStream_t stream) {
     if (a.n <= 0) return 0;
     const int64_t threads = a.n * 32;
-    neatm_kernel<<<(unsigned)((threads + 127) / 128), 128, 0, stream>>>(a);
-    return cuda_check(cudaGetLastError(), "neatm_kernel launch");
+    const unsigned grid = (unsigned)((threads + 32 * THERMAL_WARPS - 1) / (32 * THERMAL_WARPS));
+    const unsigned block = 32 * THERMAL_WARPS;
+    if (a.wise_cc)  // the capi admits colour corrections only with the 4 WISE bands
+        thermal_kernel<4, true><<<grid, block, 0, stream>>>(a);
+    else if (a.n_bands <= 2)
+        thermal_kernel<2, false><<<grid, block, 0, stream>>>(a);
+    else if (a.n_bands <= 4)
+        thermal_kernel<4, false><<<grid, block, 0, stream>>>(a);
+    else
+        thermal_kernel<MAX_BANDS, false><<<grid, block, 0, stream>>>(a);
+    return cuda_check(cudaGetLastError(), "thermal_kernel launch");
 }
 
 }  // namespace kb

@@ -1,7 +1,8 @@
-"""kete.flux on the GPU: H-G apparent magnitudes and the NEATM thermal model.
+"""kete.flux on the GPU: H-G apparent magnitudes and the NEATM and FRM thermal models.
 
-``hg_apparent_mag`` mirrors src/kete/rust/flux/reflected.rs:120-132 and ``NeatmParams``
-mirrors src/kete/rust/flux/models.rs:196-365 (constructors, ``evaluate``).  Parameter
+``hg_apparent_mag`` mirrors src/kete/rust/flux/reflected.rs:120-132, ``NeatmParams``
+mirrors src/kete/rust/flux/models.rs:196-365 and ``FrmParams`` models.rs:512-690
+(constructors, ``evaluate``).  Parameter
 filling (H, diameter, albedo; HGParams::fill, kete_core/flux/reflected.rs:177-238) is host
 logic; every flux and magnitude is computed by libketeb200.so.
 """
@@ -83,13 +84,9 @@ class ModelResults:
     magnitudes: np.ndarray | None
 
 
-def neatm_arrays(sun2obj, sun2obs, h_mag, g_param, diam, vis_albedo, beaming, emissivity,
-                 band_wavelength, band_albedos, sun_correction=None, zero_mags=None,
-                 wise_color_correction=False):
-    """Batched NEATM: per-geometry parameters (n,), band_albedos (n_bands, n).
-
-    Returns dict of fluxes/thermal_fluxes/hg_fluxes/magnitudes (n_bands, n) and
-    v_band_magnitude/v_band_flux (n,)."""
+def _thermal_arrays(entry, sun2obj, sun2obs, h_mag, g_param, diam, vis_albedo, beaming,
+                    emissivity, band_wavelength, band_albedos, sun_correction, zero_mags,
+                    wise_color_correction):
     _lib.init()
     s2obj, s2obs = _vec3n(sun2obj), _vec3n(sun2obs)
     n = s2obj.shape[1]
@@ -106,23 +103,59 @@ def neatm_arrays(sun2obj, sun2obs, h_mag, g_param, diam, vis_albedo, beaming, em
     vm, vf = np.empty(n), np.empty(n)
     a = _lib.Args()
     args = [a.ptr(s2obj), a.ptr(s2obs), a.ptr(per(h_mag)), a.ptr(per(g_param)), a.ptr(per(diam)),
-            a.ptr(per(vis_albedo)), a.ptr(per(beaming)), a.ptr(per(emissivity))]
+            a.ptr(per(vis_albedo))]
+    if beaming is not None:
+        args.append(a.ptr(per(beaming)))
+    args.append(a.ptr(per(emissivity)))
     L = _lib.lib()
     v = _lib.C.c_void_p
-    L.kete_b200_neatm.argtypes = [_lib.C.c_int64] + [v] * 8 + [_lib.C.c_int, v, v, v, v,
-                                                                _lib.C.c_int] + [v] * 6 + [
+    fn = getattr(L, entry)
+    fn.argtypes = [_lib.C.c_int64] + [v] * len(args) + [_lib.C.c_int, v, v, v, v,
+                                                         _lib.C.c_int] + [v] * 6 + [
         _lib.C.c_int, v]
-    rc = L.kete_b200_neatm(n, *args, nb, bands.ctypes.data, a.ptr(alb), sc.ctypes.data,
-                           None if zm is None else zm.ctypes.data, int(bool(wise_color_correction)),
-                           a.ptr(out["fluxes"]), a.ptr(out["thermal_fluxes"]),
-                           a.ptr(out["hg_fluxes"]), a.ptr(out["magnitudes"]), a.ptr(vm),
-                           a.ptr(vf), a.on_device, a.stream)
+    rc = fn(n, *args, nb, bands.ctypes.data, a.ptr(alb), sc.ctypes.data,
+            None if zm is None else zm.ctypes.data, int(bool(wise_color_correction)),
+            a.ptr(out["fluxes"]), a.ptr(out["thermal_fluxes"]), a.ptr(out["hg_fluxes"]),
+            a.ptr(out["magnitudes"]), a.ptr(vm), a.ptr(vf), a.on_device, a.stream)
     _lib.check(rc)
     if zm is None:
         out["magnitudes"] = None
     out["v_band_magnitude"] = vm
     out["v_band_flux"] = vf
     return out
+
+
+def neatm_arrays(sun2obj, sun2obs, h_mag, g_param, diam, vis_albedo, beaming, emissivity,
+                 band_wavelength, band_albedos, sun_correction=None, zero_mags=None,
+                 wise_color_correction=False):
+    """Batched NEATM: per-geometry parameters (n,), band_albedos (n_bands, n).
+
+    Returns dict of fluxes/thermal_fluxes/hg_fluxes/magnitudes (n_bands, n) and
+    v_band_magnitude/v_band_flux (n,)."""
+    return _thermal_arrays("kete_b200_neatm", sun2obj, sun2obs, h_mag, g_param, diam,
+                           vis_albedo, beaming, emissivity, band_wavelength, band_albedos,
+                           sun_correction, zero_mags, wise_color_correction)
+
+
+def frm_arrays(sun2obj, sun2obs, h_mag, g_param, diam, vis_albedo, emissivity, band_wavelength,
+               band_albedos, sun_correction=None, zero_mags=None, wise_color_correction=False):
+    """Batched FRM (kete_core/flux/frm.rs:78-185): as ``neatm_arrays`` without beaming."""
+    return _thermal_arrays("kete_b200_frm", sun2obj, sun2obs, h_mag, g_param, diam, vis_albedo,
+                           None, emissivity, band_wavelength, band_albedos, sun_correction,
+                           zero_mags, wise_color_correction)
+
+
+def _results(r, n):
+    return [ModelResults(r["fluxes"][:, i], r["hg_fluxes"][:, i], r["thermal_fluxes"][:, i],
+                         float(r["v_band_magnitude"][i]), float(r["v_band_flux"][i]),
+                         None if r["magnitudes"] is None else r["magnitudes"][:, i])
+            for i in range(n)]
+
+
+def _geometries(sun2obj_vecs, sun2obs_vecs):
+    s2obj = np.asarray(sun2obj_vecs, dtype=np.float64).reshape(-1, 3).T
+    s2obs = np.asarray(sun2obs_vecs, dtype=np.float64).reshape(-1, 3).T
+    return s2obj, s2obs, s2obj.shape[1]
 
 
 class NeatmParams:
@@ -160,17 +193,54 @@ class NeatmParams:
         """Fluxes and magnitudes at each geometry (models.rs:347-365)."""
         if self.diam is None or self.vis_albedo is None:
             raise ValueError("NEATM needs a diameter and a visible albedo")
-        s2obj = np.asarray(sun2obj_vecs, dtype=np.float64).reshape(-1, 3).T
-        s2obs = np.asarray(sun2obs_vecs, dtype=np.float64).reshape(-1, 3).T
-        n = s2obj.shape[1]
+        s2obj, s2obs, n = _geometries(sun2obj_vecs, sun2obs_vecs)
         alb = np.repeat(np.asarray(self.band_albedos, np.float64)[:, None], n, axis=1)
         r = neatm_arrays(s2obj, s2obs, self.h_mag, self.g_param, self.diam, self.vis_albedo,
                          self.beaming, self.emissivity, self.band_wavelength, alb,
                          self.sun_correction, self.zero_mags, self.wise_color_correction)
-        out = []
-        for i in range(n):
-            out.append(ModelResults(r["fluxes"][:, i], r["hg_fluxes"][:, i],
-                                    r["thermal_fluxes"][:, i], float(r["v_band_magnitude"][i]),
-                                    float(r["v_band_flux"][i]),
-                                    None if r["magnitudes"] is None else r["magnitudes"][:, i]))
-        return out
+        return _results(r, n)
+
+
+class FrmParams:
+    """FRM parameters of one object (src/kete/rust/flux/models.rs:512-690)."""
+
+    def __init__(self, desig, band_wavelength, band_albedos, h_mag=None, diam=None,
+                 vis_albedo=None, g_param=0.15, c_hg=None, emissivity=0.9, zero_mags=None,
+                 sun_correction=None, wise_color_correction=False):
+        self.desig = desig
+        self.h_mag, self.vis_albedo, self.diam, self.c_hg = hg_fill(h_mag, vis_albedo, diam, c_hg)
+        self.band_wavelength = list(band_wavelength)
+        self.band_albedos = list(band_albedos)
+        self.g_param, self.emissivity = g_param, emissivity
+        self.zero_mags = None if zero_mags is None else list(zero_mags)
+        self.sun_correction = ([1.0] * len(self.band_wavelength) if sun_correction is None
+                               else list(sun_correction))
+        self.wise_color_correction = wise_color_correction
+
+    @staticmethod
+    def new_neos(desig, band_albedos, h_mag=None, diam=None, vis_albedo=None, g_param=0.15,
+                 c_hg=None, emissivity=0.9):
+        if len(band_albedos) != 2:
+            raise ValueError("2 Albedos must be provided, one for each NEOS band.")
+        return FrmParams(desig, NEOS_BANDS, band_albedos, h_mag, diam, vis_albedo, g_param,
+                         c_hg, emissivity, NEOS_ZERO_MAG)
+
+    @staticmethod
+    def new_wise(desig, band_albedos, h_mag=None, diam=None, vis_albedo=None, g_param=0.15,
+                 c_hg=None, emissivity=0.9):
+        if len(band_albedos) != 4:
+            raise ValueError("4 Albedos must be provided, one for each WISE band.")
+        return FrmParams(desig, WISE_BANDS_300K, band_albedos, h_mag, diam, vis_albedo, g_param,
+                         c_hg, emissivity, WISE_ZERO_MAG_300K, WISE_SUN_CORRECTION,
+                         wise_color_correction=True)
+
+    def evaluate(self, sun2obj_vecs, sun2obs_vecs):
+        """Fluxes and magnitudes at each geometry (models.rs:663-682)."""
+        if self.diam is None or self.vis_albedo is None:
+            raise ValueError("FRM needs a diameter and a visible albedo")
+        s2obj, s2obs, n = _geometries(sun2obj_vecs, sun2obs_vecs)
+        alb = np.repeat(np.asarray(self.band_albedos, np.float64)[:, None], n, axis=1)
+        r = frm_arrays(s2obj, s2obs, self.h_mag, self.g_param, self.diam, self.vis_albedo,
+                       self.emissivity, self.band_wavelength, alb, self.sun_correction,
+                       self.zero_mags, self.wise_color_correction)
+        return _results(r, n)

@@ -1706,6 +1706,7 @@ int ko_propagate_n_body_vec(int64_t n, const double *pos, const double *vel, dou
 
 /* ------------------------------------------------------------------------------------------
  * flux (kete_core/flux/reflected.rs:23-34,255-326, common.rs:139-256, neatm.rs:19-185,
+ * frm.rs:15-185,
  * shapes.rs:42-66, sun.rs:64-75, constants/wise.rs:9-85)
  * ---------------------------------------------------------------------------------------- */
 static double hg_helper(double a, double b, double c, double phase) {
@@ -1839,13 +1840,23 @@ __attribute__((constructor)) static void ko_init_tables(void) {
     ko_fib_lattice(2048, g_shape, &g_shape_area);
 }
 
-int ko_neatm_total_flux(const double sun2obj[3], const double sun2obs[3], double h_mag,
-                        double g_param, double diam, double vis_albedo, double beaming,
-                        double emissivity, int n_bands, const double *bands,
-                        const double *band_albedos, const double *sun_correction,
-                        const double *zero_mags, int wise_color_correction, double *fluxes,
-                        double *hg_fluxes, double *thermal, double *mags, double *v_mag,
-                        double *v_flux) {
+/* frm.rs:19-30: cos of the latitude difference between facet and Sun direction */
+double ko_frm_facet_temperature(const double normal[3], const double o2s[3], double sst) {
+    double tmp = cos(asin(normal[2]) - asin(o2s[2]));
+    if (tmp > 0.0) return sqrt(sqrt(tmp)) * sst;
+    return 0.0;
+}
+
+/* neatm.rs:85-185 (model 0) and frm.rs:78-185 (model 1, beaming fixed to pi) share
+ * everything but the facet temperature. */
+static int thermal_total_flux(int model, const double sun2obj[3], const double sun2obs[3],
+                              double h_mag, double g_param, double diam, double vis_albedo,
+                              double beaming, double emissivity, int n_bands,
+                              const double *bands, const double *band_albedos,
+                              const double *sun_correction, const double *zero_mags,
+                              int wise_color_correction, double *fluxes, double *hg_fluxes,
+                              double *thermal, double *mags, double *v_mag, double *v_flux) {
+    if (model == 1) beaming = PI;
     double obj2sun[3] = {-sun2obj[0], -sun2obj[1], -sun2obj[2]};
     double obs2obj[3] = {sun2obj[0] - sun2obs[0], sun2obj[1] - sun2obs[1], sun2obj[2] - sun2obs[2]};
     double obs2obj_r = norm3(obs2obj);
@@ -1856,7 +1867,8 @@ int ko_neatm_total_flux(const double sun2obj[3], const double sun2obs[3], double
     for (int b = 0; b < n_bands; ++b) thermal[b] = 0.0;
     for (int f = 0; f < 2048; ++f) {
         const double *nrm = g_shape + 3 * f;
-        double temp = ko_neatm_facet_temperature(nrm, o2s_u, ss_temp);
+        double temp = model == 1 ? ko_frm_facet_temperature(nrm, o2s_u, ss_temp)
+                                 : ko_neatm_facet_temperature(nrm, o2s_u, ss_temp);
         double sc = lambertian_vis_scale(nrm, o2o_u, obs2obj_r, diam, emissivity);
         if (temp == 0.0 || sc == 0.0) continue;
         for (int b = 0; b < n_bands; ++b) {
@@ -1877,5 +1889,61 @@ int ko_neatm_total_flux(const double sun2obj[3], const double sun2obs[3], double
     *v_flux = -2.5 * log10(*v_mag / V_MAG_ZERO); /* flux_to_mag, as neatm.rs:167 calls it */
     if (zero_mags && mags)
         for (int b = 0; b < n_bands; ++b) mags[b] = -2.5 * log10(fluxes[b] / zero_mags[b]);
+    return KO_OK;
+}
+
+int ko_neatm_total_flux(const double sun2obj[3], const double sun2obs[3], double h_mag,
+                        double g_param, double diam, double vis_albedo, double beaming,
+                        double emissivity, int n_bands, const double *bands,
+                        const double *band_albedos, const double *sun_correction,
+                        const double *zero_mags, int wise_color_correction, double *fluxes,
+                        double *hg_fluxes, double *thermal, double *mags, double *v_mag,
+                        double *v_flux) {
+    return thermal_total_flux(0, sun2obj, sun2obs, h_mag, g_param, diam, vis_albedo, beaming,
+                              emissivity, n_bands, bands, band_albedos, sun_correction,
+                              zero_mags, wise_color_correction, fluxes, hg_fluxes, thermal, mags,
+                              v_mag, v_flux);
+}
+
+int ko_frm_total_flux(const double sun2obj[3], const double sun2obs[3], double h_mag,
+                      double g_param, double diam, double vis_albedo, double emissivity,
+                      int n_bands, const double *bands, const double *band_albedos,
+                      const double *sun_correction, const double *zero_mags,
+                      int wise_color_correction, double *fluxes, double *hg_fluxes,
+                      double *thermal, double *mags, double *v_mag, double *v_flux) {
+    return thermal_total_flux(1, sun2obj, sun2obs, h_mag, g_param, diam, vis_albedo, PI,
+                              emissivity, n_bands, bands, band_albedos, sun_correction,
+                              zero_mags, wise_color_correction, fluxes, hg_fluxes, thermal, mags,
+                              v_mag, v_flux);
+}
+
+/* Many geometries of either model, (3, n) / (n_bands, n) arrays as the device entry points
+ * take them, over the host's threads (models.rs:347-365 and 663-682 evaluate in parallel). */
+int ko_thermal_batch(int model, int64_t n, const double *sun2obj, const double *sun2obs,
+                     const double *h_mag, const double *g_param, const double *diam,
+                     const double *vis_albedo, const double *beaming, const double *emissivity,
+                     int n_bands, const double *bands, const double *band_albedos,
+                     const double *sun_correction, const double *zero_mags,
+                     int wise_color_correction, double *fluxes, double *hg_fluxes,
+                     double *thermal, double *mags, double *v_mag, double *v_flux,
+                     int n_threads) {
+    if (n_bands < 1 || n_bands > 8) return KO_VALUE_ERROR;
+#pragma omp parallel for schedule(dynamic, 64) num_threads(n_threads > 0 ? n_threads : omp_get_max_threads())
+    for (int64_t i = 0; i < n; ++i) {
+        double so[3] = {sun2obj[i], sun2obj[n + i], sun2obj[2 * n + i]};
+        double sb[3] = {sun2obs[i], sun2obs[n + i], sun2obs[2 * n + i]};
+        double alb[8], fl[8], hg[8], th[8], mg[8];
+        for (int b = 0; b < n_bands; ++b) alb[b] = band_albedos[(int64_t)b * n + i];
+        thermal_total_flux(model, so, sb, h_mag[i], g_param[i], diam[i], vis_albedo[i],
+                           model == 1 ? PI : beaming[i], emissivity[i], n_bands, bands, alb,
+                           sun_correction, zero_mags, wise_color_correction, fl, hg, th, mg,
+                           v_mag + i, v_flux + i);
+        for (int b = 0; b < n_bands; ++b) {
+            fluxes[(int64_t)b * n + i] = fl[b];
+            hg_fluxes[(int64_t)b * n + i] = hg[b];
+            thermal[(int64_t)b * n + i] = th[b];
+            if (zero_mags && mags) mags[(int64_t)b * n + i] = mg[b];
+        }
+    }
     return KO_OK;
 }

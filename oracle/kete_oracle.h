@@ -120,6 +120,25 @@ int ko_neatm_total_flux(const double sun2obj[3], const double sun2obs[3], double
                         double *v_mag, double *v_flux);
 double ko_hg_apparent_flux(const double sun2obj[3], const double sun2obs[3], double h_mag,
                            double g_param, double diam, double wavelength, double albedo);
+/* FRM (frm.rs): latitude-only facet temperatures, beaming fixed to pi. */
+double ko_frm_facet_temperature(const double normal[3], const double obj2sun_unit[3],
+                                double subsolar_temp);
+int ko_frm_total_flux(const double sun2obj[3], const double sun2obs[3], double h_mag,
+                      double g_param, double diam, double vis_albedo, double emissivity,
+                      int n_bands, const double *bands, const double *band_albedos,
+                      const double *sun_correction, const double *zero_mags,
+                      int wise_color_correction, double *fluxes, double *hg_fluxes,
+                      double *thermal, double *mags, double *v_mag, double *v_flux);
+/* Batched NEATM (model 0) / FRM (model 1) over OpenMP threads; (3, n) and (n_bands, n)
+ * arrays; beaming may be NULL for the FRM. */
+int ko_thermal_batch(int model, int64_t n, const double *sun2obj, const double *sun2obs,
+                     const double *h_mag, const double *g_param, const double *diam,
+                     const double *vis_albedo, const double *beaming, const double *emissivity,
+                     int n_bands, const double *bands, const double *band_albedos,
+                     const double *sun_correction, const double *zero_mags,
+                     int wise_color_correction, double *fluxes, double *hg_fluxes,
+                     double *thermal, double *mags, double *v_mag, double *v_flux,
+                     int n_threads);
 
 /* ---- elements -> state (population generation helper) -------------------------------- */
 int ko_elements_to_pos_vel(double epoch, double ecc, double incl, double lon_asc,

@@ -85,6 +85,14 @@ def lib():
         L.ko_neatm_total_flux.argtypes = [_dp, _dp, C.c_double, C.c_double, C.c_double,
                                           C.c_double, C.c_double, C.c_double, C.c_int, _dp, _dp,
                                           _dp, _dp, C.c_int, _dp, _dp, _dp, _dp, _dp, _dp]
+        L.ko_frm_facet_temperature.argtypes = [_dp, _dp, C.c_double]
+        L.ko_frm_facet_temperature.restype = C.c_double
+        L.ko_frm_total_flux.argtypes = [_dp, _dp, C.c_double, C.c_double, C.c_double,
+                                        C.c_double, C.c_double, C.c_int, _dp, _dp, _dp, _dp,
+                                        C.c_int, _dp, _dp, _dp, _dp, _dp, _dp]
+        L.ko_thermal_batch.argtypes = [C.c_int, C.c_int64] + [_dp] * 8 + [C.c_int, _dp, _dp,
+                                                                          _dp, _dp, C.c_int] + [
+            _dp] * 6 + [C.c_int]
         L.ko_elements_to_pos_vel.argtypes = [C.c_double] * 7 + [_dp, _dp]
     return _lib
 
@@ -308,6 +316,67 @@ def neatm_total_flux(sun2obj, sun2obs, h_mag, g_param, diam, vis_albedo, beaming
     return dict(fluxes=fl, hg_fluxes=hg, thermal_fluxes=th,
                 magnitudes=(mg if zm is not None else None), v_band_magnitude=vm.value,
                 v_band_flux=vf.value)
+
+
+def frm_facet_temperature(normal, obj2sun, sst):
+    """frm_facet_temperature (flux/frm.rs:19-30)."""
+    return lib().ko_frm_facet_temperature(_p(_v3(normal)), _p(_v3(obj2sun)), sst)
+
+
+def frm_total_flux(sun2obj, sun2obs, h_mag, g_param, diam, vis_albedo, emissivity, bands,
+                   band_albedos, sun_correction=None, zero_mags=None,
+                   wise_color_correction=False):
+    """FrmParams::apparent_total_flux (flux/frm.rs:137-185) on the 2048-facet sphere."""
+    bands = np.ascontiguousarray(bands, dtype=np.float64)
+    nb = bands.size
+    alb = np.ascontiguousarray(band_albedos, dtype=np.float64)
+    sc = np.ones(nb) if sun_correction is None else np.ascontiguousarray(sun_correction,
+                                                                         dtype=np.float64)
+    zm = None if zero_mags is None else np.ascontiguousarray(zero_mags, dtype=np.float64)
+    fl, hg, th, mg = np.zeros(nb), np.zeros(nb), np.zeros(nb), np.zeros(nb)
+    vm, vf = C.c_double(), C.c_double()
+    lib().ko_frm_total_flux(_p(_v3(sun2obj)), _p(_v3(sun2obs)), h_mag, g_param, diam,
+                            vis_albedo, emissivity, nb, _p(bands), _p(alb), _p(sc), _p(zm),
+                            int(wise_color_correction), _p(fl), _p(hg), _p(th), _p(mg),
+                            C.byref(vm), C.byref(vf))
+    return dict(fluxes=fl, hg_fluxes=hg, thermal_fluxes=th,
+                magnitudes=(mg if zm is not None else None), v_band_magnitude=vm.value,
+                v_band_flux=vf.value)
+
+
+def thermal_batch(model, sun2obj, sun2obs, h_mag, g_param, diam, vis_albedo, beaming,
+                  emissivity, bands, band_albedos, sun_correction=None, zero_mags=None,
+                  wise_color_correction=False, threads=0):
+    """Many geometries of NEATM (model 0) or FRM (model 1; beaming ignored) on the host's
+    threads: (3, n) geometry arrays, (n,) parameters, (n_bands, n) albedos."""
+    s2obj = np.ascontiguousarray(sun2obj, dtype=np.float64)
+    s2obs = np.ascontiguousarray(sun2obs, dtype=np.float64)
+    n = s2obj.shape[1]
+    per = lambda x: np.ascontiguousarray(np.broadcast_to(np.asarray(x, np.float64), (n,)))
+    bands = np.ascontiguousarray(bands, dtype=np.float64)
+    nb = bands.size
+    alb = np.ascontiguousarray(np.broadcast_to(np.asarray(band_albedos, np.float64).reshape(
+        nb, -1), (nb, n)))
+    sc = np.ones(nb) if sun_correction is None else np.ascontiguousarray(sun_correction,
+                                                                         dtype=np.float64)
+    zm = None if zero_mags is None else np.ascontiguousarray(zero_mags, dtype=np.float64)
+    out = {k: np.zeros((nb, n)) for k in ("fluxes", "hg_fluxes", "thermal_fluxes",
+                                          "magnitudes")}
+    vm, vf = np.zeros(n), np.zeros(n)
+    bm = per(np.pi if beaming is None else beaming)
+    rc = lib().ko_thermal_batch(int(model), n, _p(s2obj), _p(s2obs), _p(per(h_mag)),
+                                _p(per(g_param)), _p(per(diam)), _p(per(vis_albedo)), _p(bm),
+                                _p(per(emissivity)), nb, _p(bands), _p(alb), _p(sc), _p(zm),
+                                int(wise_color_correction), _p(out["fluxes"]),
+                                _p(out["hg_fluxes"]), _p(out["thermal_fluxes"]),
+                                _p(out["magnitudes"]), _p(vm), _p(vf), int(threads))
+    if rc != 0:
+        raise ValueError("ko_thermal_batch: n_bands must be 1..8")
+    if zm is None:
+        out["magnitudes"] = None
+    out["v_band_magnitude"] = vm
+    out["v_band_flux"] = vf
+    return out
 
 
 def elements_to_state(epoch, ecc, incl, lon_asc, peri_time, peri_arg, peri_dist):

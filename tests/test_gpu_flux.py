@@ -1,5 +1,5 @@
 """GPU magnitudes against the oracle and the reference's golden values.
-Tolerances: magnitudes 1e-9 mag; NEATM fluxes 1e-12 relative (sums are reduced in a
+Tolerances: magnitudes 1e-9 mag; NEATM and FRM fluxes 1e-12 relative (sums are reduced in a
 different order on the GPU)."""
 import numpy as np
 import pytest
@@ -65,3 +65,80 @@ def test_neos_neatm_vs_oracle(gpu, oracle):
         np.testing.assert_allclose(r["thermal_fluxes"][:, i], o["thermal_fluxes"], rtol=1e-12)
         assert np.abs(r["magnitudes"][:, i] - o["magnitudes"]).max() < 1e-9
         assert abs(r["v_band_magnitude"][i] - o["v_band_magnitude"]) < 1e-9
+
+
+def test_neos_frm_model_on_gpu(gpu, oracle):
+    # src/tests/flux/test_model.py:23-34, checked against the oracle as well
+    model = gpu.flux.FrmParams.new_neos("visible", vis_albedo=0.3, band_albedos=[0.3, 0.3],
+                                        g_param=0.15, diam=1.0)
+    out = model.evaluate([[1, 1, 0]], [[0, 1, 0]])[0]
+    assert model.desig == "visible"
+    assert out.fluxes[0] >= 0.0 and out.fluxes[1] >= 0.0
+    o = oracle.frm_total_flux([1, 1, 0], [0, 1, 0], model.h_mag, 0.15, 1.0, 0.3, 0.9,
+                              [4700.0, 8000.0], [0.3, 0.3], None, [170.662, 64.13])
+    np.testing.assert_allclose(out.fluxes, o["fluxes"], rtol=1e-12)
+    assert np.abs(out.magnitudes - o["magnitudes"]).max() < 1e-9
+
+
+def test_wise_frm_vs_oracle(gpu, oracle):
+    # WISE bands with the polynomial colour corrections (constants/wise.rs:40-85)
+    s2obj, s2obs = _geometries(2000, 5)
+    s2obj[2] *= 3.0   # Sun directions well off the equator exercise the latitude terms
+    n = s2obj.shape[1]
+    rng = np.random.default_rng(6)
+    pv = np.exp(np.log(0.14) + 0.6 * rng.normal(size=n))
+    h = rng.uniform(8, 20, n)
+    diam = 1329.0 / np.sqrt(pv) * 10 ** (-h / 5)
+    bands = [3352.6, 4602.8, 11560.8 * 0.96, 22088.3 * 1.025]
+    zm = [306.681, 170.663, 29.0448 * 1.08, 8.2839 * 0.96]
+    sc = [1.0049, 1.0193, 1.0024, 1.0012]
+    alb = np.stack([pv] * 4)
+    r = gpu.flux.frm_arrays(s2obj, s2obs, h, 0.15, diam, pv, 0.9, bands, alb, sc, zm, True)
+    for i in range(0, n, 25):
+        o = oracle.frm_total_flux(s2obj[:, i], s2obs[:, i], h[i], 0.15, diam[i], pv[i], 0.9,
+                                  bands, alb[:, i], sc, zm, wise_color_correction=True)
+        np.testing.assert_allclose(r["fluxes"][:, i], o["fluxes"], rtol=1e-12)
+        np.testing.assert_allclose(r["thermal_fluxes"][:, i], o["thermal_fluxes"], rtol=1e-12)
+        np.testing.assert_allclose(r["hg_fluxes"][:, i], o["hg_fluxes"], rtol=1e-12)
+        assert np.abs(r["magnitudes"][:, i] - o["magnitudes"]).max() < 1e-9
+        assert abs(r["v_band_magnitude"][i] - o["v_band_magnitude"]) < 1e-9
+
+
+def test_frm_differs_from_neatm(gpu):
+    # FRM is not NEATM with another beaming: night-side facets radiate (frm.rs:19-30)
+    s2obj, s2obs = _geometries(64, 7)
+    kw = dict(h_mag=15.0, g_param=0.15, diam=2.0, vis_albedo=0.1, emissivity=0.9,
+              band_wavelength=[12000.0], band_albedos=[0.1])
+    f = gpu.flux.frm_arrays(s2obj, s2obs, **kw)
+    m = gpu.flux.neatm_arrays(s2obj, s2obs, beaming=np.pi, **kw)
+    assert (f["thermal_fluxes"] > 0).all()
+    assert np.abs(f["thermal_fluxes"] / m["thermal_fluxes"] - 1).max() > 1e-3
+    np.testing.assert_allclose(f["hg_fluxes"], m["hg_fluxes"], rtol=1e-15)
+
+
+@pytest.mark.parametrize("model,bands", [("neatm", [1200.0, 3352.6, 4602.8, 11000.0, 22000.0]),
+                                         ("frm", [4700.0, 8000.0, 12000.0]),
+                                         ("frm", [5.0, 9000.0])])
+def test_band_counts_vs_oracle(gpu, oracle, model, bands):
+    # every compiled band-count form; a band below 10 nm has no thermal flux (common.rs:139-154)
+    s2obj, s2obs = _geometries(300, 8)
+    n, nb = s2obj.shape[1], len(bands)
+    rng = np.random.default_rng(9)
+    pv = np.exp(np.log(0.14) + 0.6 * rng.normal(size=n))
+    h = rng.uniform(10, 20, n)
+    diam = 1329.0 / np.sqrt(pv) * 10 ** (-h / 5)
+    alb = np.stack([pv] * nb)
+    if model == "neatm":
+        r = gpu.flux.neatm_arrays(s2obj, s2obs, h, 0.15, diam, pv, 1.2, 0.9, bands, alb)
+    else:
+        r = gpu.flux.frm_arrays(s2obj, s2obs, h, 0.15, diam, pv, 0.9, bands, alb)
+    for i in range(0, n, 7):
+        if model == "neatm":
+            o = oracle.neatm_total_flux(s2obj[:, i], s2obs[:, i], h[i], 0.15, diam[i], pv[i], 1.2,
+                                        0.9, bands, alb[:, i])
+        else:
+            o = oracle.frm_total_flux(s2obj[:, i], s2obs[:, i], h[i], 0.15, diam[i], pv[i], 0.9,
+                                      bands, alb[:, i])
+        np.testing.assert_allclose(r["thermal_fluxes"][:, i], o["thermal_fluxes"], rtol=1e-12,
+                                   atol=0.0)
+        np.testing.assert_allclose(r["fluxes"][:, i], o["fluxes"], rtol=1e-12)

@@ -129,6 +129,65 @@ def test_neatm_facet_temperature(oracle):
     assert abs(t1 - t2) < 1e-2
 
 
+def test_frm_facet_temperature(oracle):
+    # kete_core/flux/frm.rs:188-258
+    o2s = [1.0, 0.0, 0.0]
+    t = np.cos(np.pi / 4) ** 0.25
+    for n in ([1, 0, 0], [0, 1, 0], [-1, 0, 0], np.array([1.0, 1.0, 0.0]) / np.sqrt(2)):
+        assert abs(oracle.frm_facet_temperature(n, o2s, 1.0) - 1.0) < 1e-8
+    for n in ([1.0, 0.0, 1.0], [0.0, -1.0, 1.0]):
+        n = np.array(n) / np.linalg.norm(n)
+        assert abs(oracle.frm_facet_temperature(n, o2s, 1.0) - t) < 1e-8
+    f1, _ = oracle.fib_lattice(2048)
+    f2, _ = oracle.fib_lattice(1028)
+    t1 = np.mean([oracle.frm_facet_temperature(f, o2s, 1.0) for f in f1])
+    t2 = np.mean([oracle.frm_facet_temperature(f, o2s, 1.0) for f in f2])
+    assert abs(t1 - t2) < 1e-2
+
+
+def test_neos_frm_model(oracle):
+    # src/tests/flux/test_model.py:23-34: positive fluxes in both NEOS bands
+    h = -5.0 * np.log10(1.0 * np.sqrt(0.3) / 1329.0)
+    res = oracle.frm_total_flux([1, 1, 0], [0, 1, 0], h, 0.15, 1.0, 0.3, 0.9, [4700.0, 8000.0],
+                                [0.3, 0.3], None, [170.662, 64.13])
+    assert (res["fluxes"] >= 0.0).all() and (res["thermal_fluxes"] > 0.0).all()
+
+
+def _frm_thermal_numpy(oracle, sun2obj, sun2obs, diam, vis_albedo, g_param, emissivity, bands):
+    """Independent vectorised restatement of FrmParams::apparent_thermal_flux
+    (frm.rs:78-130) with common.rs's black body, Lambertian scale and sub-solar
+    temperature, used to cross-check the C oracle."""
+    normals, area = oracle.fib_lattice(2048)
+    sun2obj, sun2obs = np.asarray(sun2obj, float), np.asarray(sun2obs, float)
+    obj2sun = -sun2obj
+    obs2obj = sun2obj - sun2obs
+    r_obs = np.linalg.norm(obs2obj)
+    bond = vis_albedo * (0.29 + 0.684 * g_param)
+    sst = ((1 - bond) * 1360.8 / obj2sun.dot(obj2sun) / (np.pi * emissivity * 5.670374419e-8)) ** 0.25
+    o2s = obj2sun / np.linalg.norm(obj2sun)
+    tmp = np.cos(np.arcsin(normals[:, 2]) - np.arcsin(o2s[2]))
+    temp = np.where(tmp > 0, np.sqrt(np.sqrt(np.maximum(tmp, 0))) * sst, 0.0)
+    seen = -normals @ (obs2obj / r_obs)
+    scale = np.where(seen > 0, seen * emissivity * np.pi * (r_obs * 149597870.7 / diam) ** -2, 0.0)
+    out = []
+    for wl in bands:
+        um = wl * 1e-3
+        with np.errstate(over="ignore", divide="ignore"):
+            bb = 397.289171e17 / um**3 / (np.exp(1.43877688e4 / (um * temp)) - 1.0)
+        bb = np.where((temp < 30.0) | (wl < 10.0), 0.0, bb)
+        out.append(np.sum(np.where((temp != 0) & (scale != 0), scale * bb * area, 0.0)))
+    return np.array(out)
+
+
+@pytest.mark.parametrize("z", [0.0, 0.3, -0.7])
+def test_frm_thermal_vs_numpy(oracle, z):
+    s2obj, s2obs = [1.2, 0.9, z], [0.0, 1.0, 0.05]
+    bands = [4700.0, 8000.0, 12000.0]
+    res = oracle.frm_total_flux(s2obj, s2obs, 18.0, 0.15, 0.8, 0.12, 0.9, bands, [0.1] * 3)
+    ref = _frm_thermal_numpy(oracle, s2obj, s2obs, 0.8, 0.12, 0.15, 0.9, bands)
+    np.testing.assert_allclose(res["thermal_fluxes"], ref, rtol=1e-11)
+
+
 def test_wise_neatm_golden(oracle, goldens):
     # src/tests/flux/test_model.py:37-51 (H from diameter and albedo, reflected.rs:198-203)
     g = goldens["wise_neatm"]
