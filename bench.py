@@ -93,6 +93,13 @@ WORKLOADS["thermal_wise_1m"] = ("thermal model, FRM with the four WISE bands and
 DEFAULT_N["thermal_wise_1m"] = 1_000_000
 # ncu sm__pipe_fp64_cycles_active of the FRM WISE kernel (profiles/thermal_frm_wise_20k.md)
 THERMAL_FP64_PIPE = 0.564
+WORKLOADS["stm_cov_1m"] = ("two-body state-transition matrices with covariance propagation, {n} "
+                           "main-belt states, per-object spans U(-1000, 1000) d, one 6x6 "
+                           "covariance per object (Phi C Phi^T)")
+DEFAULT_N["stm_cov_1m"] = 1_000_000
+# bytes each object moves: pos, vel, jd0, jd1, covariance in (8 x 44); pos, vel, STM,
+# covariance, status out (8 x 78 + 4)
+STM_BYTES_PER_OBJECT = 8 * 44 + 8 * 78 + 4
 SPK21_ID = 20000042
 SURVEY_FIELDS, SURVEY_DT_LIMIT = 2000, 3.0
 
@@ -376,6 +383,8 @@ def run_reference(args, world, rank):
         return run_reference_long(args)
     if args.workload == "thermal_wise_1m":
         return run_reference_thermal(args)
+    if args.workload == "stm_cov_1m":
+        return run_reference_stm(args)
     kind = args.workload
     n = args.n or DEFAULT_N[kind]
     pos, vel, jd0, jd1, ng = workload(n, kind=kind)
@@ -1275,6 +1284,136 @@ def run_thermal(args, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
+def stm_inputs(n, seed=81):
+    """Seeded main-belt states, spans and symmetric positive covariances."""
+    from kete_b200 import synthetic
+
+    pos, vel = synthetic.main_belt(n, seed=seed)
+    rng = np.random.default_rng(seed + 1)
+    jd0 = np.full(n, EPOCH)
+    jd1 = EPOCH + rng.uniform(-1000.0, 1000.0, n)
+    sig = np.array([1e-6] * 3 + [1e-8] * 3)
+    a = rng.normal(size=(6, 6, n)) * sig[:, None, None]
+    cov = np.ascontiguousarray(np.einsum("ikn,jkn->ijn", a, a))
+    return (np.ascontiguousarray(pos), np.ascontiguousarray(vel), jd0, jd1, cov)
+
+
+def run_reference_stm(args):
+    """The corrected variational equations on kete's RK4(5) (the oracle), one thread."""
+    from oracle import oracle as O
+
+    n = args.n or DEFAULT_N["stm_cov_1m"]
+    pos, vel, jd0, jd1, cov = stm_inputs(min(n, 5000))
+    k = min(n, 2000)
+
+    def step(m):
+        for i in range(m):
+            _, _, phi = O.compute_stm(pos[:, i], vel[:, i], jd0[i], jd1[i])
+            phi @ cov[:, :, i] @ phi.T
+
+    for _ in range(args.warmup):
+        step(min(k, 50))
+    times = []
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        step(k)
+        times.append(time.perf_counter() - t)
+    total = float(np.sum(times))
+    value = k * args.steps / total
+    line = {
+        "impl": "reference", "metric": "two-body STM + covariance objects/s", "value": value,
+        "unit": "objects/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOADS["stm_cov_1m"].format(n=n), "n_objects": n},
+        "cpu_baseline": {"value": value, "unit": "objects/s", "cores": 1, "kind": "port",
+                         "sample": f"the first {k} objects per step, one thread (kete's "
+                                   "compute_stm is one call per state); the reference "
+                                   "Rust path cannot be built"},
+        "e2e": {"value": value, "unit": "objects/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_stm(args, world, rank, local):
+    """Two-body STMs with covariance propagation of every object on the device."""
+    import torch
+
+    import kete_b200
+    from kete_b200 import build, state_transition
+    from oracle import oracle as O
+
+    build.build()
+    torch.cuda.set_device(local)
+    kete_b200.init(local)
+    n = args.n or DEFAULT_N["stm_cov_1m"]
+    pos, vel, jd0, jd1, cov = stm_inputs(n, seed=81 + rank)
+    dev = torch.device("cuda", local)
+    P, V, J0, J1, Cv = (torch.from_numpy(x).to(dev) for x in (pos, vel, jd0, jd1, cov))
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        return state_transition.compute_stm_arrays(P, V, J0, J1, 1.0, Cv)
+
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    with ClockSampler(local) as clk:
+        barrier(world)
+        for k in range(args.steps):
+            flush.zero_()
+            evs[k][0].record(stream)
+            out = step()
+            evs[k][1].record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+    t_total = reduce_max(sum(a.elapsed_time(b) for a, b in evs) * 1e-3, world)
+    ms_step = 1e3 * t_total / args.steps
+    value = world * n * args.steps / t_total
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        hp = state_transition.compute_stm_arrays(pos, vel, jd0, jd1, 1.0, cov)
+    e2e_s = reduce_max((time.perf_counter() - t) / args.steps, world)
+    if rank != 0:
+        return
+    m = out[2].cpu().numpy()
+    k = min(n, 300)
+    t = time.perf_counter()
+    err = 0.0
+    for i in range(k):
+        _, _, ref = O.compute_stm(pos[:, i], vel[:, i], jd0[i], jd1[i])
+        err = max(err, float(np.abs(m[:, :, i] - ref).max() / np.abs(ref).max()))
+    cpu_s = time.perf_counter() - t
+    peak = measured_peaks().get("hbm_gbs")
+    achieved = STM_BYTES_PER_OBJECT * n / (ms_step * 1e-3) / 1e9
+    line = {
+        "metric": "two-body STM + covariance objects/s", "value": value, "unit": "objects/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": WORKLOADS["stm_cov_1m"].format(n=n), "n_objects_per_gpu": n,
+                   "l2": "flushed (256 MB write) between timed steps"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved / peak) if peak else None, "traffic": None,
+                     "bytes_per_object": STM_BYTES_PER_OBJECT,
+                     "note": "algorithmic bytes over the kernel time; the dual-number leaf "
+                             "Jacobians make it FP64/latency-bound (profiles/two_body_stm_1m.md)"},
+        "cpu_baseline": {"value": k / cpu_s, "unit": "objects/s", "cores": 1, "kind": "port",
+                         "sample": f"the first {k} objects, one thread"},
+        "e2e": {"value": world * n / e2e_s, "unit": "objects/s",
+                "h2d_bytes_per_step": 8 * 44 * n, "d2h_bytes_per_step": (8 * 78 + 4) * n},
+        "gpu_launches": args.steps,
+        "clocks": clk.summary(),
+        "parity": {"max_rel_err_vs_oracle": err, "objects_compared": k, "tolerance_rel": 2e-8,
+                   "status_ok": bool((hp[4] == 0).all())},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def ctypes_probe(_lib):
     import ctypes
 
@@ -1317,6 +1456,8 @@ def main():
         run_long(args, world, rank, local)
     elif args.workload == "thermal_wise_1m":
         run_thermal(args, world, rank, local)
+    elif args.workload == "stm_cov_1m":
+        run_stm(args, world, rank, local)
     else:
         run_gpu(args, world, rank, local)
         if world > 1:

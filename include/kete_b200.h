@@ -120,6 +120,30 @@ int kete_b200_propagate_n_body(int64_t n, const double* pos, const double* vel,
                                double* impact_jd, double* min_dist, int32_t* counters, int mode,
                                int on_device, void* stream);
 
+/* compute_stm / propagate_covariance (src/kete/state_transition.py:8-59, backed by
+ * src/kete_core/src/propagation/state_transition.rs:52-122): the two-body state-transition
+ * matrix d(pos1, vel1)/d(pos0, vel0) of n Sun-centred states from jd0 to jd1 about a central
+ * body of central_mass solar masses, out_stm 6 x 6 x n (row index first, object fastest).
+ * The matrix is that of kete's closed-form propagation (analytic_2_body, kepler.rs:254-297),
+ * whose final states out_pos / out_vel (3 x n) match kete_b200_propagate_two_body.  kete's
+ * own routine integrates the variational equations with a Jacobian off by a factor -1/2,
+ * the unscaled GM in scaled time, and returns the transpose; this one returns the matrix
+ * that the two-body propagation has.  With covariance (6 x 6 x n) given, out_cov receives
+ * Phi covariance Phi^T (6 x 6 x n).  out_stm may be NULL.  status per object as
+ * kete_b200_propagate_two_body. */
+int kete_b200_compute_stm(int64_t n, const double* pos, const double* vel, const double* jd0,
+                          const double* jd1, double central_mass, const double* covariance,
+                          double* out_pos, double* out_vel, double* out_stm, double* out_cov,
+                          int32_t* status, int on_device, void* stream);
+
+/* out_cov = Phi C Phi^T for n objects: stm rows x cols x n, covariance cols x cols x n,
+ * out_cov rows x rows x n (object index fastest; rows, cols <= 16).  With the 6 x 8
+ * matrices of kete_b200_propagate_n_body_stm and an 8 x 8 covariance of (pos, vel, A1, A2)
+ * it propagates an orbit's uncertainty through the N-body model. */
+int kete_b200_covariance_transform(int64_t n, int rows, int cols, const double* stm,
+                                   const double* covariance, double* out_cov, int on_device,
+                                   void* stream);
+
 /* propagate_n_body_spk (src/kete_core/src/propagation/mod.rs:70-118) to a sequence of epochs
  * with forward sensitivities.  Object i starts at jd0[i]; each of the n_epochs epochs
  * (shared, in the order to visit) starts a fresh integration from the previous one.  For

@@ -4,7 +4,7 @@ Drop-in GPU versions of kete's ``propagate_two_body``, ``propagate_n_body``,
 ``fov_state_check``, ``hg_apparent_mag`` and ``NeatmParams.evaluate``, computed in FP64
 by hand-written sm_100a CUDA kernels in ``libketeb200.so`` (C ABI: include/kete_b200.h).
 """
-from . import autodiff, flux, fov, spice
+from . import autodiff, flux, fov, spice, state_transition
 from .fov import (ConeFOV, NeosCmos, NeosVisit, OmniDirectionalFOV, RectangleFOV, WiseCmos,
                   ZtfCcdQuad, ZtfField, fov_spk_check, fov_state_check, fov_static_check)
 from ._lib import KeteB200Error, init
@@ -19,6 +19,7 @@ from .propagation import (
     radau_central_arrays,
 )
 from .state import Frames, SimultaneousStates, State
+from .state_transition import compute_stm, propagate_covariance, propagate_covariance_n_body
 
 __all__ = [
     "autodiff",
@@ -49,4 +50,8 @@ __all__ = [
     "Frames",
     "SimultaneousStates",
     "State",
+    "state_transition",
+    "compute_stm",
+    "propagate_covariance",
+    "propagate_covariance_n_body",
 ]

@@ -806,6 +806,64 @@ int kete_b200_propagate_two_body(int64_t n, const double* pos, const double* vel
     return S.finish();
 }
 
+int kete_b200_compute_stm(int64_t n, const double* pos, const double* vel, const double* jd0,
+                          const double* jd1, double central_mass, const double* covariance,
+                          double* out_pos, double* out_vel, double* out_stm, double* out_cov,
+                          int32_t* status, int on_device, void* stream) {
+    if (n < 0 || (n > 0 && (!pos || !vel || !jd0 || !jd1 || !out_pos || !out_vel || !status)))
+        return set_error(KETE_B200_E_ARGUMENT, "null array");
+    if (!(central_mass > 0.0) || !std::isfinite(central_mass))
+        return set_error(KETE_B200_E_ARGUMENT, "central_mass must be positive");
+    if ((covariance == nullptr) != (out_cov == nullptr))
+        return set_error(KETE_B200_E_ARGUMENT, "covariance and out_cov go together");
+    std::lock_guard<std::mutex> lk(g_mu);
+    DevState* ds;
+    int rc = ensure_device(ds);
+    if (rc) return rc;
+    if (n == 0) return 0;
+    cudaStream_t st = (cudaStream_t)stream;
+    Stager S{*ds, st, on_device};
+    const double* d_pos = S.in(pos, 3 * (size_t)n);
+    const double* d_vel = S.in(vel, 3 * (size_t)n);
+    const double* d_jd0 = S.in(jd0, (size_t)n);
+    const double* d_jd1 = S.in(jd1, (size_t)n);
+    const double* d_cov = S.in(covariance, 36 * (size_t)n);
+    double* d_op = S.out(out_pos, 3 * (size_t)n);
+    double* d_ov = S.out(out_vel, 3 * (size_t)n);
+    double* d_stm = S.out(out_stm, 36 * (size_t)n);
+    double* d_oc = S.out(out_cov, 36 * (size_t)n);
+    int32_t* d_st = S.out(status, (size_t)n);
+    if (S.rc) return S.rc;
+    // GM of the central body: kete's GMS for one solar mass (constants/gravity.rs:9)
+    const double mu = central_mass == 1.0 ? GMS : GMS * central_mass;
+    if ((rc = launch_two_body_stm(n, d_pos, d_vel, d_jd0, d_jd1, mu, d_cov, d_op, d_ov, d_stm, d_oc,
+                                  d_st, st)))
+        return rc;
+    return S.finish();
+}
+
+int kete_b200_covariance_transform(int64_t n, int rows, int cols, const double* stm,
+                                   const double* covariance, double* out_cov, int on_device,
+                                   void* stream) {
+    if (n < 0 || (n > 0 && (!stm || !covariance || !out_cov)))
+        return set_error(KETE_B200_E_ARGUMENT, "null array");
+    if (rows < 1 || rows > 16 || cols < 1 || cols > 16)
+        return set_error(KETE_B200_E_ARGUMENT, "rows and cols must be 1..16");
+    std::lock_guard<std::mutex> lk(g_mu);
+    DevState* ds;
+    int rc = ensure_device(ds);
+    if (rc) return rc;
+    if (n == 0) return 0;
+    cudaStream_t st = (cudaStream_t)stream;
+    Stager S{*ds, st, on_device};
+    const double* d_stm = S.in(stm, (size_t)rows * cols * n);
+    const double* d_cov = S.in(covariance, (size_t)cols * cols * n);
+    double* d_out = S.out(out_cov, (size_t)rows * rows * n);
+    if (S.rc) return S.rc;
+    if ((rc = launch_covariance(n, rows, cols, d_stm, d_cov, d_out, st))) return rc;
+    return S.finish();
+}
+
 int kete_b200_propagate_n_body(int64_t n, const double* pos, const double* vel, const double* jd0,
                                const double* jd1, int frame, int64_t center, int include_asteroids,
                                const double* nongrav, double* out_pos, double* out_vel,

@@ -46,6 +46,12 @@ struct NBodyArgs {
 int launch_two_body(int64_t n, const double* pos, const double* vel, const double* jd0,
                     const double* jd1, const double* obs, double* out_pos, double* out_vel,
                     double* out_jd, int32_t* status, cudaStream_t stream);
+int launch_two_body_stm(int64_t n, const double* pos, const double* vel, const double* jd0,
+                        const double* jd1, double mu, const double* cov, double* out_pos,
+                        double* out_vel, double* out_stm, double* out_cov, int32_t* status,
+                        cudaStream_t stream);
+int launch_covariance(int64_t n, int rows, int cols, const double* phi, const double* cov,
+                      double* out, cudaStream_t stream);
 int launch_nbody_thread(const NBodyArgs& a, int block, cudaStream_t stream);
 int launch_nbody_nodes(const NBodyArgs& a, int variant, int grid, cudaStream_t stream);
 int nodes_grid_size(int variant, int* grid);

@@ -32,6 +32,7 @@ __device__ __forceinline__ double g_2(double s, double beta) {
 struct KepEq {
     double r0, rv0, beta, b_sqrt, dt;
     bool hyperbolic;
+    double mu;  // GM of the central body (GMS in kete)
     __device__ __forceinline__ double f(double x) const {
         double g1, g2;
         if (!hyperbolic) {
@@ -43,7 +44,7 @@ struct KepEq {
             g2 = (1.0 - cosh(b_sqrt * x)) / beta;
         }
         const double g3 = (x - g1) / beta;
-        return r0 * g1 + rv0 * g2 + GMS * g3 - dt;
+        return r0 * g1 + rv0 * g2 + mu * g3 - dt;
     }
     __device__ __forceinline__ double d(double x) const {
         double g2d, g1d;
@@ -54,7 +55,7 @@ struct KepEq {
             g1d = cosh(b_sqrt * x);
         }
         const double g3d = (1.0 - g1d) / beta;
-        return r0 * g1d + rv0 * g2d + GMS * g3d;
+        return r0 * g1d + rv0 * g2d + mu * g3d;
     }
 };
 
@@ -81,34 +82,56 @@ __device__ __forceinline__ int newton(const KepEq& q, double start, double atol,
 }
 
 __device__ __forceinline__ int solve_kepler_universal(double dt, double r0, double v0, double rv0,
-                                                      double& s_out, double& beta_out) {
-    const double beta = 2.0 * GMS / r0 - powi<2>(v0);
+                                                      double& s_out, double& beta_out,
+                                                      double mu = GMS) {
+    const double beta = 2.0 * mu / r0 - powi<2>(v0);
     const double b_sqrt = sqrt(fabs(beta));
     double res = 0.0;
     int rc;
     if (beta >= PARABOLIC_BETA) {
-        const double period = GMS * powi<-3>(b_sqrt);
+        const double period = mu * powi<-3>(b_sqrt);
         const double dtm = fmod(dt, period * TAU);
-        KepEq q{r0, rv0, beta, b_sqrt, dtm, false};
+        KepEq q{r0, rv0, beta, b_sqrt, dtm, false, mu};
         const double guess = (1.0 / b_sqrt) * dtm / period;
         rc = newton(q, guess, 1e-11, res);
     } else if (fabs(beta) < PARABOLIC_BETA) {
-        const double a0 = -6.0 * dt / GMS;
-        const double a1 = 6.0 * r0 / GMS;
-        const double a2 = 3.0 * rv0 / GMS;
+        const double a0 = -6.0 * dt / mu;
+        const double a1 = 6.0 * r0 / mu;
+        const double a2 = 3.0 * rv0 / mu;
         const double p = (3.0 * a1 - powi<2>(a2)) / 3.0;
         const double qq = (9.0 * a1 * a2 - 27.0 * a0 - 2.0 * powi<3>(a2)) / 27.0;
         const double w = pow(qq / 2.0 + sqrt(powi<2>(qq) / 4.0 + powi<3>(p) / 27.0), 1.0 / 3.0);
         res = w - p / (3.0 * w) - a2 / 3.0;
         rc = ST_OK;
     } else {
-        KepEq q{r0, rv0, beta, b_sqrt, dt, true};
-        rc = newton(q, GMS_SQRT * fabs(beta) * dt, 1e-11, res);
+        KepEq q{r0, rv0, beta, b_sqrt, dt, true, mu};
+        // kete's starting point uses its GMS_SQRT literal (kepler.rs:228)
+        const double mu_sqrt = mu == GMS ? GMS_SQRT : sqrt(mu);
+        rc = newton(q, mu_sqrt * fabs(beta) * dt, 1e-11, res);
     }
     if (rc != ST_OK) return ST_CONVERGENCE;
     s_out = res;
     beta_out = beta;
     return ST_OK;
+}
+
+// The f and g update of one closed-form step from the solved anomaly s (kepler.rs:270-288).
+__device__ __forceinline__ void two_body_apply(double s, double beta, double r0, double rv0,
+                                               double p[3], double v[3], double mu = GMS) {
+    const double g1 = g_1(s, beta), g2 = g_2(s, beta);
+    const double f = 1.0 - mu / r0 * g2;
+    const double g = r0 * g1 + rv0 * g2;
+    double np[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) np[i] = p[i] * f + v[i] * g;
+    const double nr0 = norm3(np[0], np[1], np[2]);
+    const double f_dot = -mu / (nr0 * r0) * g1;
+    const double g_dot = 1.0 - (mu / nr0) * g2;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        v[i] = p[i] * f_dot + v[i] * g_dot;
+        p[i] = np[i];
+    }
 }
 
 // One closed-form step; returns ST_CONVERGENCE when the solver fails.
@@ -118,20 +141,7 @@ __device__ __forceinline__ int two_body_leaf(double time, double p[3], double v[
     const double rv0 = p[0] * v[0] + p[1] * v[1] + p[2] * v[2];
     double s, beta;
     if (solve_kepler_universal(time, r0, v0, rv0, s, beta) != ST_OK) return ST_CONVERGENCE;
-    const double g1 = g_1(s, beta), g2 = g_2(s, beta);
-    const double f = 1.0 - GMS / r0 * g2;
-    const double g = r0 * g1 + rv0 * g2;
-    double np[3];
-#pragma unroll
-    for (int i = 0; i < 3; ++i) np[i] = p[i] * f + v[i] * g;
-    const double nr0 = norm3(np[0], np[1], np[2]);
-    const double f_dot = -GMS / (nr0 * r0) * g1;
-    const double g_dot = 1.0 - (GMS / nr0) * g2;
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-        v[i] = p[i] * f_dot + v[i] * g_dot;
-        p[i] = np[i];
-    }
+    two_body_apply(s, beta, r0, rv0, p, v);
     return ST_OK;
 }
 

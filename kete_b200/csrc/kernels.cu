@@ -887,3 +887,91 @@ int launch_nbody_long(const LongArgs& a, cudaStream_t stream) {
 }
 
 }  // namespace kb
+
+// -------------------------------------------------------------------------------------------
+// Two-body state-transition matrices with covariance propagation (compute_stm,
+// propagate_covariance: src/kete/state_transition.py:8-59, corrected as kepler_stm.cuh
+// describes), and the covariance sandwich Phi C Phi^T on its own for other matrices.
+// -------------------------------------------------------------------------------------------
+#include "kepler_stm.cuh"
+
+namespace kb {
+
+// out (rows x rows) = Phi (rows x cols) C (cols x cols) Phi^T for object i; SoA with the
+// object index fastest.
+__device__ __forceinline__ void covariance_sandwich(int64_t n, int64_t i, int rows, int cols,
+                                                    const double* Phi, bool phi_soa,
+                                                    const double* C, double* out) {
+    for (int r = 0; r < rows; ++r)
+        for (int q = r; q < rows; ++q) {
+            double acc = 0.0;
+            for (int a = 0; a < cols; ++a) {
+                const double pra = phi_soa ? Phi[(int64_t)(r * cols + a) * n + i] : Phi[r * cols + a];
+                double inner = 0.0;
+                for (int b = 0; b < cols; ++b) {
+                    const double pqb = phi_soa ? Phi[(int64_t)(q * cols + b) * n + i] : Phi[q * cols + b];
+                    inner += C[(int64_t)(a * cols + b) * n + i] * pqb;
+                }
+                acc += pra * inner;
+            }
+            out[(int64_t)(r * rows + q) * n + i] = acc;
+            out[(int64_t)(q * rows + r) * n + i] = acc;
+        }
+}
+
+__global__ void __launch_bounds__(128) two_body_stm_kernel(
+    int64_t n, const double* __restrict__ pos, const double* __restrict__ vel,
+    const double* __restrict__ jd0, const double* __restrict__ jd1, double mu,
+    const double* __restrict__ cov, double* __restrict__ out_pos, double* __restrict__ out_vel,
+    double* __restrict__ out_stm, double* __restrict__ out_cov, int32_t* __restrict__ status) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double p[3] = {pos[i], pos[n + i], pos[2 * n + i]};
+    double v[3] = {vel[i], vel[n + i], vel[2 * n + i]};
+    double Phi[36];
+    int rc = analytic_2_body_stm(jd1[i] - jd0[i], p, v, mu, Phi);
+    if (rc != ST_OK) {
+        const double nan = __longlong_as_double(0x7ff8000000000000LL);
+        p[0] = p[1] = p[2] = v[0] = v[1] = v[2] = nan;
+#pragma unroll
+        for (int k = 0; k < 36; ++k) Phi[k] = nan;
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        out_pos[c * n + i] = p[c];
+        out_vel[c * n + i] = v[c];
+    }
+    if (out_stm)
+#pragma unroll
+        for (int k = 0; k < 36; ++k) out_stm[k * n + i] = Phi[k];
+    if (cov && out_cov) covariance_sandwich(n, i, 6, 6, Phi, false, cov, out_cov);
+    status[i] = rc;
+}
+
+__global__ void __launch_bounds__(128) covariance_kernel(int64_t n, int rows, int cols,
+                                                         const double* __restrict__ phi,
+                                                         const double* __restrict__ cov,
+                                                         double* __restrict__ out) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    covariance_sandwich(n, i, rows, cols, phi, true, cov, out);
+}
+
+int launch_two_body_stm(int64_t n, const double* pos, const double* vel, const double* jd0,
+                        const double* jd1, double mu, const double* cov, double* out_pos,
+                        double* out_vel, double* out_stm, double* out_cov, int32_t* status,
+                        cudaStream_t stream) {
+    if (n <= 0) return 0;
+    two_body_stm_kernel<<<(unsigned)((n + 127) / 128), 128, 0, stream>>>(
+        n, pos, vel, jd0, jd1, mu, cov, out_pos, out_vel, out_stm, out_cov, status);
+    return cuda_check(cudaGetLastError(), "two_body_stm_kernel launch");
+}
+
+int launch_covariance(int64_t n, int rows, int cols, const double* phi, const double* cov,
+                      double* out, cudaStream_t stream) {
+    if (n <= 0) return 0;
+    covariance_kernel<<<(unsigned)((n + 127) / 128), 128, 0, stream>>>(n, rows, cols, phi, cov, out);
+    return cuda_check(cudaGetLastError(), "covariance_kernel launch");
+}
+
+}  // namespace kb

@@ -1705,6 +1705,131 @@ int ko_propagate_n_body_vec(int64_t n, const double *pos, const double *vel, dou
 }
 
 /* ------------------------------------------------------------------------------------------
+ * two-body state-transition matrix: compute_state_transition (kete_core/propagation/
+ * state_transition.rs:6-122) on the RK4(5) Fehlberg integrator (runge_kutta.rs:33-158), with
+ * its three defects corrected: the Jacobian of the central acceleration is
+ * cm (3 r r^T - r^2 I) / r^5 (acceleration.rs:267-290 has a factor -1/2), the scaled-time
+ * acceleration uses GM = cm (central_accel uses GMS), and the physical matrix is
+ * D Phi D^-1 with D = diag(1, 1, 1, sqrt(GMS) x 3) instead of its transpose.
+ * ---------------------------------------------------------------------------------------- */
+#define STM_DIM 42
+
+static void stm_ivp(const double *y, double cm, double *dy) {
+    double r2 = y[0] * y[0] + y[1] * y[1] + y[2] * y[2];
+    double r = sqrt(r2);
+    double r3 = r2 * r, r5 = r3 * r2;
+    for (int i = 0; i < 3; ++i) {
+        dy[i] = y[3 + i];
+        dy[3 + i] = -y[i] * cm / r3;
+    }
+    double G[3][3];
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) G[a][b] = cm * (3.0 * y[a] * y[b] - (a == b ? r2 : 0.0)) / r5;
+    /* M column-major (nalgebra reshape): M(row, col) = y[6 + col * 6 + row]; dM = A M with
+     * A = [[0, I], [G, 0]] */
+    for (int c = 0; c < 6; ++c) {
+        const double *m = y + 6 + c * 6;
+        double *dm = dy + 6 + c * 6;
+        for (int row = 0; row < 3; ++row) dm[row] = m[3 + row];
+        for (int row = 0; row < 3; ++row) dm[3 + row] = G[row][0] * m[0] + G[row][1] * m[1] + G[row][2] * m[2];
+    }
+}
+
+static double vnorm(const double *x, int n) {
+    double s2 = 0.0;
+    for (int i = 0; i < n; ++i) s2 += x[i] * x[i];
+    return sqrt(s2);
+}
+
+/* RK45Integrator::step (runge_kutta.rs:33-113); the recursion on a rejected step becomes a
+ * loop.  Returns the next step size, or 0 on failure. */
+static double rk45_step(double *t, double *y, double *der, double h, double cm, double tol) {
+    double k2[STM_DIM], k3[STM_DIM], k4[STM_DIM], k5[STM_DIM], k6[STM_DIM], tmp[STM_DIM],
+        e[STM_DIM];
+    for (int attempt = 0; attempt < 10000; ++attempt) {
+        if (h != h || fabs(h) < 1e-30) return 0.0;
+        for (int i = 0; i < STM_DIM; ++i) tmp[i] = y[i] + der[i] * (h / 4.0);
+        stm_ivp(tmp, cm, k2);
+        for (int i = 0; i < STM_DIM; ++i) k2[i] *= h;
+        for (int i = 0; i < STM_DIM; ++i) tmp[i] = y[i] + der[i] * (3.0 * h / 32.0) + k2[i] * (9.0 / 32.0);
+        stm_ivp(tmp, cm, k3);
+        for (int i = 0; i < STM_DIM; ++i) k3[i] *= h;
+        for (int i = 0; i < STM_DIM; ++i)
+            tmp[i] = y[i] + der[i] * (h * 1932.0 / 2197.0) - k2[i] * (7200.0 / 2197.0) +
+                     k3[i] * (7296.0 / 2197.0);
+        stm_ivp(tmp, cm, k4);
+        for (int i = 0; i < STM_DIM; ++i) k4[i] *= h;
+        for (int i = 0; i < STM_DIM; ++i)
+            tmp[i] = y[i] + der[i] * (h * 439.0 / 216.0) - k2[i] * 8.0 + k3[i] * (3680.0 / 513.0) -
+                     k4[i] * (845.0 / 4104.0);
+        stm_ivp(tmp, cm, k5);
+        for (int i = 0; i < STM_DIM; ++i) k5[i] *= h;
+        for (int i = 0; i < STM_DIM; ++i)
+            tmp[i] = y[i] - der[i] * (h * 8.0 / 27.0) + k2[i] * 2.0 - k3[i] * (3544.0 / 2565.0) +
+                     k4[i] * (1859.0 / 4104.0) - k5[i] * (11.0 / 40.0);
+        stm_ivp(tmp, cm, k6);
+        for (int i = 0; i < STM_DIM; ++i) k6[i] *= h;
+        for (int i = 0; i < STM_DIM; ++i)
+            e[i] = der[i] * (h / -360.0) + k3[i] * (128.0 / 4275.0) + k4[i] * (2197.0 / 75240.0) -
+                   k5[i] / 50.0 - k6[i] * (2.0 / 55.0);
+        double trunc_err = vnorm(e, STM_DIM);
+        double new_step;
+        if (trunc_err == 0.0) {
+            new_step = 2.0 * h;
+        } else {
+            new_step = 0.9 * h * pow(tol / trunc_err, 1.0 / 5.0);
+            if (trunc_err > tol) {
+                h = new_step;
+                continue;
+            }
+        }
+        for (int i = 0; i < STM_DIM; ++i)
+            y[i] += der[i] * (h * 16.0 / 135.0) + k3[i] * (6656.0 / 12825.0) +
+                    k4[i] * (28561.0 / 56430.0) - k5[i] * (9.0 / 50.0) + k6[i] * (2.0 / 55.0);
+        *t += h;
+        stm_ivp(y, cm, der);
+        return new_step;
+    }
+    return 0.0;
+}
+
+int ko_compute_stm(const double pos[3], const double vel[3], double jd0, double jd1,
+                   double central_mass, double out_pos[3], double out_vel[3], double stm[36]) {
+    double y[STM_DIM], der[STM_DIM];
+    memset(y, 0, sizeof y);
+    for (int i = 0; i < 3; ++i) {
+        y[i] = pos[i];
+        y[3 + i] = vel[i] / GMS_SQRT;
+    }
+    for (int k = 0; k < 6; ++k) y[6 + k * 6 + k] = 1.0;
+    const double tol = 1e-12;
+    double t = jd0 * GMS_SQRT, tf = jd1 * GMS_SQRT;
+    if (fabs(t - tf) >= 1e-30) {
+        stm_ivp(y, central_mass, der);
+        double h = rk45_step(&t, y, der, tf - t, central_mass, tol);
+        if (h == 0.0) return KO_CONVERGENCE;
+        int guard = 0;
+        while (fabs(t - tf) > tol) {
+            if (fabs(t - tf) < fabs(h)) h = tf - t;
+            h = rk45_step(&t, y, der, h, central_mass, tol);
+            if (h == 0.0 || ++guard > 10000000) return KO_CONVERGENCE;
+        }
+    }
+    for (int i = 0; i < 3; ++i) {
+        out_pos[i] = y[i];
+        out_vel[i] = y[3 + i] * GMS_SQRT;
+    }
+    /* physical matrix (row-major): D M D^-1 */
+    for (int row = 0; row < 6; ++row)
+        for (int c = 0; c < 6; ++c) {
+            double m = y[6 + c * 6 + row];
+            double da = row >= 3 ? GMS_SQRT : 1.0, db = c >= 3 ? 1.0 / GMS_SQRT : 1.0;
+            stm[row * 6 + c] = da * m * db;
+        }
+    return KO_OK;
+}
+
+/* ------------------------------------------------------------------------------------------
  * flux (kete_core/flux/reflected.rs:23-34,255-326, common.rs:139-256, neatm.rs:19-185,
  * frm.rs:15-185,
  * shapes.rs:42-66, sun.rs:64-75, constants/wise.rs:9-85)

@@ -99,6 +99,10 @@ void ko_fov_check_visible(const double obs7[7], const double normals12[12], int6
                           double dt_limit, int include_extended, int32_t *flags,
                           double *out7);
 
+/* ---- two-body state-transition matrix (corrected state_transition.rs) -------------------- */
+int ko_compute_stm(const double pos[3], const double vel[3], double jd0, double jd1,
+                   double central_mass, double out_pos[3], double out_vel[3], double stm[36]);
+
 /* ---- flux -------------------------------------------------------------------------------- */
 double ko_hg_phase_curve_correction(double g_param, double phase);
 double ko_hg_apparent_mag(const double sun2obj[3], const double sun2obs[3], double h_mag,

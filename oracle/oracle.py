@@ -93,6 +93,7 @@ def lib():
         L.ko_thermal_batch.argtypes = [C.c_int, C.c_int64] + [_dp] * 8 + [C.c_int, _dp, _dp,
                                                                           _dp, _dp, C.c_int] + [
             _dp] * 6 + [C.c_int]
+        L.ko_compute_stm.argtypes = [_dp, _dp, C.c_double, C.c_double, C.c_double, _dp, _dp, _dp]
         L.ko_elements_to_pos_vel.argtypes = [C.c_double] * 7 + [_dp, _dp]
     return _lib
 
@@ -377,6 +378,17 @@ def thermal_batch(model, sun2obj, sun2obs, h_mag, g_param, diam, vis_albedo, bea
     out["v_band_magnitude"] = vm
     out["v_band_flux"] = vf
     return out
+
+
+def compute_stm(pos, vel, jd0, jd1, central_mass=1.0):
+    """Two-body state-transition matrix by the corrected variational equations on kete's
+    RK4(5) Fehlberg integrator (state_transition.rs:6-122): returns (pos, vel, stm 6x6)."""
+    p, v, m = np.zeros(3), np.zeros(3), np.zeros(36)
+    rc = lib().ko_compute_stm(_p(_v3(pos)), _p(_v3(vel)), float(jd0), float(jd1),
+                              float(central_mass), _p(p), _p(v), _p(m))
+    if rc != 0:
+        raise ValueError("ko_compute_stm failed")
+    return p, v, m.reshape(6, 6)
 
 
 def elements_to_state(epoch, ecc, incl, lon_asc, peri_time, peri_arg, peri_dist):
