@@ -1424,7 +1424,7 @@ int kete_b200_fov_check_visible(int64_t n_obj, const double* pos, const double* 
 }
 
 int kete_b200_set_launch_config(int nodes_variant, int nodes_refill, int thread_block) {
-    if (nodes_variant < 0 || nodes_variant > 5 || thread_block < 32 || thread_block > 1024 ||
+    if (nodes_variant < 0 || nodes_variant > 8 || thread_block < 32 || thread_block > 1024 ||
         thread_block % 32)
         return set_error(KETE_B200_E_ARGUMENT, "bad launch configuration");
     std::lock_guard<std::mutex> lk(g_mu);

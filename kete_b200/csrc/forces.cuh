@@ -328,6 +328,108 @@ struct SpkForceT {
         return ST_OK;
     }
 
+    // eval_fast in two halves, for callers that evaluate the force at the same time more than
+    // once (the corrector iterations of one Radau step share their node times):
+    // fast_positions writes the bodies' positions at t (and the Sun's and Jupiter's
+    // velocities) to cache[k * stride], k = 0 .. cached_doubles(P) - 1; fast_forces sums the
+    // accelerations from them in eval_fast's order.
+    __device__ __forceinline__ static int cached_doubles(const FastPlan& P) {
+        int k = 6 * P.n_vel;
+        for (int it = P.n_vel; it < P.n_items; ++it)
+            if (P.item[it].role >= 0) k += 3;
+        return k;
+    }
+
+    __device__ __forceinline__ void fast_positions(const FastPlan& P, double t, double* cache,
+                                                   int stride) const {
+        const double jds = __dmul_rn(t - 2451545.0, 86400.0);
+        const double* pool = c_eph.pool;
+        const int n_vel = P.n_vel;
+        int k = 0;
+#pragma unroll 1
+        for (int it = 0; it < n_vel; it += 2) {
+            const bool has_b = it + 1 < n_vel;
+            const double* ra = fast_record(pool, P.item[it], jds);
+            const double* rb = fast_record(pool, P.item[has_b ? it + 1 : it], jds);
+            double pa[3], va[3], pb[3], vb[3];
+            cheb_pair<FAST_NC, KU>(ra, rb, jds, pa, va, pb, vb);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                cache[(k + c) * stride] = pa[c];
+                cache[(k + 3 + c) * stride] = va[c];
+            }
+            k += 6;
+            if (has_b) {
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    cache[(k + c) * stride] = pb[c];
+                    cache[(k + 3 + c) * stride] = vb[c];
+                }
+                k += 6;
+            }
+        }
+        double cp[3] = {0.0, 0.0, 0.0};
+        const int n_items = P.n_items;
+#pragma unroll 1
+        for (int it = n_vel; it < n_items; it += 3) {
+            const double* r0 = fast_record(pool, P.item[it], jds);
+            const double* r1 = fast_record(pool, P.item[it + 1], jds);
+            const double* r2 = fast_record(pool, P.item[it + 2], jds);
+            double p3[3][3];
+            cheb_pos3<FAST_NC, KU>(r0, r1, r2, jds, p3[0], p3[1], p3[2]);
+#pragma unroll
+            for (int h = 0; h < 3; ++h) {
+                const FastItem& I = P.item[it + h];
+                double* bp = p3[h];
+                if (I.role == -2) continue;
+                if (I.role < 0) {
+                    cp[0] = bp[0]; cp[1] = bp[1]; cp[2] = bp[2];
+                    continue;
+                }
+                if (I.chained) {
+                    bp[0] += cp[0]; bp[1] += cp[1]; bp[2] += cp[2];
+                }
+#pragma unroll
+                for (int c = 0; c < 3; ++c) cache[(k + c) * stride] = bp[c];
+                k += 3;
+            }
+        }
+    }
+
+    __device__ __forceinline__ int fast_forces(const FastPlan& P, bool exact, const double x[3],
+                                               const double v[3], const double* cache, int stride,
+                                               double out[3]) {
+        double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
+        const int n_vel = P.n_vel;
+        int k = 0;
+#pragma unroll 1
+        for (int it = 0; it < n_vel; ++it, k += 6) {
+            const FastItem& A = P.item[it];
+            const double bp[3] = {cache[k * stride], cache[(k + 1) * stride], cache[(k + 2) * stride]};
+            const double bv[3] = {cache[(k + 3) * stride], cache[(k + 4) * stride],
+                                  cache[(k + 5) * stride]};
+            const ForceEntry fe{A.mass, A.radius, 0, A.kind, A.naif_id, 0};
+            const int rc = body<true>(fe, exact, x, v, bp, bv, acc0, acc1, acc2);
+            if (rc != ST_OK) return rc;
+        }
+        const double zero[3] = {0.0, 0.0, 0.0};
+        const int n_items = P.n_items;
+#pragma unroll 1
+        for (int it = n_vel; it < n_items; ++it) {
+            const FastItem& I = P.item[it];
+            if (I.role < 0) continue;
+            const double bp[3] = {cache[k * stride], cache[(k + 1) * stride], cache[(k + 2) * stride]};
+            k += 3;
+            const ForceEntry fe{I.mass, I.radius, 0, I.kind, I.naif_id, 0};
+            const int rc = body<false>(fe, exact, x, v, bp, zero, acc0, acc1, acc2);
+            if (rc != ST_OK) return rc;
+        }
+        out[0] = acc0;
+        out[1] = acc1;
+        out[2] = acc2;
+        return ST_OK;
+    }
+
     // `exact` marks the evaluations at the integrator's accepted states: only those check
     // for impacts (r <= body radius, acceleration.rs:147-158) and update the closest-approach
     // record.  The flag is a runtime value so one copy of the force code serves every call

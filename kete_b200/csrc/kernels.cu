@@ -265,6 +265,9 @@ static const void* nodes_kernel_ptr(int variant) {
         case 3: return (const void*)nbody_nodes_kernel<1, true>;
         case 4: return (const void*)nbody_nodes_kernel<3, true>;
         case 5: return (const void*)nbody_nodes_kernel<4, true>;
+        case 6: return (const void*)nbody_nodes_kernel<1, true, true>;
+        case 7: return (const void*)nbody_nodes_kernel<3, true, true>;
+        case 8: return (const void*)nbody_nodes_kernel<4, true, true>;
         default: return (const void*)nbody_nodes_kernel<1, false>;
     }
 }
@@ -279,6 +282,9 @@ int launch_nbody_nodes(const NBodyArgs& a, int variant, int grid, cudaStream_t s
         case 3: nbody_nodes_kernel<1, true><<<grid, block, 0, stream>>>(a); break;
         case 4: nbody_nodes_kernel<3, true><<<grid, block, 0, stream>>>(a); break;
         case 5: nbody_nodes_kernel<4, true><<<grid, block, 0, stream>>>(a); break;
+        case 6: nbody_nodes_kernel<1, true, true><<<grid, block, 0, stream>>>(a); break;
+        case 7: nbody_nodes_kernel<3, true, true><<<grid, block, 0, stream>>>(a); break;
+        case 8: nbody_nodes_kernel<4, true, true><<<grid, block, 0, stream>>>(a); break;
         default: nbody_nodes_kernel<1, false><<<grid, block, 0, stream>>>(a); break;
     }
     return cuda_check(cudaGetLastError(), "nbody_nodes_kernel launch");

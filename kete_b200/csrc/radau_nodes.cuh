@@ -25,7 +25,14 @@ namespace kb {
 
 constexpr int NODE_G = 8;
 
-enum Phase : int { PH_EXACT_INIT = 0, PH_ITER = 1, PH_EXACT_STEP = 2, PH_DONE = 3 };
+enum Phase : int {
+    PH_EXACT_INIT = 0,
+    PH_ITER = 1,
+    PH_EXACT_STEP = 2,
+    PH_DONE = 3,
+    PH_WAIT = 4,      // WS: step accepted, the next one starts with the warp's other groups
+    PH_FINISHED = 5,  // WS: no object left for this group
+};
 
 __device__ __forceinline__ void nodes_store(const NBodyArgs& a, int64_t i, int rc, const double x[3],
                                             const double v[3], const SpkForce& F, double t_impact,
@@ -52,6 +59,7 @@ __device__ __forceinline__ void nodes_store(const NBodyArgs& a, int64_t i, int r
 
 constexpr int NODES_BLOCK = 128;
 constexpr int NODE_ROW = 17;  // doubles per node row in shared memory (16 used + 1 pad)
+constexpr int EPH_CACHE = 38; // WS: doubles of ephemeris cache per lane (the planets need 36)
 
 // MINB: minimum resident blocks per SM requested from the compiler (1 = no register cap);
 // the host picks the instantiation (occupancy against spills is measured, not guessed).
@@ -63,7 +71,18 @@ constexpr int NODE_ROW = 17;  // doubles per node row in shared memory (16 used 
 // below the integration tolerance; impacts and closest approaches found by lane 7 only
 // count when the iteration converges.  SE = false evaluates the updated state in a round
 // of its own, as radau.rs:331-338 does.
-template <int MINB, bool SE>
+//
+// WS (warp-synchronous steps): the corrector iterations of a step evaluate the force at the
+// same node times, so each lane keeps the bodies' positions at its last evaluation time in
+// shared memory and later iterations skip the Chebyshev records (about four fifths of an
+// evaluation).  That only saves time when no lane of the warp needs fresh records in the
+// round, so a group whose step is accepted waits until the warp's other groups have
+// finished their steps too, and all of them start their next steps in the same round; a
+// group that finished its object fetches the next one at that point as well.  Each object's
+// integration is the same as with WS = false up to rounding: the cached positions are
+// rounded to doubles before the force terms read them, where the uncached evaluation may
+// fuse the Chebyshev scaling into the difference x - body.
+template <int MINB, bool SE, bool WS = false>
 __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_nodes_kernel(NBodyArgs a) {
     // node table: per node j, w_pow[j][0..6], u_pow[j][0..6], spacing, frac2 (rows padded
     // to 17 doubles so the 8 lanes of a group read 8 different banks); row 8 is the step
@@ -75,6 +94,8 @@ __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_nodes_kernel(NBodyArg
     __shared__ double s_e[NODES_BLOCK / NODE_G][NODE_G * 3];
     // per group: the running compensations of x and v (compensated summation of the updates)
     __shared__ double s_cmp[NODES_BLOCK / NODE_G][6];
+    // WS: per lane, the bodies' positions at cache_t (slot k of lane l at k * NODES_BLOCK + l)
+    __shared__ double s_cache[WS ? EPH_CACHE * NODES_BLOCK : 1];
     for (int i = threadIdx.x; i < 9 * NODE_ROW; i += blockDim.x) {
         const int j = i / NODE_ROW, k = i % NODE_ROW;
         double val = 0.0;
@@ -112,6 +133,11 @@ __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_nodes_kernel(NBodyArg
     SpkForce F;
     F.n_force = a.n_force;
     int rc = ST_OK;
+    const FastPlan& plan = a.n_force == c_eph.n_force_planets ? c_eph.fast_planets : c_eph.fast_all;
+    const bool use_cache = WS && plan.ok && SpkForce::cached_doubles(plan) <= EPH_CACHE;
+    double* cache = s_cache + threadIdx.x;
+    double cache_t = __longlong_as_double(0x7ff8000000000000LL);  // nothing cached yet
+    bool wait_predict = false;  // WS: the waiting step starts from the predicted b
 
     auto fetch = [&]() -> bool {
         int64_t k;
@@ -174,12 +200,32 @@ __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_nodes_kernel(NBodyArg
         phase = PH_ITER;
     };
 
-    if (!fetch()) return;
-    if (rc != ST_OK) finish(rc);
+    if (!fetch()) {
+        if (!WS) return;
+        phase = PH_FINISHED;  // WS: the lanes stay for the warp's collective votes
+    } else if (rc != ST_OK) {
+        finish(rc);
+    }
 
     int obj_rounds = 0;
     const int max_obj_rounds = a.max_loops * 11;
     for (;;) {
+        if (WS) {
+            // no group of the warp in the middle of a step: waiting groups start their next
+            // steps and finished groups take their next objects, all in this round
+            const bool busy = phase == PH_ITER || phase == PH_EXACT_INIT || phase == PH_EXACT_STEP;
+            if (!__any_sync(0xffffffffu, busy)) {
+                if (phase == PH_WAIT) {
+                    start_step(wait_predict);
+                } else if (phase == PH_DONE) {
+                    obj_rounds = 0;
+                    if (!a.queue || !fetch()) phase = PH_FINISHED;
+                    else if (rc != ST_OK) finish(rc);
+                }
+            }
+            if (__all_sync(0xffffffffu, phase == PH_FINISHED)) break;
+            if (phase == PH_WAIT || phase == PH_DONE || phase == PH_FINISHED) continue;
+        }
         if (phase != PH_DONE && ++obj_rounds > max_obj_rounds) {
             finish(ST_TIMEOUT);
             continue;
@@ -224,7 +270,16 @@ __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_nodes_kernel(NBodyArg
             te = t + f * h;
         }
         double ev[3];
-        int erc = F.eval(exact, te, xe, ve, ev);
+        int erc;
+        if (use_cache && te >= plan.lo && te <= plan.hi) {
+            if (te != cache_t) {
+                F.fast_positions(plan, te, cache, NODES_BLOCK);
+                cache_t = te;
+            }
+            erc = F.fast_forces(plan, exact, xe, ve, cache, NODES_BLOCK, ev);
+        } else {
+            erc = F.eval(exact, te, xe, ve, ev);
+        }
         // any lane of the group failing fails the group (only DAF limits / impacts occur);
         // the step-end lane's outcome only counts once the iteration converges
         const unsigned bad = __ballot_sync(gmask, erc != ST_OK && !(iter_round && se_lane));
@@ -246,7 +301,12 @@ __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_nodes_kernel(NBodyArg
                 }
                 h = copysign(0.1, tf - t);
                 failures = 0;
-                start_step(false);
+                if (WS) {
+                    wait_predict = false;
+                    phase = PH_WAIT;
+                } else {
+                    start_step(false);
+                }
                 continue;
             }
             cnt.steps++;
@@ -257,7 +317,12 @@ __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_nodes_kernel(NBodyArg
                 continue;
             }
             failures = 0;
-            start_step(true);
+            if (WS) {
+                wait_predict = true;
+                phase = PH_WAIT;
+            } else {
+                start_step(true);
+            }
             continue;
         }
         // ---- corrector iteration: exchange the 7 node evaluations, form g and b ----
@@ -356,7 +421,12 @@ __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_nodes_kernel(NBodyArg
                 continue;
             }
             failures = 0;
-            start_step(true);
+            if (WS) {
+                wait_predict = true;
+                phase = PH_WAIT;
+            } else {
+                start_step(true);
+            }
             continue;
         }
         if (se_lane) {  // iteration not converged: forget the step-end lane's record

@@ -112,10 +112,12 @@ def test_spk_states_vs_oracle(gpu, oracle_spk):
 
 # launch configurations: one object per thread; eight node lanes per object without a
 # register cap; with a 128-register cap on a persistent grid that refills from a queue; and
-# the step-end-lane forms (lane 7 supplies the exact evaluation of each accepted step)
+# the step-end-lane forms (lane 7 supplies the exact evaluation of each accepted step); and
+# the warp-synchronous forms that cache the bodies' positions across a step's iterations
 CONFIGS = (dict(mode=1, variant=0, refill=0), dict(mode=2, variant=0, refill=0),
            dict(mode=2, variant=2, refill=1), dict(mode=2, variant=3, refill=1),
-           dict(mode=2, variant=5, refill=0))
+           dict(mode=2, variant=5, refill=0), dict(mode=2, variant=7, refill=1),
+           dict(mode=2, variant=6, refill=0))
 MODES = CONFIGS
 
 
@@ -143,6 +145,39 @@ def _compare_nbody(gpu, oracle, pos, vel, jd0, jd1, ng=None, frame=2, center=10,
         if ok.any():
             assert np.mean(det["counters"][0][ok] == ons[ok]) > 0.95, cfg
     return err, det, close
+
+
+@pytest.mark.parametrize("refill", [0, 1])
+def test_warp_synchronous_forms_match(gpu, refill):
+    """Variants 6-8 change only when each group's next step starts and reuse the bodies'
+    positions across a step's iterations.  The cached positions are rounded to doubles
+    before the force terms read them, where the uncached path may fuse the last multiply
+    into the difference, so results agree with the same register budget without caching to
+    rounding: statuses equal, positions within the 1e-9 AU parity bar, step counts equal
+    for nearly every object.  (The closest planet distance is sampled at the points the
+    corrector evaluates, so it moves with the iteration count, as it does between the
+    thread and node forms; it is not compared.)"""
+    n = 3000
+    pos, vel, ng = synthetic.mixed(n, seed=61, nongrav_frac=0.2)
+    rng = np.random.default_rng(62)
+    jd0 = EPOCH + rng.uniform(-30.0, 30.0, n)
+    jd1 = EPOCH + rng.uniform(-400.0, 400.0, n)
+    out = {}
+    for variant in (3, 4, 5, 6, 7, 8):
+        _set(gpu, dict(mode=2, variant=variant, refill=refill))
+        out[variant] = gpu.propagate_n_body_arrays(pos, vel, jd0, jd1, nongrav=ng, mode=2,
+                                                   with_details=True)
+    _set(gpu, dict(mode=2, variant=0, refill=0))
+    for base, ws in ((3, 6), (4, 7), (5, 8)):
+        p0, v0, s0, d0 = out[base]
+        p1, v1, s1, d1 = out[ws]
+        assert np.array_equal(s0, s1)
+        ok = s0 == 0
+        assert np.abs(p0[:, ok] - p1[:, ok]).max() < 1e-9
+        assert np.abs(v0[:, ok] - v1[:, ok]).max() < 1e-11
+        assert np.mean(d0["counters"][0][ok] == d1["counters"][0][ok]) > 0.98
+        assert np.array_equal(d0["counters"][2][ok] - d0["counters"][0][ok],
+                              d1["counters"][2][ok] - d1["counters"][0][ok])
 
 
 def test_nbody_cfg1_vs_oracle(gpu, oracle_spk):
