@@ -44,8 +44,8 @@ SPAN = 365.25
 # relativistic terms (2 x 34), solar/Jovian J2 (2 x 42), Earth J2 (30).
 FLOPS_PER_EVAL = 1802
 # ncu dram__bytes_read.sum + dram__bytes_write.sum of one node-kernel launch on the default
-# workload (profiles/nbody_nodes_kernel_10k.md)
-NODES_10K_DRAM_BYTES = 860_672 + 4_864
+# workload, per launch configuration captured (profiles/nbody_nodes_kernel_10k.md)
+NODES_10K_DRAM_BYTES = {(7, 0): 1_299_200 + 2_048, (4, 1): 860_672 + 4_864}
 FLOPS_PER_ITER = 7 * FLOPS_PER_EVAL + 1201  # 7 node evaluations + predictor/g/b/test
 FLOPS_PER_STEP = 120       # state update + step-size control
 
@@ -545,7 +545,8 @@ def run_gpu(args, world, rank, local):
         achieved = flops / (ms_step * 1e-3) / 1e12
         # DRAM bytes per launch of the node kernel from one ncu capture of this workload
         # (profiles/nbody_nodes_kernel_10k.md); other workloads have none recorded
-        traffic = NODES_10K_DRAM_BYTES if (kind == "nbody_mba_10k" and best.get("mode") == 2) else None
+        traffic = (NODES_10K_DRAM_BYTES.get((best.get("variant"), best.get("refill")))
+                   if (kind == "nbody_mba_10k" and best.get("mode") == 2) else None)
         roof = {"bound": "fp64", "achieved": achieved, "peak": tflops_probe, "unit": "TFLOP/s",
                 "frac": achieved / tflops_probe if tflops_probe else None, "traffic": traffic,
                 "traffic_unit": "bytes per launch (DRAM read + write)",
@@ -810,6 +811,15 @@ def run_survey(args, world, rank, local):
         v, mags = survey_magnitudes(ff, oo, ss, table, h, pv)
         return ff, oo, ss, v, mags
 
+    # launch configuration of the chunk re-propagations, tuned on a 200k-object sample over
+    # one chunk's span (2 x dt_limit)
+    from kete_b200 import tune
+
+    m = min(n, 200_000)
+    launch, _ = tune.autotune(P[:, :m].contiguous(), V[:, :m].contiguous(),
+                              torch.full((m,), EPOCH, dtype=torch.float64, device=dev),
+                              torch.full((m,), EPOCH + 2 * SURVEY_DT_LIMIT, dtype=torch.float64,
+                                         device=dev), nongrav=G[:, :m].contiguous())
     for _ in range(args.warmup):
         chain(P, V)
     torch.cuda.synchronize()
@@ -888,6 +898,7 @@ def run_survey(args, world, rank, local):
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOADS["survey_10m"].format(n=n, f=F), "n_objects_per_gpu": n,
                    "n_fields": F, "chunks": n_chunks[0], "detections": int(len(oo)),
+                   "launch": launch,
                    "l2": "inputs (the population's states) larger than L2",
                    "parallelism": f"replicas x{world} (objects independent)"},
         "roofline": {"bound": "hbm", "kernel": "fov_prefilter_kernel (one chunk)",
