@@ -89,7 +89,8 @@ template <class Policy>
 __device__ __forceinline__ void sens_rounds(SensGroup& G, SpkForce& F, Policy& P,
                                             const double* nrow, double* sb, double* se, int lane,
                                             int comp, unsigned gmask, int warp_lane,
-                                            int max_rounds) {
+                                            int max_rounds, EphCache& C) {
+    const FastPlan& plan = F.n_force == c_eph.n_force_planets ? c_eph.fast_planets : c_eph.fast_all;
     for (int rounds = 0;; ++rounds) {
         if (G.phase == SP_BEGIN) {  // MIN_STEP, then truncate to the end (radau.rs:187-190,214-216)
             if (!P.begin_attempt(G)) {
@@ -143,7 +144,18 @@ __device__ __forceinline__ void sens_rounds(SensGroup& G, SpkForce& F, Policy& P
             te = G.t + f * G.h;
         }
         double ev[3];
-        int erc = F.eval(!iter_round, te, xe, ve, ev);
+        int erc;
+        // the corrector iterations of an attempt share their node times: the bodies'
+        // positions come from the lane's cache after the first
+        if (C.on && te >= plan.lo && te <= plan.hi) {
+            if (te != C.t) {
+                SpkForce::fast_positions(plan, te, C.p, C.stride);
+                C.t = te;
+            }
+            erc = F.fast_forces(plan, !iter_round, xe, ve, C.p, C.stride, ev);
+        } else {
+            erc = F.eval(!iter_round, te, xe, ve, ev);
+        }
         const unsigned bad = __ballot_sync(gmask, erc != ST_OK);
         if (bad) {
             const int src = __ffs(bad) - 1 - (warp_lane & ~(SG - 1));
@@ -339,6 +351,7 @@ __global__ void __launch_bounds__(SENS_BLOCK, MINB) nbody_sens_forward_kernel(Se
     __shared__ double s_node[8 * NODE_ROW_S];
     __shared__ double s_b[SENS_BLOCK / SG][21];
     __shared__ double s_e[SENS_BLOCK / SG][SG * 3];
+    __shared__ double s_cache[EPH_CACHE * SENS_BLOCK];  // per-lane body positions
     sens_load_nodes(s_node);
     __syncthreads();
     const int lane = threadIdx.x & (SG - 1);
@@ -386,7 +399,11 @@ __global__ void __launch_bounds__(SENS_BLOCK, MINB) nbody_sens_forward_kernel(Se
     __syncwarp(gmask);
     G.phase = G.rc == ST_OK ? SP_EXACT_INIT : SP_DONE;
     const int max_rounds = a.max_loops * 12;
-    sens_rounds(G, F, P, nrow, sb, se, lane, comp, gmask, warp_lane, max_rounds);
+    const FastPlan& plan = a.n_force == c_eph.n_force_planets ? c_eph.fast_planets : c_eph.fast_all;
+    EphCache C{s_cache + threadIdx.x, SENS_BLOCK,
+               plan.ok && SpkForce::cached_doubles(plan) <= EPH_CACHE,
+               __longlong_as_double(0x7ff8000000000000LL)};
+    sens_rounds(G, F, P, nrow, sb, se, lane, comp, gmask, warp_lane, max_rounds, C);
     if (lane == 0) {
         int rc = G.rc;
         if (rc == ST_OK && P.nck > a.ckpt_cap) rc = ST_CHECKPOINT_FULL;
@@ -444,10 +461,13 @@ struct SensReplayPolicy {
 // Jacobian of the force at one point (dual numbers): J (3 x 6) = d a / d(x, v) and
 // jp (3 x 2) = d a / d(A1, A2).  Out of line: one copy serves every call site.
 __device__ __noinline__ int sens_jacobian(TangentForce& T, double t, const double* x,
-                                          const double* v, double* J, double* jp) {
+                                          const double* v, double* J, double* jp, EphCache& C) {
     double xx[3] = {x[0], x[1], x[2]}, vv[3] = {v[0], v[1], v[2]};
     double ev[3], JJ[3][6], jj[3][2];
-    const int rc = T.eval(false, t, xx, vv, ev, JJ, jj);
+    const FastPlan& plan = T.n_force == c_eph.n_force_planets ? c_eph.fast_planets : c_eph.fast_all;
+    const int rc = (C.on && t >= plan.lo && t <= plan.hi)
+                       ? T.eval_cached(plan, C, t, xx, vv, ev, JJ, jj)
+                       : T.eval(false, t, xx, vv, ev, JJ, jj);
 #pragma unroll
     for (int r = 0; r < 3; ++r) {
 #pragma unroll
@@ -502,6 +522,13 @@ __global__ void __launch_bounds__(SENS_BLOCK, MINB) nbody_sens_backward_kernel(S
     T.ng = F.ng;
     T.impact_id = 0;
     T.min_dist = 1e300;
+    // per-lane body positions in dynamic shared memory (EPH_CACHE x SENS_BLOCK doubles,
+    // launch_sens_backward), shared by the replay and the Jacobian rounds
+    extern __shared__ double s_dyn[];
+    const FastPlan& plan = a.n_force == c_eph.n_force_planets ? c_eph.fast_planets : c_eph.fast_all;
+    EphCache C{s_dyn + threadIdx.x, SENS_BLOCK,
+               plan.ok && SpkForce::cached_doubles(plan) <= EPH_CACHE,
+               __longlong_as_double(0x7ff8000000000000LL)};
 
     double R[3][3];
     sens_rotation(a.frame, R);
@@ -563,7 +590,7 @@ __global__ void __launch_bounds__(SENS_BLOCK, MINB) nbody_sens_backward_kernel(S
             __syncwarp(gmask);
             G.phase = SP_BEGIN;
             SensReplayPolicy P{rec, 0, lane, sb};
-            sens_rounds(G, F, P, nrow, sb, se, lane, comp, gmask, warp_lane, max_rounds);
+            sens_rounds(G, F, P, nrow, sb, se, lane, comp, gmask, warp_lane, max_rounds, C);
             if (G.phase != SP_PAUSE) {
                 fail = G.rc != ST_OK ? G.rc : ST_TIMEOUT;
                 break;
@@ -601,7 +628,7 @@ __global__ void __launch_bounds__(SENS_BLOCK, MINB) nbody_sens_backward_kernel(S
                     }
                 }
                 double J[18], jp[6];
-                const int jrc = sens_jacobian(T, te, xe, ve, J, jp);
+                const int jrc = sens_jacobian(T, te, xe, ve, J, jp, C);
                 const unsigned bad = __ballot_sync(gmask, jrc != ST_OK && (lane < 7 || conv));
                 if (bad) {
                     fail = ST_DAF_LIMITS;
@@ -718,7 +745,7 @@ __global__ void __launch_bounds__(SENS_BLOCK, MINB) nbody_sens_backward_kernel(S
         if (c1 > c0) {
             const double* c = ck + (size_t)c0 * SENS_STRIDE;
             double J[18], jp[6];
-            const int jrc = sens_jacobian(T, c[0], c + 4, c + 7, J, jp);
+            const int jrc = sens_jacobian(T, c[0], c + 4, c + 7, J, jp, C);
             if (__any_sync(gmask, jrc != ST_OK)) {
                 fail = ST_DAF_LIMITS;
                 break;

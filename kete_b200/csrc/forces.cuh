@@ -175,6 +175,16 @@ __device__ __forceinline__ int from_ssb_equatorial(double t, int frame, const Ce
     return ST_OK;
 }
 
+// Per-lane cache of the bodies' positions at one time (the fast plan's layout, see
+// SpkForceT::fast_positions) in shared memory: slot k of a lane at p[k * stride].
+constexpr int EPH_CACHE = 38;  // doubles reserved per lane (the planets need 36)
+struct EphCache {
+    double* p;
+    int stride;
+    bool on;   // the plan fits and the cache is in use
+    double t;  // time of the cached positions (NaN: none)
+};
+
 // Acceleration from the SPK perturbers (spk_accel, acceleration.rs:121-168).  KU: the
 // Chebyshev loops' unrolling (cheb_pair); SpkForce is the lane-parallel kernels' compact form.
 template <int KU>
@@ -340,8 +350,8 @@ struct SpkForceT {
         return k;
     }
 
-    __device__ __forceinline__ void fast_positions(const FastPlan& P, double t, double* cache,
-                                                   int stride) const {
+    __device__ __forceinline__ static void fast_positions(const FastPlan& P, double t,
+                                                          double* cache, int stride) {
         const double jds = __dmul_rn(t - 2451545.0, 86400.0);
         const double* pool = c_eph.pool;
         const int n_vel = P.n_vel;

@@ -876,7 +876,23 @@ int launch_sens_forward(const SensArgs& a, cudaStream_t stream) {
 int launch_sens_backward(const SensArgs& a, cudaStream_t stream) {
     if (a.n <= 0) return 0;
     const int64_t threads = a.n * SG;
-    nbody_sens_backward_kernel<1><<<(unsigned)((threads + SENS_BLOCK - 1) / SENS_BLOCK), SENS_BLOCK, 0, stream>>>(a);
+    // the per-lane ephemeris cache takes the block past the 48 KB of shared memory a kernel
+    // gets without opting in: opt in once per device
+    constexpr int cache_bytes = EPH_CACHE * SENS_BLOCK * (int)sizeof(double);
+    static bool opted[64] = {};
+    int dev = 0;
+    int rc = cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    if (rc) return rc;
+    if (dev < 0 || dev >= 64) return cuda_check(cudaErrorInvalidDevice, "device index");
+    if (!opted[dev]) {
+        if ((rc = cuda_check(cudaFuncSetAttribute(nbody_sens_backward_kernel<1>,
+                                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                  cache_bytes),
+                             "cudaFuncSetAttribute")))
+            return rc;
+        opted[dev] = true;
+    }
+    nbody_sens_backward_kernel<1><<<(unsigned)((threads + SENS_BLOCK - 1) / SENS_BLOCK), SENS_BLOCK, cache_bytes, stream>>>(a);
     return cuda_check(cudaGetLastError(), "nbody_sens_backward_kernel launch");
 }
 

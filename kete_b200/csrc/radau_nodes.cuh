@@ -59,7 +59,6 @@ __device__ __forceinline__ void nodes_store(const NBodyArgs& a, int64_t i, int r
 
 constexpr int NODES_BLOCK = 128;
 constexpr int NODE_ROW = 17;  // doubles per node row in shared memory (16 used + 1 pad)
-constexpr int EPH_CACHE = 38; // WS: doubles of ephemeris cache per lane (the planets need 36)
 
 // MINB: minimum resident blocks per SM requested from the compiler (1 = no register cap);
 // the host picks the instantiation (occupancy against spills is measured, not guessed).

@@ -246,6 +246,48 @@ struct TangentForce {
         }
         return ST_OK;
     }
+
+    // The same (exact = false) from the fast plan's body positions in the lane's cache,
+    // evaluated at t if the cache holds another time: the bodies are summed in the fast
+    // plan's order (Sun, Jupiter, then the reference's order), a rounding-level change.
+    __device__ int eval_cached(const FastPlan& P, EphCache& C, double t, const double x[3],
+                               const double v[3], double out[3], double J[3][6],
+                               double jp[3][2]) {
+        if (t != C.t) {
+            SpkForce::fast_positions(P, t, C.p, C.stride);
+            C.t = t;
+        }
+        D6 acc[3] = {dconst(0.0), dconst(0.0), dconst(0.0)};
+        double dpar[3][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+        const double zero[3] = {0.0, 0.0, 0.0};
+        const int s = C.stride;
+        int k = 0;
+        for (int it = 0; it < P.n_items; ++it) {
+            const FastItem& I = P.item[it];
+            if (it >= P.n_vel && I.role < 0) continue;
+            const double bp[3] = {C.p[k * s], C.p[(k + 1) * s], C.p[(k + 2) * s]};
+            double bv[3] = {0.0, 0.0, 0.0};
+            if (it < P.n_vel) {
+                bv[0] = C.p[(k + 3) * s];
+                bv[1] = C.p[(k + 4) * s];
+                bv[2] = C.p[(k + 5) * s];
+                k += 6;
+            } else {
+                k += 3;
+            }
+            const ForceEntry fe{I.mass, I.radius, 0, I.kind, I.naif_id, 0};
+            body_dual(fe, ng, x, v, bp, it < P.n_vel ? bv : zero, acc, dpar);
+        }
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            out[i] = acc[i].v;
+#pragma unroll
+            for (int j = 0; j < 6; ++j) J[i][j] = acc[i].d[j];
+            jp[i][0] = dpar[i][0];
+            jp[i][1] = dpar[i][1];
+        }
+        return ST_OK;
+    }
 };
 
 }  // namespace kb
