@@ -319,7 +319,9 @@ int kete_b200_fp64_probe(int64_t iters, double* tflops, float* ms);
 /* Launch configuration of the N-body kernels (no counterpart in the reference; set by the
  * autotuner).  nodes_variant: register cap of the node-parallel kernel (0 none, 1 = 168
  * registers / 3 blocks per SM, 2 = 128 / 4), plus 3 for the form whose eighth lane
- * evaluates the step end during each corrector iteration; nodes_refill: 1 = persistent grid whose
+ * evaluates the step end during each corrector iteration, plus 6 (with the step-end lane)
+ * for the form whose lane groups start their steps together and reuse the bodies' positions
+ * across a step's corrector iterations; default 7; nodes_refill: 1 = persistent grid whose
  * lane groups take objects from a queue as they finish; thread_block: block size of the
  * one-object-per-thread kernel. */
 int kete_b200_set_launch_config(int nodes_variant, int nodes_refill, int thread_block);

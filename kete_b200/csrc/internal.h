@@ -60,7 +60,7 @@ int launch_span_order(int64_t n, const double* jd0, const double* jd1, int* scra
 
 // launch configuration chosen by the tuner (kete_b200_set_launch_config)
 struct LaunchConfig {
-    int nodes_variant = 0;  // register cap of the node kernel (see launch_nbody_nodes)
+    int nodes_variant = 7;  // node-kernel form (see launch_nbody_nodes); 7 measured fastest
     int nodes_refill = 0;   // 1: persistent grid with an object queue
     int thread_block = 128;
 };

@@ -24,10 +24,10 @@ from .propagation import propagate_n_body_arrays
 CONFIGS = [dict(mode=_lib.MODE_NODES, variant=v, refill=r) for v, r in
            itertools.product((0, 1, 2, 3, 4, 5, 6, 7, 8), (0, 1))] + [dict(mode=_lib.MODE_THREAD,
                                                                  variant=0, refill=0)]
-_current = dict(mode=_lib.MODE_NODES, variant=0, refill=0, thread_block=128)
+_current = dict(mode=_lib.MODE_NODES, variant=7, refill=0, thread_block=128)
 
 
-def set_config(mode=_lib.MODE_NODES, variant=0, refill=0, thread_block=128):
+def set_config(mode=_lib.MODE_NODES, variant=7, refill=0, thread_block=128):
     L = _lib.lib()
     L.kete_b200_set_launch_config.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int]
     _lib.check(L.kete_b200_set_launch_config(int(variant), int(refill), int(thread_block)))

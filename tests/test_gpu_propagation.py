@@ -157,6 +157,8 @@ def test_warp_synchronous_forms_match(gpu, refill):
     for nearly every object.  (The closest planet distance is sampled at the points the
     corrector evaluates, so it moves with the iteration count, as it does between the
     thread and node forms; it is not compared.)"""
+    from kete_b200 import tune
+
     n = 3000
     pos, vel, ng = synthetic.mixed(n, seed=61, nongrav_frac=0.2)
     rng = np.random.default_rng(62)
@@ -167,7 +169,7 @@ def test_warp_synchronous_forms_match(gpu, refill):
         _set(gpu, dict(mode=2, variant=variant, refill=refill))
         out[variant] = gpu.propagate_n_body_arrays(pos, vel, jd0, jd1, nongrav=ng, mode=2,
                                                    with_details=True)
-    _set(gpu, dict(mode=2, variant=0, refill=0))
+    tune.set_config()
     for base, ws in ((3, 6), (4, 7), (5, 8)):
         p0, v0, s0, d0 = out[base]
         p1, v1, s1, d1 = out[ws]
@@ -320,7 +322,7 @@ def test_mixed_coefficients_and_asteroids_vs_oracle(gpu, oracle, mixed_spk, spk_
         jd0, jd1 = np.full(n, EPOCH), np.full(n, EPOCH + 200.0)
         for inc in (False, True):
             op, ov, ost, _, _ = oracle.propagate_n_body(pos, vel, jd0, jd1, include_extended=inc)
-            for cfg in CONFIGS[:2] + CONFIGS[3:4]:
+            for cfg in CONFIGS[:2] + CONFIGS[3:4] + CONFIGS[5:6]:
                 mode = _set(gpu, cfg)
                 p, v, st = gpu.propagate_n_body_arrays(pos, vel, jd0, jd1, include_asteroids=inc,
                                                        mode=mode)
@@ -330,4 +332,6 @@ def test_mixed_coefficients_and_asteroids_vs_oracle(gpu, oracle, mixed_spk, spk_
         gpu.spice.kernel_reload([spk_path])
         oracle.spk_reset()
         oracle.spk_load_bytes(open(spk_path, "rb").read())
-        _set(gpu, dict(mode=2, variant=0, refill=0))
+        from kete_b200 import tune
+
+        tune.set_config()
