@@ -18,6 +18,7 @@ restatement of kete's path (the oracle) on all host cores on the same workload.
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import subprocess
@@ -823,13 +824,19 @@ def run_survey(args, world, rank, local):
     for _ in range(args.warmup):
         chain(P, V)
     torch.cuda.synchronize()
+    from kete_b200 import _lib as klib
+
+    count = klib.lib().kete_b200_kernel_launches
+    count.restype = ctypes.c_int64
     with ClockSampler(local) as clk:
         barrier(world)
+        launches0 = count()
         t = time.perf_counter()
         for _ in range(args.steps):
             ff, oo, ss, vmag, bmag = chain(P, V)
         torch.cuda.synchronize()
         chain_s = reduce_max((time.perf_counter() - t) / args.steps, world)
+        launches = int(count() - launches0)
         barrier(world)
     value = world * n * F / chain_s
     # end to end: the population starts in pinned host memory
@@ -916,7 +923,7 @@ def run_survey(args, world, rank, local):
         "e2e": {"value": world * n * F / e2e_s, "unit": "object-fields/s",
                 "h2d_bytes_per_step": int(pos.nbytes + vel.nbytes + ng.nbytes + table.nbytes),
                 "d2h_bytes_per_step": int(len(oo) * (4 + 4 + 56 + 8 + 16))},
-        "gpu_launches": None,
+        "gpu_launches": launches,
         "clocks": clk.summary(),
         "parity": {"sample_objects": int(len(idx)), "oracle_pairs": len(ref),
                    "gpu_pairs_in_sample": len(got), "mismatches_off_edge": mism,

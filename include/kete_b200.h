@@ -326,6 +326,10 @@ int kete_b200_fp64_probe(int64_t iters, double* tflops, float* ms);
  * one-object-per-thread kernel. */
 int kete_b200_set_launch_config(int nodes_variant, int nodes_refill, int thread_block);
 
+/* Number of kernels this library has enqueued since it was loaded (no counterpart in the
+ * reference): read it before and after a call to count the call's GPU launches. */
+int64_t kete_b200_kernel_launches(void);
+
 #ifdef __cplusplus
 }
 #endif

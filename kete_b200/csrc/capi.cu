@@ -693,6 +693,8 @@ extern "C" {
 
 int kete_b200_version(void) { return 100; }
 
+int64_t kete_b200_kernel_launches(void) { return g_kernel_launches.load(); }
+
 const char* kete_b200_last_error(void) { return g_last_error.c_str(); }
 
 int kete_b200_init(int device) {

@@ -1,5 +1,6 @@
 // internal.h -- host-side declarations shared by the C-ABI layer and the kernel TU.
 #pragma once
+#include <atomic>
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -16,6 +17,7 @@ struct EphemConst;
 // set the thread's last error message; returns `code`
 int set_error(int code, const std::string& msg);
 int cuda_check(cudaError_t e, const char* what);
+extern std::atomic<int64_t> g_kernel_launches;  // kernels.cu
 
 // kernels.cu
 int upload_tables(const Tables& t);

@@ -1,6 +1,7 @@
 // kernels.cu -- propagation kernels (two-body, N-body Radau, ephemeris queries) and their
 // host launchers.  All device constants (Radau tables, ephemeris tables) live in this
 // translation unit.
+#include <atomic>
 #include <cstdio>
 
 #include "common.cuh"
@@ -12,6 +13,15 @@
 #include "radau_nodes.cuh"
 
 namespace kb {
+
+// Kernels launched by this library since it was loaded (kete_b200_kernel_launches): every
+// launch helper below adds the kernels it enqueued when it checks the launch.
+std::atomic<int64_t> g_kernel_launches{0};
+
+static int launched(int kernels, const char* what) {
+    g_kernel_launches.fetch_add(kernels, std::memory_order_relaxed);
+    return cuda_check(cudaGetLastError(), what);
+}
 
 int upload_tables(const Tables& t) {
     return cuda_check(cudaMemcpyToSymbol(c_tab, &t, sizeof(Tables)), "upload Radau tables");
@@ -65,7 +75,7 @@ int launch_two_body(int64_t n, const double* pos, const double* vel, const doubl
     const int64_t grid = (n + block - 1) / block;
     two_body_kernel<<<(unsigned)grid, block, 0, stream>>>(n, pos, vel, jd0, jd1, obs, out_pos,
                                                           out_vel, out_jd, status);
-    return cuda_check(cudaGetLastError(), "two_body_kernel launch");
+    return launched(1, "two_body_kernel launch");
 }
 
 // -------------------------------------------------------------------------------------------
@@ -119,7 +129,7 @@ int launch_nbody_thread(const NBodyArgs& a, int block, cudaStream_t stream) {
     if (block <= 0) block = 128;
     const int64_t grid = (a.n + block - 1) / block;
     nbody_thread_kernel<<<(unsigned)grid, block, 0, stream>>>(a);
-    return cuda_check(cudaGetLastError(), "nbody_thread_kernel launch");
+    return launched(1, "nbody_thread_kernel launch");
 }
 
 // -------------------------------------------------------------------------------------------
@@ -153,7 +163,7 @@ int launch_radau_central(int64_t n, const double* pos, const double* vel, const 
     const int block = 128;
     radau_central_kernel<<<(unsigned)((n + block - 1) / block), block, 0, stream>>>(
         n, pos, vel, t0, t1, out_pos, out_vel, status);
-    return cuda_check(cudaGetLastError(), "radau_central_kernel launch");
+    return launched(1, "radau_central_kernel launch");
 }
 
 // -------------------------------------------------------------------------------------------
@@ -195,7 +205,7 @@ int launch_spk_states(int64_t n, int32_t slot, const double* jd,
     const int block = 128;
     spk_states_kernel<<<(unsigned)((n + block - 1) / block), block, 0, stream>>>(
         n, slot, jd, center_chain, frame, out6, status);
-    return cuda_check(cudaGetLastError(), "spk_states_kernel launch");
+    return launched(1, "spk_states_kernel launch");
 }
 
 }  // namespace kb
@@ -287,7 +297,7 @@ int launch_nbody_nodes(const NBodyArgs& a, int variant, int grid, cudaStream_t s
         case 8: nbody_nodes_kernel<4, true, true><<<grid, block, 0, stream>>>(a); break;
         default: nbody_nodes_kernel<1, false><<<grid, block, 0, stream>>>(a); break;
     }
-    return cuda_check(cudaGetLastError(), "nbody_nodes_kernel launch");
+    return launched(1, "nbody_nodes_kernel launch");
 }
 
 // Resident grid for the persistent (refill) form: blocks per SM from the occupancy API.
@@ -374,7 +384,7 @@ int launch_span_order(int64_t n, const double* jd0, const double* jd1, int* scra
     order_scan_kernel<<<1, 32, 0, stream>>>(scratch);
     order_scatter_kernel<<<grid, block, 0, stream>>>(n, jd0, jd1, scratch,
                                                      (int32_t*)(scratch + ORDER_SCRATCH_HEADER));
-    return cuda_check(cudaGetLastError(), "span order launch");
+    return launched(3, "span order launch");
 }
 
 }  // namespace kb
@@ -400,7 +410,7 @@ int launch_hg_mag(int64_t n, const double* s2obj, const double* s2obs, const dou
                   const double* g, double* out, cudaStream_t stream) {
     if (n <= 0) return 0;
     hg_mag_kernel<<<(unsigned)((n + 127) / 128), 128, 0, stream>>>(n, s2obj, s2obs, h, g, out);
-    return cuda_check(cudaGetLastError(), "hg_mag_kernel launch");
+    return launched(1, "hg_mag_kernel launch");
 }
 
 // -------------------------------------------------------------------------------------------
@@ -577,7 +587,7 @@ int launch_neatm(const NeatmArgs& a, cudaStream_t stream) {
         thermal_kernel<4, false><<<grid, block, 0, stream>>>(a);
     else
         thermal_kernel<MAX_BANDS, false><<<grid, block, 0, stream>>>(a);
-    return cuda_check(cudaGetLastError(), "thermal_kernel launch");
+    return launched(1, "thermal_kernel launch");
 }
 
 }  // namespace kb
@@ -589,14 +599,14 @@ namespace kb {
 int launch_fov_prefilter(const FovArgs& a, cudaStream_t stream) {
     if (a.n_obj <= 0 || a.n_fov <= 0) return 0;
     fov_prefilter_kernel<<<(unsigned)((a.n_obj + 127) / 128), 128, 0, stream>>>(a);
-    return cuda_check(cudaGetLastError(), "fov_prefilter_kernel launch");
+    return launched(1, "fov_prefilter_kernel launch");
 }
 
 int launch_fov_gather(const FovArgs& a, int64_t m, double* gpos, double* gvel, double* gjd0,
                       double* gjd1, cudaStream_t stream) {
     if (m <= 0) return 0;
     fov_gather_kernel<<<(unsigned)((m + 127) / 128), 128, 0, stream>>>(a, m, gpos, gvel, gjd0, gjd1);
-    return cuda_check(cudaGetLastError(), "fov_gather_kernel launch");
+    return launched(1, "fov_gather_kernel launch");
 }
 
 int launch_fov_contains(int64_t n_vec, const double* vec, int64_t n_fov, const double* fov,
@@ -605,14 +615,14 @@ int launch_fov_contains(int64_t n_vec, const double* vec, int64_t n_fov, const d
     if (n_vec <= 0 || n_fov <= 0) return 0;
     fov_contains_kernel<<<(unsigned)((n_vec + 127) / 128), 128, 0, stream>>>(
         n_vec, vec, n_fov, fov, capacity, counter, out_fov, out_idx);
-    return cuda_check(cudaGetLastError(), "fov_contains_kernel launch");
+    return launched(1, "fov_contains_kernel launch");
 }
 
 int launch_fov_finish(const FovArgs& a, int64_t m, const double* npos, const double* nvel,
                       const int32_t* nst, cudaStream_t stream) {
     if (m <= 0) return 0;
     fov_nbody_finish_kernel<<<(unsigned)((m + 127) / 128), 128, 0, stream>>>(a, m, npos, nvel, nst);
-    return cuda_check(cudaGetLastError(), "fov_nbody_finish_kernel launch");
+    return launched(1, "fov_nbody_finish_kernel launch");
 }
 
 }  // namespace kb
@@ -856,7 +866,7 @@ __global__ void __launch_bounds__(64) nbody_stm_kernel(StmArgs a) {
 int launch_nbody_stm(const StmArgs& a, cudaStream_t stream) {
     if (a.n <= 0) return 0;
     nbody_stm_kernel<<<(unsigned)((a.n + 63) / 64), 64, 0, stream>>>(a);
-    return cuda_check(cudaGetLastError(), "nbody_stm_kernel launch");
+    return launched(1, "nbody_stm_kernel launch");
 }
 
 }  // namespace kb
@@ -870,7 +880,7 @@ int launch_sens_forward(const SensArgs& a, cudaStream_t stream) {
     if (a.n <= 0) return 0;
     const int64_t threads = a.n * SG;
     nbody_sens_forward_kernel<1><<<(unsigned)((threads + SENS_BLOCK - 1) / SENS_BLOCK), SENS_BLOCK, 0, stream>>>(a);
-    return cuda_check(cudaGetLastError(), "nbody_sens_forward_kernel launch");
+    return launched(1, "nbody_sens_forward_kernel launch");
 }
 
 int launch_sens_backward(const SensArgs& a, cudaStream_t stream) {
@@ -893,7 +903,7 @@ int launch_sens_backward(const SensArgs& a, cudaStream_t stream) {
         opted[dev] = true;
     }
     nbody_sens_backward_kernel<1><<<(unsigned)((threads + SENS_BLOCK - 1) / SENS_BLOCK), SENS_BLOCK, cache_bytes, stream>>>(a);
-    return cuda_check(cudaGetLastError(), "nbody_sens_backward_kernel launch");
+    return launched(1, "nbody_sens_backward_kernel launch");
 }
 
 }  // namespace kb
@@ -905,7 +915,7 @@ int launch_nbody_long(const LongArgs& a, cudaStream_t stream) {
     const int64_t n_batch = (a.n + a.batch - 1) / a.batch;
     const int block = LONG_MASSIVE + a.batch <= 32 ? 32 : 64;
     nbody_long_kernel<<<(unsigned)n_batch, block, 0, stream>>>(a);
-    return cuda_check(cudaGetLastError(), "nbody_long_kernel launch");
+    return launched(1, "nbody_long_kernel launch");
 }
 
 }  // namespace kb
@@ -986,14 +996,14 @@ int launch_two_body_stm(int64_t n, const double* pos, const double* vel, const d
     if (n <= 0) return 0;
     two_body_stm_kernel<<<(unsigned)((n + 127) / 128), 128, 0, stream>>>(
         n, pos, vel, jd0, jd1, mu, cov, out_pos, out_vel, out_stm, out_cov, status);
-    return cuda_check(cudaGetLastError(), "two_body_stm_kernel launch");
+    return launched(1, "two_body_stm_kernel launch");
 }
 
 int launch_covariance(int64_t n, int rows, int cols, const double* phi, const double* cov,
                       double* out, cudaStream_t stream) {
     if (n <= 0) return 0;
     covariance_kernel<<<(unsigned)((n + 127) / 128), 128, 0, stream>>>(n, rows, cols, phi, cov, out);
-    return cuda_check(cudaGetLastError(), "covariance_kernel launch");
+    return launched(1, "covariance_kernel launch");
 }
 
 }  // namespace kb

@@ -335,3 +335,22 @@ def test_mixed_coefficients_and_asteroids_vs_oracle(gpu, oracle, mixed_spk, spk_
         from kete_b200 import tune
 
         tune.set_config()
+
+
+def test_kernel_launch_counter(gpu):
+    """kete_b200_kernel_launches counts the kernels each call enqueues."""
+    import ctypes
+
+    from kete_b200 import _lib
+
+    count = _lib.lib().kete_b200_kernel_launches
+    count.restype = ctypes.c_int64
+    pos, vel = synthetic.main_belt(64, seed=91)
+    jd0, jd1 = np.full(64, EPOCH), np.full(64, EPOCH + 30.0)
+    c0 = count()
+    gpu.propagate_two_body_arrays(pos, vel, jd0, jd1)
+    c1 = count()
+    gpu.propagate_n_body_arrays(pos, vel, jd0, jd1, mode=2)
+    c2 = count()
+    assert c1 - c0 == 1
+    assert c2 - c1 in (1, 4)  # node kernel, plus the three ordering kernels with refill
