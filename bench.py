@@ -915,7 +915,9 @@ def run_survey(args, world, rank, local):
                      if peaks.get("hbm_gbs") else None, "traffic": None,
                      "chunk_ms": fov_ms, "bytes_algorithmic": fov_bytes,
                      "note": "time of one chunk's fov_check_visible call (prefilter, n-body "
-                             "branch if any, result copy-back)"},
+                             "branch if any, result copy-back); the chain's dominant kernel is "
+                             "the node kernel of the chunk re-propagations (about 25 of the 27 s; "
+                             "its roofline: profiles/nbody_nodes_kernel_10k.md)"},
         "cpu_baseline": {"value": len(idx) * F / cpu_s, "unit": "object-fields/s",
                          "cores": os.cpu_count(), "kind": "port",
                          "sample": f"seeded {len(idx)}-object subsample of the population, full "
