@@ -46,7 +46,8 @@ SPAN = 365.25
 FLOPS_PER_EVAL = 1802
 # ncu dram__bytes_read.sum + dram__bytes_write.sum of one node-kernel launch on the default
 # workload, per launch configuration captured (profiles/nbody_nodes_kernel_10k.md)
-NODES_10K_DRAM_BYTES = {(7, 0): 1_299_200 + 2_048, (4, 1): 860_672 + 4_864}
+NODES_10K_DRAM_BYTES = {(7, 1): 1_438_464 + 2_471_168, (7, 0): 1_299_200 + 2_048,
+                        (4, 1): 860_672 + 4_864}
 FLOPS_PER_ITER = 7 * FLOPS_PER_EVAL + 1201  # 7 node evaluations + predictor/g/b/test
 FLOPS_PER_STEP = 120       # state update + step-size control
 
@@ -477,7 +478,7 @@ def run_gpu(args, world, rank, local):
         steps_total, iters_total, exact_total = (int(x) for x in cnt)
         flops = (iters_total * FLOPS_PER_ITER + exact_total * FLOPS_PER_EVAL +
                  steps_total * FLOPS_PER_STEP)
-    launches_per_step = (3 if (nbody and best.get("refill")) else 0) + 1
+    launches_per_step = (3 if (nbody and best.get("mode") == 2) else 0) + 1
 
     for _ in range(args.warmup):
         step(d)

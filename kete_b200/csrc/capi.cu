@@ -912,15 +912,15 @@ int kete_b200_propagate_n_body(int64_t n, const double* pos, const double* vel, 
         if ((rc = launch_nbody_thread(a, g_launch.thread_block, st))) return rc;
     } else if (mode == KETE_B200_MODE_NODES || mode == KETE_B200_MODE_AUTO) {
         int grid = 0;
-        if (g_launch.nodes_refill) {
-            // persistent grid taking objects longest span first; scratch holds the queue
-            // counter, the span histogram and the processing order
-            void* q = nullptr;
-            if ((rc = staging(*ds, 31, (ORDER_SCRATCH_HEADER + (size_t)n) * sizeof(int), &q)))
-                return rc;
-            if ((rc = launch_span_order(n, a.jd0, a.jd1, (int*)q, st))) return rc;
+        // objects in order of their work (span in orbital periods), most first; scratch holds
+        // the queue counter, the work histogram and the processing order
+        void* q = nullptr;
+        if ((rc = staging(*ds, 31, (ORDER_SCRATCH_HEADER + (size_t)n) * sizeof(int), &q)))
+            return rc;
+        if ((rc = launch_span_order(n, a.pos, a.vel, a.jd0, a.jd1, (int*)q, st))) return rc;
+        a.order = (const int32_t*)((int*)q + ORDER_SCRATCH_HEADER);
+        if (g_launch.nodes_refill) {  // persistent grid taking the next object from the queue
             a.queue = (int*)q;
-            a.order = (const int32_t*)((int*)q + ORDER_SCRATCH_HEADER);
             if ((rc = nodes_grid_size(g_launch.nodes_variant, &grid))) return rc;
             const int64_t need = (n * 8 + 127) / 128;
             if (grid > need) grid = (int)need;

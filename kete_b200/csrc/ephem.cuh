@@ -21,7 +21,7 @@ constexpr int MAX_SLOT = 32;
 constexpr int MAX_FORCE = 16;
 constexpr int MAX_CHAIN = 3;
 // span ordering of the persistent N-body grid: buckets and scratch header size (ints)
-constexpr int ORDER_BUCKETS = 64;
+constexpr int ORDER_BUCKETS = 120;
 constexpr int ORDER_SCRATCH_HEADER = 256;
 
 // Segment types held on the device: 2 and 3 (Chebyshev position / position and velocity),

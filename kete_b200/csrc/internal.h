@@ -57,7 +57,8 @@ int launch_covariance(int64_t n, int rows, int cols, const double* phi, const do
 int launch_nbody_thread(const NBodyArgs& a, int block, cudaStream_t stream);
 int launch_nbody_nodes(const NBodyArgs& a, int variant, int grid, cudaStream_t stream);
 int nodes_grid_size(int variant, int* grid);
-int launch_span_order(int64_t n, const double* jd0, const double* jd1, int* scratch,
+int launch_span_order(int64_t n, const double* pos, const double* vel, const double* jd0,
+                      const double* jd1, int* scratch,
                       cudaStream_t stream);
 
 // launch configuration chosen by the tuner (kete_b200_set_launch_config)

@@ -320,30 +320,43 @@ int nodes_grid_size(int variant, int* grid) {
 namespace kb {
 
 // -------------------------------------------------------------------------------------------
-// Processing order for the persistent (refill) grid: objects with the longest integration
-// spans first, so the groups that finish early pick up the short ones and the tail is short.
-// Spans are bucketed on a log2 scale (quarter-octave buckets); within a bucket the order is
+// Processing order of the node kernel: objects with the most work first, where the work is
+// the integration span in units of the object's orbital period (span x two-body mean motion
+// from the vis-viva energy; r^-1.5 for unbound orbits), since the Radau steps scale with
+// the orbit.  With a persistent grid the groups that finish early pick up the small ones
+// and the tail is short; with one group per object, neighbours in a warp get similar work,
+// so the warp-synchronous forms' groups wait less for each other.  Work is bucketed on a
+// log2 scale (eighth-octave buckets from 2^-8 to 2^7 radians); within a bucket the order is
 // whatever the atomics give -- it does not affect any object's result.
 //
-// Scratch layout (ints): [0] object queue, [1..64] bucket histogram, [65..128] bucket
-// cursors, then order[n] from int offset ORDER_SCRATCH_HEADER.
+// Scratch layout (ints): [0] object queue, [1..ORDER_BUCKETS] bucket histogram, then the
+// bucket cursors, then order[n] from int offset ORDER_SCRATCH_HEADER.
 // -------------------------------------------------------------------------------------------
-__device__ __forceinline__ int span_bucket(double jd0, double jd1) {
+static_assert(1 + 2 * ORDER_BUCKETS <= ORDER_SCRATCH_HEADER, "order header too small");
+
+__device__ __forceinline__ int work_bucket(int64_t i, int64_t n, const double* __restrict__ pos,
+                                           const double* __restrict__ vel, double jd0, double jd1) {
     const double span = fabs(jd1 - jd0);
-    if (!(span > 1.0)) return ORDER_BUCKETS - 1;  // short, zero or NaN spans go last
-    const int b = (int)(log2(span) * 4.0);
-    const int k = ORDER_BUCKETS - 1 - (b < 0 ? 0 : (b > ORDER_BUCKETS - 1 ? ORDER_BUCKETS - 1 : b));
-    return k;  // bucket 0 = longest spans
+    const double px = pos[i], py = pos[n + i], pz = pos[2 * n + i];
+    const double vx = vel[i], vy = vel[n + i], vz = vel[2 * n + i];
+    const double r = sqrt(px * px + py * py + pz * pz);
+    const double inv_a = 2.0 / r - (vx * vx + vy * vy + vz * vz) / GMS;
+    const double mean_motion = inv_a > 0.0 ? sqrt(GMS * inv_a * inv_a * inv_a) : sqrt(GMS / (r * r * r));
+    const double work = span * mean_motion;
+    if (!(work > 0.0) || !isfinite(work)) return ORDER_BUCKETS - 1;  // no work, NaN last
+    const int b = (int)floor(log2(work) * 8.0) + 64;
+    return ORDER_BUCKETS - 1 - (b < 0 ? 0 : (b > ORDER_BUCKETS - 1 ? ORDER_BUCKETS - 1 : b));
 }
 
-__global__ void order_hist_kernel(int64_t n, const double* __restrict__ jd0,
+__global__ void order_hist_kernel(int64_t n, const double* __restrict__ pos,
+                                  const double* __restrict__ vel, const double* __restrict__ jd0,
                                   const double* __restrict__ jd1, int* __restrict__ scratch) {
     __shared__ int h[ORDER_BUCKETS];
     for (int i = threadIdx.x; i < ORDER_BUCKETS; i += blockDim.x) h[i] = 0;
     __syncthreads();
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x)
-        atomicAdd(&h[span_bucket(jd0[i], jd1[i])], 1);
+        atomicAdd(&h[work_bucket(i, n, pos, vel, jd0[i], jd1[i])], 1);
     __syncthreads();
     for (int i = threadIdx.x; i < ORDER_BUCKETS; i += blockDim.x)
         if (h[i]) atomicAdd(&scratch[1 + i], h[i]);
@@ -359,30 +372,31 @@ __global__ void order_scan_kernel(int* __restrict__ scratch) {
     }
 }
 
-__global__ void order_scatter_kernel(int64_t n, const double* __restrict__ jd0,
+__global__ void order_scatter_kernel(int64_t n, const double* __restrict__ pos,
+                                     const double* __restrict__ vel, const double* __restrict__ jd0,
                                      const double* __restrict__ jd1, int* __restrict__ scratch,
                                      int32_t* __restrict__ order) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
-        const int b = span_bucket(jd0[i], jd1[i]);
-        const int pos = atomicAdd(&scratch[1 + ORDER_BUCKETS + b], 1);
-        if (pos >= 0 && pos < n) order[pos] = (int32_t)i;
+        const int b = work_bucket(i, n, pos, vel, jd0[i], jd1[i]);
+        const int p = atomicAdd(&scratch[1 + ORDER_BUCKETS + b], 1);
+        if (p >= 0 && p < n) order[p] = (int32_t)i;
     }
 }
 
-// Zero the header, histogram the spans, scan, scatter.  scratch must hold
+// Zero the header, histogram the work, scan, scatter.  scratch must hold
 // ORDER_SCRATCH_HEADER + n ints; order = scratch + ORDER_SCRATCH_HEADER.
-int launch_span_order(int64_t n, const double* jd0, const double* jd1, int* scratch,
-                      cudaStream_t stream) {
+int launch_span_order(int64_t n, const double* pos, const double* vel, const double* jd0,
+                      const double* jd1, int* scratch, cudaStream_t stream) {
     int rc = cuda_check(cudaMemsetAsync(scratch, 0, ORDER_SCRATCH_HEADER * sizeof(int), stream),
                         "clear order header");
     if (rc || n <= 0) return rc;
     const int block = 256;
     int64_t g = (n + block - 1) / block;
     const int grid = (int)(g > 1184 ? 1184 : g);
-    order_hist_kernel<<<grid, block, 0, stream>>>(n, jd0, jd1, scratch);
+    order_hist_kernel<<<grid, block, 0, stream>>>(n, pos, vel, jd0, jd1, scratch);
     order_scan_kernel<<<1, 32, 0, stream>>>(scratch);
-    order_scatter_kernel<<<grid, block, 0, stream>>>(n, jd0, jd1, scratch,
+    order_scatter_kernel<<<grid, block, 0, stream>>>(n, pos, vel, jd0, jd1, scratch,
                                                      (int32_t*)(scratch + ORDER_SCRATCH_HEADER));
     return launched(3, "span order launch");
 }

@@ -99,7 +99,7 @@ extern "C" int kete_b200_propagate_n_body_noalloc(
     a.min_dist = min_dist;
     a.counters = counters;
     a.max_loops = 1 << 20;
-    if ((rc = launch_span_order(n, jd0, jd1, scratch, st))) return rc;
+    if ((rc = launch_span_order(n, pos, vel, jd0, jd1, scratch, st))) return rc;
     a.queue = scratch;
     a.order = (const int32_t*)(scratch + ORDER_SCRATCH_HEADER);
     int grid = 0;
