@@ -917,7 +917,7 @@ def run_survey(args, world, rank, local):
                      "chunk_ms": fov_ms, "bytes_algorithmic": fov_bytes,
                      "note": "time of one chunk's fov_check_visible call (prefilter, n-body "
                              "branch if any, result copy-back); the chain's dominant kernel is "
-                             "the node kernel of the chunk re-propagations (about 25 of the 27 s; "
+                             "the node kernel of the chunk re-propagations (about 22 of the 24 s; "
                              "its roofline: profiles/nbody_nodes_kernel_10k.md)"},
         "cpu_baseline": {"value": len(idx) * F / cpu_s, "unit": "object-fields/s",
                          "cores": os.cpu_count(), "kind": "port",
