@@ -332,8 +332,10 @@ __device__ __forceinline__ void cheb_record3(const double* __restrict__ rec, int
 // epoch is at or after t.  Records are kept as the DAF stores them (4*MAXDIM + 11 doubles);
 // the host has checked every record's orders and step sizes, so the indices below stay in
 // bounds (KQMAX1 <= MAXDIM + 1 <= 26, KQ <= KQMAX1 - 1, no zero step).
+// work: 76 doubles per thread at work[k * stride] (shared memory), or null for local arrays.
 __device__ __forceinline__ void mda_record(const double* __restrict__ pool, const SegDesc& d,
-                                           double jds, double p[3], double v[3]) {
+                                           double jds, double p[3], double v[3],
+                                           double* work = nullptr, int stride = 1) {
     const double* epochs = pool + d.epoch_offset;
     int lo = 0, hi = d.n_rec;
     while (lo < hi) {  // first record whose final epoch is >= jds
@@ -349,41 +351,52 @@ __device__ __forceinline__ void mda_record(const double* __restrict__ pool, cons
     const double* dt_arr = rec + 7 + md;
     const int kqmax1 = (int)rec[4 * md + 7];
     const double delta = jds - rec[0];
-    double fc[25], wc[25], w[26];
+    double lfc[25], lwc[25], lw[26];
+    // the work arrays: the caller's shared-memory columns, or this thread's local arrays
+    const int sd = work ? stride : 1;
+    double* fcp = work ? work : lfc;
+    double* wcp = work ? work + 25 * stride : lwc;
+    double* wp = work ? work + 50 * stride : lw;
+#define FC(j) fcp[(j) * sd]
+#define WC(j) wcp[(j) * sd]
+#define WW(j) wp[(j) * sd]
     double tp = delta;
     for (int j = 0; j < kqmax1 - 2; ++j) {
-        fc[j] = tp / g[j];
-        wc[j] = delta / g[j];
+        FC(j) = tp / g[j];
+        WC(j) = delta / g[j];
         tp = delta + g[j];
     }
-    for (int j = 0; j < kqmax1; ++j) w[j] = 1.0 / (double)(j + 1);
+    for (int j = 0; j < kqmax1; ++j) WW(j) = 1.0 / (double)(j + 1);
     int ks = kqmax1 - 1, ks1 = ks - 1, jx = 0;
     while (ks >= 2) {
         jx += 1;
-        for (int j = 0; j < jx; ++j) w[j + ks] = fc[j] * w[j + ks1] - wc[j] * w[j + ks];
+        for (int j = 0; j < jx; ++j) WW(j + ks) = FC(j) * WW(j + ks1) - WC(j) * WW(j + ks);
         ks = ks1;
         ks1 -= 1;
     }
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
         double sum = 0.0;
-        for (int j = (int)rec[4 * md + 8 + c]; j >= 1; --j) sum += dt_arr[c * md + j - 1] * w[j + ks - 1];
+        for (int j = (int)rec[4 * md + 8 + c]; j >= 1; --j) sum += dt_arr[c * md + j - 1] * WW(j + ks - 1);
         p[c] = (ref[2 * c] + delta * (sum * delta + ref[2 * c + 1])) / AU_KM;
     }
-    for (int j = 0; j < jx; ++j) w[j + ks] = fc[j] * w[j + ks1] - wc[j] * w[j + ks];
+    for (int j = 0; j < jx; ++j) WW(j + ks) = FC(j) * WW(j + ks1) - WC(j) * WW(j + ks);
     ks -= 1;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
         double sum = 0.0;
-        for (int j = (int)rec[4 * md + 8 + c]; j >= 1; --j) sum += dt_arr[c * md + j - 1] * w[j + ks - 1];
+        for (int j = (int)rec[4 * md + 8 + c]; j >= 1; --j) sum += dt_arr[c * md + j - 1] * WW(j + ks - 1);
         v[c] = (ref[2 * c + 1] + delta * sum) / AU_KM * 86400.0;
     }
+#undef FC
+#undef WC
+#undef WW
 }
 
 // try_get_raw_state for the body in `slot`: first segment (scan order) whose
 // [jd_start, jd_end] contains jd.
 __device__ __forceinline__ int eph_raw(const EphemConst& E, int slot, double jd, double p[3],
-                                       double v[3]) {
+                                       double v[3], double* work = nullptr, int stride = 1) {
     const Slot& s = E.slot[slot];
     for (int q = 0; q < s.count; ++q) {
         const SegDesc& d = E.seg[s.first + q];
@@ -392,7 +405,7 @@ __device__ __forceinline__ int eph_raw(const EphemConst& E, int slot, double jd,
             // explicit multiply so the compiler cannot fuse it into the subtraction below
             const double jds = __dmul_rn(jd - 2451545.0, 86400.0);
             if (d.type == 1 || d.type == 21) {
-                mda_record(E.pool, d, jds, p, v);
+                mda_record(E.pool, d, jds, p, v, work, stride);
                 return ST_OK;
             }
             // record index floor((t - start) / intlen) (spk_segments.rs:358); the quotient

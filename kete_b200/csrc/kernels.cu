@@ -170,9 +170,15 @@ int launch_radau_central(int64_t n, const double* pos, const double* vel, const 
 // batched SpkCollection::try_get_state (spk.rs:87-96): state of body `slot` (chained to the
 // barycentre) minus the centre chain, in `frame`.
 // -------------------------------------------------------------------------------------------
-__global__ void spk_states_kernel(int64_t n, int32_t slot, const double* jd,
-                                  CenterChain center_chain, int frame, double* out6,
-                                  int32_t* status) {
+constexpr int SPK_BLOCK = 64;
+__global__ void __launch_bounds__(SPK_BLOCK) spk_states_kernel(int64_t n, int32_t slot,
+                                                               const double* jd,
+                                                               CenterChain center_chain,
+                                                               int frame, double* out6,
+                                                               int32_t* status) {
+    // the modified-difference work arrays of types 1/21 (76 doubles a thread) in shared
+    // memory rather than local memory
+    __shared__ double s_work[76 * SPK_BLOCK];
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const double t = jd[i];
@@ -182,7 +188,7 @@ __global__ void spk_states_kernel(int64_t n, int32_t slot, const double* jd,
     int s = slot;
     for (int k = 0; k < 3 && s >= 0 && rc == ST_OK; ++k) {
         double sp[3], sv[3];
-        rc = eph_raw(c_eph, s, t, sp, sv);
+        rc = eph_raw(c_eph, s, t, sp, sv, s_work + threadIdx.x, SPK_BLOCK);
         for (int q = 0; q < 3; ++q) {
             p[q] += sp[q];
             v[q] += sv[q];
@@ -202,7 +208,7 @@ int launch_spk_states(int64_t n, int32_t slot, const double* jd,
                       const CenterChain& center_chain, int frame, double* out6, int32_t* status,
                       cudaStream_t stream) {
     if (n <= 0) return 0;
-    const int block = 128;
+    const int block = SPK_BLOCK;
     spk_states_kernel<<<(unsigned)((n + block - 1) / block), block, 0, stream>>>(
         n, slot, jd, center_chain, frame, out6, status);
     return launched(1, "spk_states_kernel launch");
