@@ -145,6 +145,48 @@ def frm_arrays(sun2obj, sun2obs, h_mag, g_param, diam, vis_albedo, emissivity, b
                            zero_mags, wise_color_correction)
 
 
+def neatm_flux(sun2obj, sun2obs, v_albedo, g_param, beaming, diameter, wavelength,
+               emissivity=0.9):
+    """kete.flux.neatm_flux (src/kete/rust/flux/common.rs:223-261): NEATM thermal flux in
+    Jy of one object at one wavelength (nm).  Array arguments (sun2obj/sun2obs (3, n) or
+    (n, 3), parameters scalar or (n,)) return an (n,) array, computed on the GPU."""
+    return _single_band_thermal("neatm", sun2obj, sun2obs, v_albedo, g_param, diameter,
+                                wavelength, emissivity, beaming)
+
+
+def frm_flux(sun2obj, sun2obs, v_albedo, g_param, diameter, wavelength, emissivity=0.9):
+    """kete.flux.frm_flux (src/kete/rust/flux/common.rs:292-327): FRM thermal flux in Jy of
+    one object at one wavelength (nm); arrays as for ``neatm_flux``."""
+    return _single_band_thermal("frm", sun2obj, sun2obs, v_albedo, g_param, diameter,
+                                wavelength, emissivity, None)
+
+
+def _as_3n(v):
+    """(3,) -> (3, 1); (3, n) as given; (n, 3) transposed."""
+    a = np.asarray(v, dtype=np.float64)
+    if a.ndim == 1:
+        return a.reshape(3, 1)
+    return np.ascontiguousarray(a if a.shape[0] == 3 else a.T)
+
+
+def _single_band_thermal(model, sun2obj, sun2obs, v_albedo, g_param, diameter, wavelength,
+                         emissivity, beaming):
+    scalar = np.asarray(sun2obj).ndim == 1
+    s2obj = _as_3n(sun2obj)
+    n = s2obj.shape[1]
+    s2obs = np.ascontiguousarray(np.broadcast_to(_as_3n(sun2obs), (3, n)))
+    pv = np.broadcast_to(np.asarray(v_albedo, np.float64), (n,))
+    diam = np.broadcast_to(np.asarray(diameter, np.float64), (n,))
+    h = -5.0 * np.log10(diam * np.sqrt(pv) / C_V)  # HGParams::try_new with C_V (reflected.rs)
+    args = (s2obj, s2obs, h, g_param, diam, pv)
+    if model == "neatm":
+        r = neatm_arrays(*args, beaming, emissivity, [float(wavelength)], np.zeros((1, n)))
+    else:
+        r = frm_arrays(*args, emissivity, [float(wavelength)], np.zeros((1, n)))
+    out = r["thermal_fluxes"][0]
+    return float(out[0]) if scalar else out
+
+
 def _results(r, n):
     return [ModelResults(r["fluxes"][:, i], r["hg_fluxes"][:, i], r["thermal_fluxes"][:, i],
                          float(r["v_band_magnitude"][i]), float(r["v_band_flux"][i]),

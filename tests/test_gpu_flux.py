@@ -142,3 +142,23 @@ def test_band_counts_vs_oracle(gpu, oracle, model, bands):
         np.testing.assert_allclose(r["thermal_fluxes"][:, i], o["thermal_fluxes"], rtol=1e-12,
                                    atol=0.0)
         np.testing.assert_allclose(r["fluxes"][:, i], o["fluxes"], rtol=1e-12)
+
+
+def test_single_band_thermal_functions(gpu, oracle):
+    # kete.flux.neatm_flux / frm_flux (src/kete/rust/flux/common.rs:223-327): thermal flux
+    # only, one wavelength, H from the diameter and albedo
+    s2obj, s2obs = [1.5, 0.4, 0.1], [0.0, 1.0, 0.0]
+    h = -5.0 * np.log10(2.0 * np.sqrt(0.1) / 1329.0)
+    f = gpu.flux.neatm_flux(s2obj, s2obs, 0.1, 0.15, 1.2, 2.0, 12000.0)
+    o = oracle.neatm_total_flux(s2obj, s2obs, h, 0.15, 2.0, 0.1, 1.2, 0.9, [12000.0], [0.0])
+    assert abs(f / o["thermal_fluxes"][0] - 1) < 1e-12
+    f = gpu.flux.frm_flux(s2obj, s2obs, 0.1, 0.15, 2.0, 12000.0)
+    o = oracle.frm_total_flux(s2obj, s2obs, h, 0.15, 2.0, 0.1, 0.9, [12000.0], [0.0])
+    assert abs(f / o["thermal_fluxes"][0] - 1) < 1e-12
+    s2obj_n, s2obs_n = _geometries(50, 11)
+    fa = gpu.flux.frm_flux(s2obj_n, s2obs_n, 0.1, 0.15, 2.0, 22000.0)
+    assert fa.shape == (50,)
+    for i in range(0, 50, 10):
+        o = oracle.frm_total_flux(s2obj_n[:, i], s2obs_n[:, i], h, 0.15, 2.0, 0.1, 0.9,
+                                  [22000.0], [0.0])
+        assert abs(fa[i] / o["thermal_fluxes"][0] - 1) < 1e-12
