@@ -665,6 +665,16 @@ struct Stager {
 
 // Everything the allocation-free entry point needs, read under the lock without allocating:
 // the ephemeris must already be resident on the current device.
+// The node-kernel variant to launch for a force list: the warp-synchronous variants (6-8)
+// only pay off with the body-position cache, so a plan that does not fit it (or no fast plan)
+// runs their uncached twins (3-5), which integrate identically.
+int nodes_variant_for(int variant, int n_force) {
+    if (variant < 6) return variant;
+    const FastPlan& P = n_force == g_eph.n_force_planets ? g_eph.fast_planets : g_eph.fast_all;
+    if (!P.ok || fast_plan_cache_doubles(P) > EPH_CACHE) return variant - 3;
+    return variant;
+}
+
 int noalloc_snapshot(int include_asteroids, int64_t center, NBodyArgs& a, LaunchConfig& cfg) {
     std::lock_guard<std::mutex> lk(g_mu);
     if (!g_eph.loaded) return set_error(KETE_B200_E_NO_EPHEMERIS, "no SPK loaded");
@@ -682,6 +692,7 @@ int noalloc_snapshot(int include_asteroids, int64_t center, NBodyArgs& a, Launch
     if ((rc = center_chain(center, a.chain))) return rc;
     a.n_force = n_force;
     cfg = g_launch;
+    cfg.nodes_variant = nodes_variant_for(cfg.nodes_variant, n_force);
     return 0;
 }
 
@@ -919,13 +930,14 @@ int kete_b200_propagate_n_body(int64_t n, const double* pos, const double* vel, 
             return rc;
         if ((rc = launch_span_order(n, a.pos, a.vel, a.jd0, a.jd1, (int*)q, st))) return rc;
         a.order = (const int32_t*)((int*)q + ORDER_SCRATCH_HEADER);
+        const int variant = nodes_variant_for(g_launch.nodes_variant, a.n_force);
         if (g_launch.nodes_refill) {  // persistent grid taking the next object from the queue
             a.queue = (int*)q;
-            if ((rc = nodes_grid_size(g_launch.nodes_variant, &grid))) return rc;
+            if ((rc = nodes_grid_size(variant, &grid))) return rc;
             const int64_t need = (n * 8 + 127) / 128;
             if (grid > need) grid = (int)need;
         }
-        if ((rc = launch_nbody_nodes(a, g_launch.nodes_variant, grid, st))) return rc;
+        if ((rc = launch_nbody_nodes(a, variant, grid, st))) return rc;
     } else {
         return set_error(KETE_B200_E_ARGUMENT, "unknown propagation mode");
     }
@@ -1414,7 +1426,8 @@ int kete_b200_fov_check_visible(int64_t n_obj, const double* pos, const double* 
         nb.out_vel = (double*)ov;
         nb.status = (int32_t*)os;
         nb.max_loops = 1 << 20;
-        if ((rc = launch_nbody_nodes(nb, g_launch.nodes_variant, 0, st))) return rc;
+        if ((rc = launch_nbody_nodes(nb, nodes_variant_for(g_launch.nodes_variant, nb.n_force), 0, st)))
+            return rc;
         if ((rc = launch_fov_finish(a, m, (double*)op, (double*)ov, (int32_t*)os, st))) return rc;
         if ((rc = cuda_check(cudaMemcpyAsync(h, cnt, sizeof h, cudaMemcpyDeviceToHost, st), "read counters")))
             return rc;

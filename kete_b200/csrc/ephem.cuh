@@ -22,6 +22,8 @@ constexpr int MAX_FORCE = 16;
 constexpr int MAX_CHAIN = 3;
 // span ordering of the persistent N-body grid: buckets and scratch header size (ints)
 constexpr int ORDER_BUCKETS = 120;
+constexpr int EPH_CACHE = 38;  // body-position cache, doubles per lane (the planets need 36)
+
 constexpr int ORDER_SCRATCH_HEADER = 256;
 
 // Segment types held on the device: 2 and 3 (Chebyshev position / position and velocity),
@@ -94,6 +96,15 @@ struct FastPlan {
     int32_t n_vel, pad_;
     FastItem item[MAX_ITEMS];
 };
+
+// Doubles a lane's body-position cache needs for a fast plan (SpkForceT::fast_positions):
+// position and velocity of the first n_vel bodies, positions of the other force bodies.
+inline __host__ __device__ int fast_plan_cache_doubles(const FastPlan& P) {
+    int k = 6 * P.n_vel;
+    for (int it = P.n_vel; it < P.n_items; ++it)
+        if (P.item[it].role >= 0) k += 3;
+    return k;
+}
 
 struct EphemConst {
     int32_t n_seg, n_slot;

@@ -177,7 +177,6 @@ __device__ __forceinline__ int from_ssb_equatorial(double t, int frame, const Ce
 
 // Per-lane cache of the bodies' positions at one time (the fast plan's layout, see
 // SpkForceT::fast_positions) in shared memory: slot k of a lane at p[k * stride].
-constexpr int EPH_CACHE = 38;  // doubles reserved per lane (the planets need 36)
 struct EphCache {
     double* p;
     int stride;
@@ -344,10 +343,7 @@ struct SpkForceT {
     // velocities) to cache[k * stride], k = 0 .. cached_doubles(P) - 1; fast_forces sums the
     // accelerations from them in eval_fast's order.
     __device__ __forceinline__ static int cached_doubles(const FastPlan& P) {
-        int k = 6 * P.n_vel;
-        for (int it = P.n_vel; it < P.n_items; ++it)
-            if (P.item[it].role >= 0) k += 3;
-        return k;
+        return fast_plan_cache_doubles(P);
     }
 
     __device__ __forceinline__ static void fast_positions(const FastPlan& P, double t,
