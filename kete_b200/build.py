@@ -13,7 +13,9 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libketeb200.so")
-SOURCES = ["kernels.cu", "capi.cu", "noalloc.cu"]
+OBJ_DIR = os.path.join(HERE, "_build")  # object files of the incremental build (not shipped)
+SOURCES = ["sens.cu", "adjoint.cu", "nodes.cu", "kernels.cu", "long.cu", "capi.cu",
+           "noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -42,21 +44,47 @@ def needs_build() -> bool:
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 
-def build(verbose: bool = False, ptxas_info: bool = False, force: bool = False) -> str:
-    if not force and not needs_build():
-        return LIB
-    cmd = [nvcc(), *host_compiler(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "--shared",
+def _compile(src: str, obj: str, ptxas_info: bool) -> subprocess.CompletedProcess:
+    cmd = [nvcc(), *host_compiler(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-c",
            "-Xcompiler", "-fPIC", "-Xcompiler", "-O2", "-I", os.path.join(HERE, "..", "include"),
-           "-o", LIB + ".tmp", *sources(), "-lcudart_static", "-ldl", "-lpthread", "-lrt"]
+           "-o", obj, src]
     if ptxas_info:
         cmd.insert(1, "-Xptxas=-v")
+    return subprocess.run(cmd, capture_output=True, text=True)
+
+
+def build(verbose: bool = False, ptxas_info: bool = False, force: bool = False) -> str:
+    """Compile the translation units whose sources or headers changed to object files under
+    kete_b200/_build (in parallel), then link the shared library next to this file."""
+    if not force and not needs_build():
+        return LIB
+    from concurrent.futures import ThreadPoolExecutor
+
+    os.makedirs(OBJ_DIR, exist_ok=True)
+    srcs = sources()
+    objs = [os.path.join(OBJ_DIR, os.path.basename(s) + ".o") for s in srcs]
+    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if not f.endswith(".cu")]
+    headers.append(os.path.join(HERE, "..", "include", "kete_b200.h"))
+    newest_header = max(os.path.getmtime(h) for h in headers if os.path.exists(h))
+    todo = [(s, o) for s, o in zip(srcs, objs)
+            if force or ptxas_info or not os.path.exists(o)
+            or os.path.getmtime(o) < max(newest_header, os.path.getmtime(s))]
+    if todo:
+        with ThreadPoolExecutor(max_workers=len(todo)) as ex:
+            results = list(ex.map(lambda so: _compile(so[0], so[1] + ".tmp", ptxas_info), todo))
+        for (s, o), res in zip(todo, results):
+            if res.returncode != 0:
+                raise RuntimeError(f"nvcc failed on {os.path.basename(s)}:\n" + res.stdout + res.stderr)
+            if verbose or ptxas_info:
+                print(res.stdout + res.stderr, file=sys.stderr)
+            os.replace(o + ".tmp", o)
+    link = [nvcc(), *host_compiler(), *ARCH, "--shared", "-o", LIB + ".tmp", *objs,
+            "-lcudart_static", "-ldl", "-lpthread", "-lrt"]
     if verbose:
-        print(" ".join(cmd), file=sys.stderr)
-    res = subprocess.run(cmd, capture_output=True, text=True)
+        print(" ".join(link), file=sys.stderr)
+    res = subprocess.run(link, capture_output=True, text=True)
     if res.returncode != 0:
-        raise RuntimeError("nvcc failed:\n" + res.stdout + res.stderr)
-    if verbose or ptxas_info:
-        print(res.stdout + res.stderr, file=sys.stderr)
+        raise RuntimeError("nvcc link failed:\n" + res.stdout + res.stderr)
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

@@ -1,0 +1,44 @@
+// adjoint.cu -- reverse-mode gradients: the checkpointed forward pass and the discrete
+// adjoint pass (adjoint.cuh) with their host launchers.
+#include "common.cuh"
+#include "forces.cuh"
+#include "internal.h"
+#include "adjoint.cuh"
+
+namespace kb {
+KB_CONSTANT_UPLOADER(adjoint)
+}  // namespace kb
+
+namespace kb {
+
+int launch_sens_forward(const SensArgs& a, cudaStream_t stream) {
+    if (a.n <= 0) return 0;
+    const int64_t threads = a.n * SG;
+    nbody_sens_forward_kernel<1><<<(unsigned)((threads + SENS_BLOCK - 1) / SENS_BLOCK), SENS_BLOCK, 0, stream>>>(a);
+    return launched(1, "nbody_sens_forward_kernel launch");
+}
+
+int launch_sens_backward(const SensArgs& a, cudaStream_t stream) {
+    if (a.n <= 0) return 0;
+    const int64_t threads = a.n * SG;
+    // the per-lane ephemeris cache takes the block past the 48 KB of shared memory a kernel
+    // gets without opting in: opt in once per device
+    constexpr int cache_bytes = EPH_CACHE * SENS_BLOCK * (int)sizeof(double);
+    static bool opted[64] = {};
+    int dev = 0;
+    int rc = cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    if (rc) return rc;
+    if (dev < 0 || dev >= 64) return cuda_check(cudaErrorInvalidDevice, "device index");
+    if (!opted[dev]) {
+        if ((rc = cuda_check(cudaFuncSetAttribute(nbody_sens_backward_kernel<1>,
+                                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                  cache_bytes),
+                             "cudaFuncSetAttribute")))
+            return rc;
+        opted[dev] = true;
+    }
+    nbody_sens_backward_kernel<1><<<(unsigned)((threads + SENS_BLOCK - 1) / SENS_BLOCK), SENS_BLOCK, cache_bytes, stream>>>(a);
+    return launched(1, "nbody_sens_backward_kernel launch");
+}
+
+}  // namespace kb

@@ -28,6 +28,7 @@
 #pragma once
 #include "common.cuh"
 #include "forces.cuh"
+#include "radau.cuh"
 #include "internal.h"
 #include "tangent.cuh"
 
@@ -460,7 +461,7 @@ struct SensReplayPolicy {
 
 // Jacobian of the force at one point (dual numbers): J (3 x 6) = d a / d(x, v) and
 // jp (3 x 2) = d a / d(A1, A2).  Out of line: one copy serves every call site.
-__device__ __noinline__ int sens_jacobian(TangentForce& T, double t, const double* x,
+static __device__ __noinline__ int sens_jacobian(TangentForce& T, double t, const double* x,
                                           const double* v, double* J, double* jp, EphCache& C) {
     double xx[3] = {x[0], x[1], x[2]}, vv[3] = {v[0], v[1], v[2]};
     double ev[3], JJ[3][6], jj[3][2];

@@ -15,10 +15,27 @@
 
 namespace kb {
 
-// Device constants.  Only kernels.cu includes the device headers, so these are defined
-// once; the host uploads them with upload_tables / upload_ephem.
-__constant__ Tables c_tab;
-__constant__ EphemConst c_eph;
+// Device constants.  Every kernel translation unit (kernels.cu, nodes.cu, sens.cu, adjoint.cu,
+// long.cu)
+// holds its own copy (internal linkage); KB_CONSTANT_UPLOADER defines the TU's writer and
+// upload_tables / upload_ephem call all of them.
+static __constant__ Tables c_tab;
+static __constant__ EphemConst c_eph;
+
+// Defines upload_consts_<tu>(tables, ephem): copies whichever argument is non-null into this
+// translation unit's constants.
+#define KB_CONSTANT_UPLOADER(tu)                                                              \
+    int upload_consts_##tu(const Tables* t, const EphemConst* e) {                            \
+        if (t) {                                                                               \
+            const int rc = cuda_check(cudaMemcpyToSymbol(c_tab, t, sizeof(Tables)),            \
+                                      "upload Radau tables (" #tu ")");                        \
+            if (rc) return rc;                                                                 \
+        }                                                                                      \
+        if (e)                                                                                 \
+            return cuda_check(cudaMemcpyToSymbol(c_eph, e, sizeof(EphemConst)),                \
+                              "upload ephemeris table (" #tu ")");                             \
+        return 0;                                                                              \
+    }
 
 __device__ __forceinline__ void eq_to_ecl(const double v[3], double o[3]) {
     const double c = c_tab.rot_c, s = c_tab.rot_s;
@@ -70,7 +87,7 @@ struct NonGrav {
 
 // Returns the non-gravitational acceleration (added by the caller), so that no array of the
 // caller has its address taken by this out-of-line function.
-__device__ __noinline__ double3 nongrav_accel(const NonGrav ng, const double3 rp, const double3 rv) {
+static __device__ __noinline__ double3 nongrav_accel(const NonGrav ng, const double3 rp, const double3 rv) {
     const double pos_in[3] = {rp.x, rp.y, rp.z};
     const double vel[3] = {rv.x, rv.y, rv.z};
     double acc[3] = {0.0, 0.0, 0.0};

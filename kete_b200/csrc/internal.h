@@ -19,9 +19,20 @@ int set_error(int code, const std::string& msg);
 int cuda_check(cudaError_t e, const char* what);
 extern std::atomic<int64_t> g_kernel_launches;  // kernels.cu
 
-// kernels.cu
+// every launch helper adds the kernels it enqueued when it checks the launch
+inline int launched(int kernels, const char* what) {
+    g_kernel_launches.fetch_add(kernels, std::memory_order_relaxed);
+    return cuda_check(cudaGetLastError(), what);
+}
+
+// kernels.cu: write the device constants of every kernel translation unit
 int upload_tables(const Tables& t);
 int upload_ephem(const EphemConst& e);
+int upload_consts_kernels(const Tables* t, const EphemConst* e);
+int upload_consts_nodes(const Tables* t, const EphemConst* e);
+int upload_consts_sens(const Tables* t, const EphemConst* e);
+int upload_consts_adjoint(const Tables* t, const EphemConst* e);
+int upload_consts_long(const Tables* t, const EphemConst* e);
 
 struct NBodyArgs {
     int64_t n;

@@ -147,7 +147,7 @@ __device__ __forceinline__ int two_body_leaf(double time, double p[3], double v[
 
 // analytic_2_body (kepler.rs:254-297), in place.  Stack entries hold the remaining
 // half-intervals and the depth value their recursive call would receive.
-__device__ __noinline__ int analytic_2_body(double time, double p[3], double v[3]) {
+static __device__ __noinline__ int analytic_2_body(double time, double p[3], double v[3]) {
     double st_dt[12];
     int st_depth[12];
     int top = 0;

@@ -142,7 +142,7 @@ __device__ __forceinline__ int two_body_leaf_stm(double dt, double p[3], double 
 
 // analytic_2_body with the state-transition matrix Phi (row-major 6x6) chained through the
 // leaves; Phi starts as the identity.
-__device__ __noinline__ int analytic_2_body_stm(double time, double p[3], double v[3], double mu,
+static __device__ __noinline__ int analytic_2_body_stm(double time, double p[3], double v[3], double mu,
                                                 double Phi[36]) {
 #pragma unroll
     for (int k = 0; k < 36; ++k) Phi[k] = (k % 7 == 0) ? 1.0 : 0.0;

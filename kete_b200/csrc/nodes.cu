@@ -1,0 +1,66 @@
+// nodes.cu -- host launchers of the node-parallel Radau kernel (radau_nodes.cuh): every
+// register-cap / step-end / warp-synchronous instantiation the tuner chooses from.  Its own
+// translation unit so the instantiations compile in parallel with the other kernels.
+#include "common.cuh"
+#include "forces.cuh"
+#include "internal.h"
+#include "radau_nodes.cuh"
+
+namespace kb {
+KB_CONSTANT_UPLOADER(nodes)
+}  // namespace kb
+
+namespace kb {
+
+// Node-parallel Radau: 8 lanes per object.  With a.queue == null each group integrates one
+// object (grid covers n groups); with a queue the grid is persistent and groups refill.
+// variant: 0 = no register cap, 1 = >= 3 blocks/SM (168 registers), 2 = >= 4 blocks/SM;
+// +3: the step-end lane form (exact evaluations taken from lane 7, see radau_nodes.cuh).
+static const void* nodes_kernel_ptr(int variant) {
+    switch (variant) {
+        case 1: return (const void*)nbody_nodes_kernel<3, false>;
+        case 2: return (const void*)nbody_nodes_kernel<4, false>;
+        case 3: return (const void*)nbody_nodes_kernel<1, true>;
+        case 4: return (const void*)nbody_nodes_kernel<3, true>;
+        case 5: return (const void*)nbody_nodes_kernel<4, true>;
+        case 6: return (const void*)nbody_nodes_kernel<1, true, true>;
+        case 7: return (const void*)nbody_nodes_kernel<3, true, true>;
+        case 8: return (const void*)nbody_nodes_kernel<4, true, true>;
+        default: return (const void*)nbody_nodes_kernel<1, false>;
+    }
+}
+
+int launch_nbody_nodes(const NBodyArgs& a, int variant, int grid, cudaStream_t stream) {
+    if (a.n <= 0) return 0;
+    const int block = NODES_BLOCK;
+    if (grid <= 0) grid = (int)((a.n * NODE_G + block - 1) / block);
+    switch (variant) {
+        case 1: nbody_nodes_kernel<3, false><<<grid, block, 0, stream>>>(a); break;
+        case 2: nbody_nodes_kernel<4, false><<<grid, block, 0, stream>>>(a); break;
+        case 3: nbody_nodes_kernel<1, true><<<grid, block, 0, stream>>>(a); break;
+        case 4: nbody_nodes_kernel<3, true><<<grid, block, 0, stream>>>(a); break;
+        case 5: nbody_nodes_kernel<4, true><<<grid, block, 0, stream>>>(a); break;
+        case 6: nbody_nodes_kernel<1, true, true><<<grid, block, 0, stream>>>(a); break;
+        case 7: nbody_nodes_kernel<3, true, true><<<grid, block, 0, stream>>>(a); break;
+        case 8: nbody_nodes_kernel<4, true, true><<<grid, block, 0, stream>>>(a); break;
+        default: nbody_nodes_kernel<1, false><<<grid, block, 0, stream>>>(a); break;
+    }
+    return launched(1, "nbody_nodes_kernel launch");
+}
+
+// Resident grid for the persistent (refill) form: blocks per SM from the occupancy API.
+int nodes_grid_size(int variant, int* grid) {
+    int dev = 0, sms = 0, per_sm = 0;
+    int rc = cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    if (rc) return rc;
+    if ((rc = cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attr")))
+        return rc;
+    if ((rc = cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                             &per_sm, nodes_kernel_ptr(variant), NODES_BLOCK, 0),
+                         "occupancy")))
+        return rc;
+    *grid = sms * (per_sm > 0 ? per_sm : 1);
+    return 0;
+}
+
+}  // namespace kb
