@@ -1,15 +1,22 @@
 #!/usr/bin/env python
 """Benchmark: FP64 Gauss-Radau N-body propagation throughput (object-years/s) on B200.
 
-Workload (default): the plain N-body configuration -- 10,000 seeded main-belt states
-propagated 365.25 days under the Sun, eight planets and the Moon read from a seeded
-synthetic SPK type-2 ephemeris (degree-13 Chebyshev records).  One step = one propagation
-of the whole population.  ``value`` is device-resident throughput (inputs already in HBM,
-one kernel launch per step, CUDA-event timed, L2 flushed between steps); ``e2e`` is the
-same through the public C ABI with pinned host buffers (host->device and device->host
-copies inside the timed region).
+Workload (default): the batched uneven N-body configuration -- 1,000,000 seeded states
+(90% main belt, 10% NEO; 5% carry JPL comet non-gravitational A1/A2) each propagated to its
+own target epoch drawn uniform in +-5 years, under the Sun, eight planets and the Moon read
+from a seeded synthetic SPK type-2 ephemeris (degree-13 Chebyshev records).  One step = one
+propagation of the whole population by the node-parallel persistent kernel (the ordering
+kernels and the node kernel replayed from a captured CUDA graph).  ``value`` is
+device-resident throughput (inputs already in HBM, CUDA-event timed, L2 flushed between
+steps); ``e2e`` is the same through the public C ABI with pinned host buffers
+(host->device and device->host copies inside the timed region).  The same line carries the
+plain form (one thread per object, one launch per call) timed on the same inputs, the
+reverse-mode gradient cost on the differentiation workload, the CPU oracle on a seeded 1%
+subsample, and parity against the oracle on that subsample with objects that pass within
+0.01 AU of a planet reported separately.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl kete_b200|reference]
+                  [--workload nbody_mixed_1m|nbody_mba_10k|...]
 
 With N > 1 (torchrun) every rank propagates its own population (weak scaling, no data
 exchange); the time is the maximum over ranks.  ``--impl reference`` times the CPU
@@ -39,17 +46,41 @@ SPAN = 365.25
 
 # algorithmic FP64 flops (add/sub/mul = 1, fma = 2, div = 1, sqrt = 1) the force model and
 # the Radau step need, term by term, for the PLANETS force list with 14-coefficient Chebyshev
-# records: positions and velocities of the Sun and Jupiter (2 x 223: their velocities enter
-# the relativistic and non-gravitational terms), positions of the other 9 records (9 x 108),
-# Earth/Moon + barycentre (6), 10 Newtonian terms (10 x 19) with 2 relative velocities (6),
-# relativistic terms (2 x 34), solar/Jovian J2 (2 x 42), Earth J2 (30).
-FLOPS_PER_EVAL = 1802
-# ncu dram__bytes_read.sum + dram__bytes_write.sum of one node-kernel launch on the default
-# workload, per launch configuration captured (profiles/nbody_nodes_kernel_10k.md)
-NODES_10K_DRAM_BYTES = {(7, 1): 1_438_464 + 2_471_168, (7, 0): 1_299_200 + 2_048,
-                        (4, 1): 860_672 + 4_864}
-FLOPS_PER_ITER = 7 * FLOPS_PER_EVAL + 1201  # 7 node evaluations + predictor/g/b/test
+# records.  The records of one evaluation time: positions and velocities of the Sun and
+# Jupiter (2 x 223: their velocities enter the relativistic and non-gravitational terms),
+# positions of the other 9 records (9 x 108), Earth/Moon + barycentre (6) -- 1424 in all.
+# The force terms at given body positions: 10 Newtonian terms (10 x 19) with 2 relative
+# velocities (6), relativistic terms (2 x 34), solar/Jovian J2 (2 x 42), Earth J2 (30) --
+# 378 in all.
+FLOPS_RECORDS = 1424
+FLOPS_FORCE_TERMS = 378
+FLOPS_PER_EVAL = FLOPS_RECORDS + FLOPS_FORCE_TERMS  # 1802: one evaluation from scratch
+FLOPS_ITER_ALGEBRA = 1201  # predictors (840), node times (14), g (168), b (168), test (11)
+FLOPS_PER_ITER = 7 * FLOPS_PER_EVAL + FLOPS_ITER_ALGEBRA  # reference: records every node eval
 FLOPS_PER_STEP = 120       # state update + step-size control
+
+
+def flop_models(steps, iters, exact):
+    """FP64 flops of one propagation from the kernel's own counters (accepted steps,
+    corrector iterations, exact evaluations), in two models:
+    - "work": what the cached algorithm needs -- the records at the 8 distinct times of a step
+      (7 nodes + the step end) and once per object at its start, plus the force terms of
+      every node and exact evaluation and the Radau algebra;
+    - "reference": kete's own count, which evaluates the records at every node evaluation of
+      every corrector iteration (radau.rs:249-291 calls spk_accel per node)."""
+    starts = max(exact - steps, 0)
+    work = ((8 * steps + starts) * FLOPS_RECORDS +
+            iters * (7 * FLOPS_FORCE_TERMS + FLOPS_ITER_ALGEBRA) +
+            exact * FLOPS_FORCE_TERMS + steps * FLOPS_PER_STEP)
+    reference = iters * FLOPS_PER_ITER + exact * FLOPS_PER_EVAL + steps * FLOPS_PER_STEP
+    return work, reference
+
+
+# DRAM traffic of the node kernel from ncu captures (dram__bytes_read.sum +
+# dram__bytes_write.sum, one launch), per object, keyed by workload and launch configuration
+NODE_TRAFFIC = {}
+
+CLOSE_AU = 0.01  # objects whose closest planet approach is below this are reported apart
 
 
 def log(*a):
@@ -227,6 +258,12 @@ def barrier(world):
         import torch.distributed as dist
 
         dist.barrier()
+
+
+def bench_config(kind, n):
+    """The workload description both arms print (identical keys and values)."""
+    return {"workload": WORKLOADS[kind].format(n=n), "n_objects": n, "seed": 21,
+            "l2": "flushed (256 MB write) between timed GPU steps"}
 
 
 def cpu_sample(kind, n):
@@ -415,7 +452,7 @@ def run_reference(args, world, rank):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": WORKLOADS[kind].format(n=n), "n_objects": n},
+        "config": bench_config(kind, n),
         "cpu_baseline": {"value": value, "unit": unit, "cores": cores, "kind": "port",
                          "sample": sample + "; the reference Rust/rayon path cannot be built "
                                    "(no Rust toolchain), so the C restatement of kete's FP64 code "
@@ -454,7 +491,14 @@ def run_gpu(args, world, rank, local):
     best = None
     if nbody:
         if args.mode == 0:
-            best, sweep = tune.autotune(d["pos"], d["vel"], d["jd0"], d["jd1"], nongrav=d.get("ng"))
+            # a large population is tuned on a seeded eighth of it (still several waves of
+            # lane groups on 148 SMs), which keeps the sweep of every configuration short
+            sub = slice(None) if n <= 200_000 else slice(0, None, 8)
+            best, sweep = tune.autotune(d["pos"][:, sub].contiguous(),
+                                        d["vel"][:, sub].contiguous(),
+                                        d["jd0"][sub].contiguous(), d["jd1"][sub].contiguous(),
+                                        nongrav=(d["ng"][:, sub].contiguous() if "ng" in d
+                                                 else None))
         else:
             best = dict(mode=args.mode, variant=args.variant, refill=args.refill)
             tune.set_config(**best)
@@ -468,16 +512,17 @@ def run_gpu(args, world, rank, local):
         return kete_b200.propagate_two_body_arrays(arrs["pos"], arrs["vel"], arrs["jd0"],
                                                    arrs["jd1"])
 
-    flops = None
+    flops = flops_ref = None
     steps_total = iters_total = 0
+    min_dist = None
     if nbody:  # counts for the flop model (deterministic: same inputs every step)
         _, _, _, det = kete_b200.propagate_n_body_arrays(d["pos"], d["vel"], d["jd0"], d["jd1"],
                                                          nongrav=d.get("ng"), mode=best["mode"],
                                                          with_details=True)
         cnt = det["counters"].to(torch.int64).sum(dim=1).cpu().numpy()
         steps_total, iters_total, exact_total = (int(x) for x in cnt)
-        flops = (iters_total * FLOPS_PER_ITER + exact_total * FLOPS_PER_EVAL +
-                 steps_total * FLOPS_PER_STEP)
+        flops, flops_ref = flop_models(steps_total, iters_total, exact_total)
+        min_dist = det["min_dist"].cpu().numpy()
     launches_per_step = (3 if (nbody and best.get("mode") == 2) else 0) + 1
 
     for _ in range(args.warmup):
@@ -523,6 +568,33 @@ def run_gpu(args, world, rank, local):
     ms_step = 1e3 * t_total / args.steps
     value = world * units * args.steps / t_total
 
+    # the plain form on the same inputs: one thread per object, one launch per call
+    plain = None
+    if nbody and best.get("mode") != _lib.MODE_THREAD:
+        cur = tune.current()
+        tune.set_config(mode=_lib.MODE_THREAD, variant=0, refill=0)
+        plain_steps = max(1, min(args.steps, 2))
+        kete_b200.propagate_n_body_arrays(d["pos"], d["vel"], d["jd0"], d["jd1"],
+                                          nongrav=d.get("ng"), mode=_lib.MODE_THREAD)
+        torch.cuda.synchronize()
+        pev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(plain_steps)]
+        barrier(world)
+        for k in range(plain_steps):
+            flush.zero_()
+            pev[k][0].record(stream)
+            kete_b200.propagate_n_body_arrays(d["pos"], d["vel"], d["jd0"], d["jd1"],
+                                              nongrav=d.get("ng"), mode=_lib.MODE_THREAD)
+            pev[k][1].record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+        p_total = reduce_max(sum(a.elapsed_time(b) for a, b in pev) * 1e-3, world)
+        tune.set_config(**cur)
+        plain = {"form": "nbody_thread_kernel: one thread per object, one launch per call",
+                 "steps": plain_steps, "ms_per_step": 1e3 * p_total / plain_steps,
+                 "value": world * units * plain_steps / p_total, "unit": unit,
+                 "batched_over_plain": (p_total / plain_steps) / (t_total / args.steps)}
+
     # end to end through the C ABI with pinned host buffers
     hp = {k: torch.from_numpy(np.ascontiguousarray(v)).pin_memory() for k, v in host.items()}
     hnp = {k: v.numpy() for k, v in hp.items()}
@@ -545,15 +617,27 @@ def run_gpu(args, world, rank, local):
     hbm_bytes = int(h2d + d2h)
     if nbody:
         achieved = flops / (ms_step * 1e-3) / 1e12
-        # DRAM bytes per launch of the node kernel from one ncu capture of this workload
-        # (profiles/nbody_nodes_kernel_10k.md); other workloads have none recorded
-        traffic = (NODES_10K_DRAM_BYTES.get((best.get("variant"), best.get("refill")))
-                   if (kind == "nbody_mba_10k" and best.get("mode") == 2) else None)
+        achieved_ref = flops_ref / (ms_step * 1e-3) / 1e12
+        tr = NODE_TRAFFIC.get((kind, best.get("variant"), best.get("refill")))
+        traffic = None if tr is None else tr["bytes_per_object"] * n
         roof = {"bound": "fp64", "achieved": achieved, "peak": tflops_probe, "unit": "TFLOP/s",
-                "frac": achieved / tflops_probe if tflops_probe else None, "traffic": traffic,
+                "frac": achieved / tflops_probe if tflops_probe else None,
+                "flop_model": "work: records at the 8 distinct times of each step, force terms "
+                              "at every evaluation, Radau algebra (kernel counters)",
+                "flops_per_launch": flops,
+                "achieved_reference_model": achieved_ref,
+                "frac_reference_model": achieved_ref / tflops_probe if tflops_probe else None,
+                "flops_per_launch_reference_model": flops_ref,
+                "traffic": traffic,
                 "traffic_unit": "bytes per launch (DRAM read + write)",
+                "traffic_source": (None if tr is None else
+                                   f"ncu dram__bytes_read.sum + dram__bytes_write.sum of "
+                                   f"{tr['captured']}, scaled to {n} objects "
+                                   f"({tr['bytes_per_object']:.1f} B per object)"),
                 "peak_source": "measured DFMA probe (kete_b200_fp64_probe) in this run",
-                "flops_per_launch": flops, "hbm_bytes_algorithmic": hbm_bytes}
+                "hbm_bytes_algorithmic": hbm_bytes}
+        if tr is not None and tr.get("fp64_pipe") is not None:
+            roof["fp64_pipe_active_ncu"] = tr["fp64_pipe"]
     else:
         gbs = hbm_bytes / (ms_step * 1e-3) / 1e9
         roof = {"bound": "hbm", "achieved": gbs, "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
@@ -571,37 +655,60 @@ def run_gpu(args, world, rank, local):
     err = np.linalg.norm(gp - op, axis=0)
     ok = (gst == 0) & (st_cpu == 0)
     tol = 1e-9 if nbody else 1e-12
+    parity = {"objects_compared": int(ok.sum()),
+              "status_mismatches": int((gst != st_cpu).sum()),
+              "gpu_status_counts": np.bincount(gst, minlength=8).tolist(),
+              "cpu_status_counts": np.bincount(st_cpu, minlength=8).tolist(),
+              "tolerance_au": tol,
+              "sample": ("the full workload" if len(idx) == n else
+                         f"seeded 1% subsample ({len(idx)} objects, every 100th)")}
+    if nbody:
+        close = min_dist[idx] < CLOSE_AU
+        far = ok & ~close
+        near = ok & close
+        parity["max_err_au"] = float(err[far].max()) if far.any() else None
+        parity["max_err_au_note"] = (f"objects whose closest planet approach stays above "
+                                     f"{CLOSE_AU} AU")
+        parity["close_approach"] = {
+            "threshold_au": CLOSE_AU, "objects": int(close.sum()),
+            "max_err_au": float(err[near].max()) if near.any() else None,
+            "within_tolerance": int((err[near] <= tol).sum()),
+            "listed": [{"object": int(idx[i]), "min_planet_dist_au": float(min_dist[idx[i]]),
+                        "err_au": float(err[i]), "gpu_status": int(gst[i]),
+                        "cpu_status": int(st_cpu[i])}
+                       for i in np.flatnonzero(close)[:25]]}
+    else:
+        parity["max_err_au"] = float(err[ok].max()) if ok.any() else None
     line = {
         "metric": metric, "value": value, "unit": unit, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOADS[kind].format(n=n), "n_objects_per_gpu": n,
-                   "launch": best, "autotune_sweep_ms": sweep,
+        "config": bench_config(kind, n),
+        "launch": {"config": best, "autotune_sweep_ms": sweep,
+                   "autotune_inputs": ("the workload" if n <= 200_000 else
+                                       "every 8th object of the workload"),
                    "cuda_graph": graph is not None,
-                   "l2": "flushed (256 MB write) between timed steps",
                    "parallelism": f"replicas x{world} (objects independent)"},
         "roofline": roof,
         "cpu_baseline": {"value": cpu_units / cpu_dt, "unit": unit, "cores": cores,
                          "kind": "port",
                          "sample": ("the full workload" if len(idx) == n else
-                                    f"seeded 1% subsample ({len(idx)} objects)") +
+                                    f"seeded 1% subsample ({len(idx)} objects, every 100th), "
+                                    "rate per object-year") +
                                    ", oracle (C restatement of kete's FP64 path) with OpenMP on "
                                    "all host cores"},
         "e2e": {"value": e2e_value, "unit": unit, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": args.steps * launches_per_step,
         "clocks": clk.summary(),
-        "parity": {"max_err_au": float(err[ok].max()) if ok.any() else None,
-                   "objects_compared": int(ok.sum()),
-                   "status_mismatches": int((gst != st_cpu).sum()),
-                   "gpu_status_counts": np.bincount(gst, minlength=8).tolist(),
-                   "cpu_status_counts": np.bincount(st_cpu, minlength=8).tolist(),
-                   "tolerance_au": tol},
+        "parity": parity,
     }
+    if plain is not None:
+        line["plain"] = plain
     if nbody:
         line["object_steps_per_s"] = world * steps_total * args.steps / t_total
         line["corrector_iterations_per_step"] = iters_total / max(steps_total, 1)
-    if kind == "nbody_mba_10k" and not args.no_adjoint:
+    if kind in ("nbody_mba_10k", "nbody_mixed_1m") and not args.no_adjoint:
         line["adjoint"] = adjoint_section(dev, max(1, args.warmup), max(1, min(args.steps, 3)))
     print(json.dumps(line), flush=True)
 
@@ -904,7 +1011,7 @@ def run_survey(args, world, rank, local):
         "unit": "object-fields/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": chain_s * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOADS["survey_10m"].format(n=n, f=F), "n_objects_per_gpu": n,
+        "config": {"workload": WORKLOADS["survey_10m"].format(n=n, f=F), "n_objects": n,
                    "n_fields": F, "chunks": n_chunks[0], "detections": int(len(oo)),
                    "launch": launch,
                    "l2": "inputs (the population's states) larger than L2",
@@ -1115,7 +1222,7 @@ def run_long(args, world, rank, local):
         "ms_per_step": 1e3 * t_total / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOADS["nbody_long_10k"].format(n=n, years=LONG_YEARS),
-                   "n_objects_per_gpu": n, "batch": 10,
+                   "n_objects": n, "batch": 10,
                    "l2": "flushed (256 MB write) between timed steps"},
         "roofline": {"bound": "latency", "achieved": None, "peak": None, "unit": None,
                      "frac": None, "traffic": None,
@@ -1416,7 +1523,7 @@ def run_stm(args, world, rank, local):
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": WORKLOADS["stm_cov_1m"].format(n=n), "n_objects_per_gpu": n,
+        "config": {"workload": WORKLOADS["stm_cov_1m"].format(n=n), "n_objects": n,
                    "l2": "flushed (256 MB write) between timed steps"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if peak else None, "traffic": None,
@@ -1453,7 +1560,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="kete_b200", choices=["kete_b200", "reference"])
     ap.add_argument("--n", type=int, default=0, help="objects (0 = the workload's size)")
-    ap.add_argument("--workload", default="nbody_mba_10k", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="nbody_mixed_1m", choices=sorted(WORKLOADS))
     ap.add_argument("--mode", type=int, default=0, help="0 = autotune, 1 = thread, 2 = nodes")
     ap.add_argument("--variant", type=int, default=0)
     ap.add_argument("--refill", type=int, default=0)

@@ -326,6 +326,17 @@ int kete_b200_fp64_probe(int64_t iters, double* tflops, float* ms);
  * one-object-per-thread kernel. */
 int kete_b200_set_launch_config(int nodes_variant, int nodes_refill, int thread_block);
 
+/* Bound on each object's Radau step loop, in step attempts, for every N-body entry point
+ * (propagate_n_body, the sensitivity and adjoint passes, the FOV N-body branch and
+ * propagate_n_body_long).  kete's RadauIntegrator::integrate (radau.rs:160-218) loops until
+ * the target epoch is reached; on the GPU every loop is bounded so that no kernel can spin
+ * without end: an object that has not arrived after max_steps attempts gets status
+ * KETE_B200_TIMEOUT and a NaN state, and the kernel returns normally.  0 restores the
+ * defaults (2^20 attempts per object; 2^24 per batch for system integration); at most
+ * KETE_B200_STEP_LIMIT_MAX. */
+#define KETE_B200_STEP_LIMIT_MAX (1 << 24)
+int kete_b200_set_step_limit(int64_t max_steps);
+
 /* Number of kernels this library has enqueued since it was loaded (no counterpart in the
  * reference): read it before and after a call to count the call's GPU launches. */
 int64_t kete_b200_kernel_launches(void);

@@ -917,7 +917,7 @@ int kete_b200_propagate_n_body(int64_t n, const double* pos, const double* vel, 
     a.impact_jd = S.out(impact_jd, (size_t)n);
     a.min_dist = S.out(min_dist, (size_t)n);
     a.counters = S.out(counters, 3 * (size_t)n);
-    a.max_loops = 1 << 20;
+    a.max_loops = g_launch.max_loops;
     if (S.rc) return S.rc;
     if (mode == KETE_B200_MODE_THREAD) {
         if ((rc = launch_nbody_thread(a, g_launch.thread_block, st))) return rc;
@@ -1122,7 +1122,7 @@ int kete_b200_propagate_n_body_stm(int64_t n, const double* pos, const double* v
     a.out_state = S.out(out_state, (size_t)n_epochs * 6 * n);
     a.out_stm = S.out(out_stm, (size_t)n_epochs * 48 * n);
     a.status = S.out(status, (size_t)n);
-    a.max_loops = 1 << 20;
+    a.max_loops = g_launch.max_loops;
     if (S.rc) return S.rc;
     if ((rc = launch_nbody_stm(a, st))) return rc;
     return S.finish();
@@ -1173,7 +1173,7 @@ int kete_b200_propagate_n_body_checkpointed(int64_t n, const double* pos, const 
     a.ckpt = S.out(checkpoints, (size_t)n * ckpt_capacity * SENS_STRIDE);
     a.ckpt_count = S.out(ckpt_count, (size_t)n);
     a.ckpt_seg = S.out(ckpt_segment, (size_t)n_epochs * n);
-    a.max_loops = 1 << 20;
+    a.max_loops = g_launch.max_loops;
     if (S.rc) return S.rc;
     if ((rc = launch_sens_forward(a, st))) return rc;
     return S.finish();
@@ -1217,7 +1217,7 @@ int kete_b200_propagate_n_body_adjoint(int64_t n, int n_epochs, const double* ep
     a.seed = S.in(seed, (size_t)n_epochs * 6 * n);
     a.out_grad = S.out(out_grad, 8 * (size_t)n);
     a.grad_status = S.out(grad_status, (size_t)n);
-    a.max_loops = 1 << 20;
+    a.max_loops = g_launch.max_loops;
     if (S.rc) return S.rc;
     // per-object attempt records of the block being transposed (library scratch)
     void* rec;
@@ -1259,7 +1259,7 @@ int kete_b200_propagate_n_body_long(int64_t n, const double* pos, const double* 
     a.out_vel = S.out(out_vel, 3 * (size_t)n);
     a.out_planets = S.out(out_planets, 54);
     a.status = S.out(status, (size_t)n);
-    a.max_loops = 1 << 24;
+    a.max_loops = g_launch.max_loops_long;
     if (planets) {
         a.planets = S.in(planets, 54);
     } else {
@@ -1425,7 +1425,7 @@ int kete_b200_fov_check_visible(int64_t n_obj, const double* pos, const double* 
         nb.out_pos = (double*)op;
         nb.out_vel = (double*)ov;
         nb.status = (int32_t*)os;
-        nb.max_loops = 1 << 20;
+        nb.max_loops = g_launch.max_loops;
         if ((rc = launch_nbody_nodes(nb, nodes_variant_for(g_launch.nodes_variant, nb.n_force), 0, st)))
             return rc;
         if ((rc = launch_fov_finish(a, m, (double*)op, (double*)ov, (int32_t*)os, st))) return rc;
@@ -1446,6 +1446,16 @@ int kete_b200_set_launch_config(int nodes_variant, int nodes_refill, int thread_
     g_launch.nodes_variant = nodes_variant;
     g_launch.nodes_refill = nodes_refill ? 1 : 0;
     g_launch.thread_block = thread_block;
+    return 0;
+}
+
+int kete_b200_set_step_limit(int64_t max_steps) {
+    if (max_steps < 0 || max_steps > KETE_B200_STEP_LIMIT_MAX)
+        return set_error(KETE_B200_E_ARGUMENT, "step limit out of range");
+    std::lock_guard<std::mutex> lk(g_mu);
+    const LaunchConfig defaults;
+    g_launch.max_loops = max_steps ? (int)max_steps : defaults.max_loops;
+    g_launch.max_loops_long = max_steps ? (int)max_steps : defaults.max_loops_long;
     return 0;
 }
 

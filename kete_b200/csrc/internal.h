@@ -77,6 +77,10 @@ struct LaunchConfig {
     int nodes_variant = 7;  // node-kernel form (see launch_nbody_nodes); 7 measured fastest
     int nodes_refill = 0;   // 1: persistent grid with an object queue
     int thread_block = 128;
+    // bound on each object's Radau step loop (kete_b200_set_step_limit): an integration that
+    // has not reached its target after this many step attempts returns ST_TIMEOUT
+    int max_loops = 1 << 20;
+    int max_loops_long = 1 << 24;  // system integration (every batch's whole span)
 };
 LaunchConfig& launch_config();
 int noalloc_snapshot(int include_asteroids, int64_t center, NBodyArgs& a, LaunchConfig& cfg);

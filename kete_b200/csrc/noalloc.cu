@@ -98,7 +98,7 @@ extern "C" int kete_b200_propagate_n_body_noalloc(
     a.impact_jd = impact_jd;
     a.min_dist = min_dist;
     a.counters = counters;
-    a.max_loops = 1 << 20;
+    a.max_loops = cfg.max_loops;
     if ((rc = launch_span_order(n, pos, vel, jd0, jd1, scratch, st))) return rc;
     a.queue = scratch;
     a.order = (const int32_t*)(scratch + ORDER_SCRATCH_HEADER);

@@ -34,6 +34,15 @@ def set_config(mode=_lib.MODE_NODES, variant=7, refill=0, thread_block=128):
     _current.update(mode=mode, variant=variant, refill=refill, thread_block=thread_block)
 
 
+def set_step_limit(max_steps: int = 0):
+    """Bound each object's Radau step loop (kete_b200_set_step_limit): an object that has not
+    reached its target epoch after ``max_steps`` step attempts gets the Timeout status and a
+    NaN state.  0 restores the default bound."""
+    L = _lib.lib()
+    L.kete_b200_set_step_limit.argtypes = [ctypes.c_int64]
+    _lib.check(L.kete_b200_set_step_limit(int(max_steps)))
+
+
 def current():
     return dict(_current)
 
