@@ -215,6 +215,33 @@ int kete_b200_propagate_n_body_long(int64_t n, const double* pos, const double* 
                                     double* out_planets, int32_t* status, int on_device,
                                     void* stream);
 
+/* spk_accel (kete_core/propagation/acceleration.rs:121-168) at n points: the acceleration of
+ * a test particle at pos/vel (3 x n, relative to the solar-system barycentre, equatorial, AU
+ * and AU/day) at its own epoch jd[i] from the loaded SPK's PLANETS (or MASSES with
+ * include_asteroids), with the non-gravitational row nongrav (NULL or 10 x n, as for
+ * kete_b200_propagate_n_body) relative to the Sun.  exact != 0 also checks for impacts
+ * (status KETE_B200_IMPACT, impact_id).  out_acc: 3 x n AU/day^2, NaN where status != 0.
+ * The same force code as the propagation kernels. */
+int kete_b200_spk_accel(int64_t n, const double* jd, const double* pos, const double* vel,
+                        int include_asteroids, const double* nongrav, int exact, double* out_acc,
+                        int32_t* status, int32_t* impact_id, int on_device, void* stream);
+
+/* vec_accel (kete_core/propagation/acceleration.rs:197-249) on n test particles: the
+ * acceleration at pos/vel (3 x n, barycentric equatorial) from massive bodies whose states
+ * the caller gives, massive = 6 x m (x, y, z, vx, vy, vz rows, one column per body) in the
+ * order of the chosen list (constants/gravity.rs): KETE_B200_BODIES_PLANETS (m = 10: Sun,
+ * Mercury and Venus barycentres, Earth, Moon, Mars to Neptune barycentres),
+ * KETE_B200_BODIES_MASSES (m = 15: PLANETS, then Ceres, Pallas, Vesta, Hygiea, Interamnia) or
+ * KETE_B200_BODIES_SIMPLE_PLANETS (m = 9: Sun, Mercury, Venus, Earth-Moon, Mars to Neptune
+ * barycentres; the system integration's force code).  nongrav as for kete_b200_spk_accel
+ * (applied to every particle).  out_acc: 3 x n; status and impact_id as above. */
+#define KETE_B200_BODIES_PLANETS 0
+#define KETE_B200_BODIES_MASSES 1
+#define KETE_B200_BODIES_SIMPLE_PLANETS 2
+int kete_b200_vec_accel(int64_t n, int bodies, const double* massive, const double* pos,
+                        const double* vel, const double* nongrav, int exact, double* out_acc,
+                        int32_t* status, int32_t* impact_id, int on_device, void* stream);
+
 /* RadauIntegrator::integrate with central_accel (propagation/mod.rs:35-46,126-138): the
  * integrator alone, for checking it against kete's closed-form two-body result. */
 int kete_b200_radau_central(int64_t n, const double* pos, const double* vel, const double* t0,

@@ -17,6 +17,8 @@ from .propagation import (
     propagate_two_body,
     propagate_two_body_arrays,
     radau_central_arrays,
+    spk_accel_arrays,
+    vec_accel_arrays,
 )
 from .state import Frames, SimultaneousStates, State
 from .state_transition import compute_stm, propagate_covariance, propagate_covariance_n_body
@@ -47,6 +49,8 @@ __all__ = [
     "propagate_two_body",
     "propagate_two_body_arrays",
     "radau_central_arrays",
+    "spk_accel_arrays",
+    "vec_accel_arrays",
     "Frames",
     "SimultaneousStates",
     "State",

@@ -968,6 +968,84 @@ int kete_b200_radau_central(int64_t n, const double* pos, const double* vel, con
     return S.finish();
 }
 
+int kete_b200_spk_accel(int64_t n, const double* jd, const double* pos, const double* vel,
+                        int include_asteroids, const double* nongrav, int exact, double* out_acc,
+                        int32_t* status, int32_t* impact_id, int on_device, void* stream) {
+    if (n < 0 || (n > 0 && (!jd || !pos || !vel || !out_acc || !status)))
+        return set_error(KETE_B200_E_ARGUMENT, "null array");
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!g_eph.loaded) return set_error(KETE_B200_E_NO_EPHEMERIS, "no SPK loaded");
+    const int n_force = include_asteroids ? g_eph.n_force_all : g_eph.n_force_planets;
+    if (n_force == 0)
+        return set_error(KETE_B200_E_NO_EPHEMERIS,
+                         include_asteroids ? "loaded SPKs lack a perturbing asteroid or planet"
+                                           : "loaded SPKs lack a planet, the Sun or the Moon");
+    DevState* ds;
+    int rc = ensure_device(ds);
+    if (rc || n == 0) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    Stager S{*ds, st, on_device};
+    AccelArgs a;
+    std::memset(&a, 0, sizeof a);
+    a.n = n;
+    a.jd = S.in(jd, (size_t)n);
+    a.pos = S.in(pos, 3 * (size_t)n);
+    a.vel = S.in(vel, 3 * (size_t)n);
+    a.nongrav = S.in(nongrav, 10 * (size_t)n);
+    a.n_force = n_force;
+    a.exact = exact ? 1 : 0;
+    a.out = S.out(out_acc, 3 * (size_t)n);
+    a.status = S.out(status, (size_t)n);
+    a.impact_id = S.out(impact_id, (size_t)n);
+    if (S.rc) return S.rc;
+    if ((rc = launch_accel(a, false, st))) return rc;
+    return S.finish();
+}
+
+int kete_b200_vec_accel(int64_t n, int bodies, const double* massive, const double* pos,
+                        const double* vel, const double* nongrav, int exact, double* out_acc,
+                        int32_t* status, int32_t* impact_id, int on_device, void* stream) {
+    if (n < 0 || (n > 0 && (!massive || !pos || !vel || !out_acc || !status)))
+        return set_error(KETE_B200_E_ARGUMENT, "null array");
+    if (bodies != KETE_B200_BODIES_PLANETS && bodies != KETE_B200_BODIES_MASSES &&
+        bodies != KETE_B200_BODIES_SIMPLE_PLANETS)
+        return set_error(KETE_B200_E_ARGUMENT, "unknown body list");
+    std::lock_guard<std::mutex> lk(g_mu);
+    DevState* ds;
+    int rc = ensure_device(ds);
+    if (rc || n == 0) return rc;
+    AccelArgs a;
+    std::memset(&a, 0, sizeof a);
+    if (bodies == KETE_B200_BODIES_SIMPLE_PLANETS) {
+        a.simple = 1;
+        a.n_massive = 9;
+    } else {
+        a.n_massive = bodies == KETE_B200_BODIES_MASSES ? N_MASSES : N_PLANETS;
+        for (int b = 0; b < a.n_massive; ++b) {
+            ForceEntry& f = a.bodies[b];
+            f.mass = MASSES[b].mass_ratio == 1.0 ? GMS : MASSES[b].mass_ratio * GMS;
+            f.radius = MASSES[b].radius;
+            f.slot = -1;
+            f.kind = MASSES[b].kind;
+            f.naif_id = (int32_t)MASSES[b].id;
+        }
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    Stager S{*ds, st, on_device};
+    a.n = n;
+    a.massive = S.in(massive, 6 * (size_t)a.n_massive);
+    a.pos = S.in(pos, 3 * (size_t)n);
+    a.vel = S.in(vel, 3 * (size_t)n);
+    a.nongrav = S.in(nongrav, 10 * (size_t)n);
+    a.exact = exact ? 1 : 0;
+    a.out = S.out(out_acc, 3 * (size_t)n);
+    a.status = S.out(status, (size_t)n);
+    a.impact_id = S.out(impact_id, (size_t)n);
+    if (S.rc) return S.rc;
+    if ((rc = launch_accel(a, true, st))) return rc;
+    return S.finish();
+}
+
 int kete_b200_hg_apparent_mag(int64_t n, const double* sun2obj, const double* sun2obs,
                               const double* h_mag, const double* g_param, double* out_mag,
                               int on_device, void* stream) {

@@ -158,6 +158,25 @@ struct LongArgs {
 };
 int launch_nbody_long(const LongArgs& a, cudaStream_t stream);
 
+// the accelerations at n points (long.cu): spk_accel, or vec_accel under given massive bodies
+struct AccelArgs {
+    int64_t n;
+    const double* jd;       // n (spk_accel)
+    const double* pos;      // 3 x n, SSB-centred equatorial
+    const double* vel;
+    const double* nongrav;  // 10 x n or null
+    int n_force;            // spk_accel: PLANETS or MASSES length of the device force table
+    int n_massive;          // vec_accel: bodies in massive (6 x n_massive) and bodies
+    int simple;             // vec_accel: 1 = SIMPLE_PLANETS (system integration's pair term)
+    const double* massive;
+    ForceEntry bodies[MAX_FORCE];  // vec_accel with PLANETS / MASSES
+    int exact;
+    double* out;            // 3 x n
+    int32_t* status;
+    int32_t* impact_id;     // n or null
+};
+int launch_accel(const AccelArgs& a, bool vec, cudaStream_t stream);
+
 struct NeatmArgs;
 struct FovArgs;
 int launch_fov_prefilter(const FovArgs& a, cudaStream_t stream);

@@ -8,6 +8,7 @@ into libketeb200.so.  The ``*_arrays`` functions are the batched forms on SoA ar
 """
 from __future__ import annotations
 
+import ctypes as C
 import sys
 from dataclasses import dataclass
 
@@ -108,6 +109,63 @@ def propagate_n_body_arrays(pos, vel, jd0, jd1, frame=Frames.Ecliptic, center=10
     if with_details:
         return out_p, out_v, st, det
     return out_p, out_v, st
+
+
+# body lists of vec_accel_arrays, with their NAIF ids in order (constants/gravity.rs:43-153)
+BODY_LISTS = {
+    "planets": (0, (10, 1, 2, 399, 301, 4, 5, 6, 7, 8)),
+    "masses": (1, (10, 1, 2, 399, 301, 4, 5, 6, 7, 8, 20000001, 20000002, 20000004, 20000010,
+                   20000704)),
+    "simple_planets": (2, (10, 1, 2, 3, 4, 5, 6, 7, 8)),
+}
+
+
+def spk_accel_arrays(jd, pos, vel, include_asteroids=False, nongrav=None, exact=False):
+    """spk_accel (kete_core/propagation/acceleration.rs:121-168) at n points.
+
+    jd (n,); pos/vel (3, n) relative to the solar-system barycentre, equatorial; nongrav None
+    or (10, n).  Returns (acc (3, n), status (n,), impact_id (n,))."""
+    n = int(pos.shape[1])
+    _lib.init()
+    out = _alloc_like(pos, (3, n), np.float64)
+    st = _alloc_like(pos, (n,), np.int32)
+    iid = _alloc_like(pos, (n,), np.int32)
+    a = _lib.Args()
+    L = _lib.lib()
+    v = C.c_void_p
+    L.kete_b200_spk_accel.argtypes = [C.c_int64, v, v, v, C.c_int, v, C.c_int, v, v, v, C.c_int,
+                                      v]
+    _lib.check(L.kete_b200_spk_accel(n, a.ptr(jd), a.ptr(pos), a.ptr(vel),
+                                     int(bool(include_asteroids)), a.ptr(nongrav), int(exact),
+                                     a.ptr(out), a.ptr(st, np.int32), a.ptr(iid, np.int32),
+                                     a.on_device, a.stream))
+    return out, st, iid
+
+
+def vec_accel_arrays(massive, pos, vel, bodies="planets", nongrav=None, exact=False):
+    """vec_accel (acceleration.rs:197-249) on n test particles under massive bodies.
+
+    massive (6, m): barycentric equatorial states of the list ``bodies`` ("planets",
+    "masses" or "simple_planets", ids in BODY_LISTS) in its order; pos/vel (3, n).  Returns
+    (acc (3, n), status (n,), impact_id (n,))."""
+    code, ids = BODY_LISTS[bodies]
+    if tuple(massive.shape) != (6, len(ids)):
+        raise ValueError(f"massive must be (6, {len(ids)}) for {bodies}")
+    n = int(pos.shape[1])
+    _lib.init()
+    out = _alloc_like(pos, (3, n), np.float64)
+    st = _alloc_like(pos, (n,), np.int32)
+    iid = _alloc_like(pos, (n,), np.int32)
+    a = _lib.Args()
+    L = _lib.lib()
+    v = C.c_void_p
+    L.kete_b200_vec_accel.argtypes = [C.c_int64, C.c_int, v, v, v, v, C.c_int, v, v, v, C.c_int,
+                                      v]
+    _lib.check(L.kete_b200_vec_accel(n, code, a.ptr(massive), a.ptr(pos), a.ptr(vel),
+                                     a.ptr(nongrav), int(exact), a.ptr(out),
+                                     a.ptr(st, np.int32), a.ptr(iid, np.int32), a.on_device,
+                                     a.stream))
+    return out, st, iid
 
 
 def radau_central_arrays(pos, vel, t0, t1):

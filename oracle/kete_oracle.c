@@ -1534,6 +1534,48 @@ static int vec_accel(double t, const double *x, const double *v, const vec_meta 
     return KO_OK;
 }
 
+/* vec_accel (acceleration.rs:197-249) for n test particles under m massive bodies whose
+ * barycentric equatorial states the caller gives (massive: 6 x m rows x, y, z, vx, vy, vz):
+ * bodies 0 = PLANETS (MASSES[0..10)), 1 = MASSES, 2 = SIMPLE_PLANETS.  Every particle sums
+ * add_acceleration over the massive list in order, and the non-gravitational model (ng:
+ * 10 x n, column i for particle i, or NULL) relative to the Sun; exact checks r <= radius.
+ * The reference's batch quirk of skipping the first particle's model belongs to the batch
+ * integration (vec_accel above), not to this per-particle form. */
+int ko_vec_accel(int bodies, const double *massive, int64_t n, const double *pos,
+                 const double *vel, const double *ng, int exact, double *out, int32_t *status) {
+    grav_params simple[N_SIMPLE];
+    simple_params(simple);
+    const grav_params *gp = bodies == 2 ? simple : MASSES;
+    const int m = bodies == 2 ? N_SIMPLE : (bodies == 1 ? 15 : 10);
+    for (int64_t i = 0; i < n; ++i) {
+        double x[3], v[3], acc[3] = {0.0, 0.0, 0.0}, row[10];
+        for (int c = 0; c < 3; ++c) {
+            x[c] = pos[c * n + i];
+            v[c] = vel[c * n + i];
+        }
+        if (ng)
+            for (int r = 0; r < 10; ++r) row[r] = ng[r * n + i];
+        int rc = KO_OK;
+        for (int k = 0; k < m; ++k) {
+            double rp[3], rv[3], w[3] = {0.0, 0.0, 0.0};
+            for (int c = 0; c < 3; ++c) {
+                rp[c] = x[c] - massive[c * m + k];
+                rv[c] = v[c] - massive[(3 + c) * m + k];
+            }
+            if (exact && norm3(rp) <= gp[k].radius) {
+                rc = KO_IMPACT;
+                break;
+            }
+            grav_add(&gp[k], w, rp, rv);
+            if (gp[k].naif_id == 10 && ng && (int)row[0] != 0) nongrav_add(row, w, rp, rv);
+            for (int c = 0; c < 3; ++c) acc[c] += w[c];
+        }
+        for (int c = 0; c < 3; ++c) out[c * n + i] = rc == KO_OK ? acc[c] : NAN;
+        status[i] = rc;
+    }
+    return KO_OK;
+}
+
 /* RadauIntegrator::integrate / step (radau.rs:160-346) over d coordinates */
 static int radau_vec(int d, double *x, double *v, double t0, double tf, const vec_meta *m) {
     radau_init();

@@ -69,6 +69,9 @@ int ko_spk_get_states(int64_t n, int64_t id, const double *jd, int64_t center, i
 #define KO_NG_STRIDE 10
 int ko_spk_accel(double t, const double pos[3], const double vel[3], int include_extended,
                  const double *ng, int exact, double out[3], int64_t *impact_id);
+/* vec_accel for test particles under given massive bodies (0 PLANETS, 1 MASSES, 2 SIMPLE) */
+int ko_vec_accel(int bodies, const double *massive, int64_t n, const double *pos,
+                 const double *vel, const double *ng, int exact, double *out, int32_t *status);
 int ko_propagate_n_body_spk(const double pos[3], const double vel[3], double jd0,
                             int frame, int64_t center, double jd1, int include_extended,
                             const double *ng, double out_pos[3], double out_vel[3],

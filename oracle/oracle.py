@@ -52,6 +52,7 @@ def lib():
         L.ko_spk_get_states.argtypes = [C.c_int64, C.c_int64, _dp, C.c_int64, C.c_int, _dp,
                                         C.POINTER(C.c_int32), C.c_int]
         L.ko_spk_accel.argtypes = [C.c_double, _dp, _dp, C.c_int, _dp, C.c_int, _dp, _i64p]
+        L.ko_vec_accel.argtypes = [C.c_int, _dp, C.c_int64, _dp, _dp, _dp, C.c_int, _dp, _i32p]
         L.ko_propagate_n_body_spk.argtypes = [_dp, _dp, C.c_double, C.c_int, C.c_int64,
                                               C.c_double, C.c_int, _dp, _dp, _dp, _i64p, _dp,
                                               _i64p, _i64p]
@@ -203,6 +204,21 @@ def spk_accel(t, pos, vel, include_extended=False, ng=None, exact=False):
     rc = lib().ko_spk_accel(t, _p(p), _p(v), int(include_extended), _p(ngp), int(exact), _p(out),
                             C.byref(iid))
     return rc, out
+
+
+def vec_accel(bodies, massive, pos, vel, ng=None, exact=False):
+    """vec_accel on test particles: bodies 0 PLANETS, 1 MASSES, 2 SIMPLE_PLANETS; massive
+    (6, m) barycentric equatorial; pos/vel (3, n).  Returns acc (3, n), status (n,)."""
+    massive = np.ascontiguousarray(massive, dtype=np.float64)
+    pos = np.ascontiguousarray(pos, dtype=np.float64)
+    vel = np.ascontiguousarray(vel, dtype=np.float64)
+    n = pos.shape[1]
+    ngp = None if ng is None else np.ascontiguousarray(ng, dtype=np.float64)
+    out = np.zeros((3, n))
+    st = np.zeros(n, dtype=np.int32)
+    lib().ko_vec_accel(int(bodies), _p(massive), n, _p(pos), _p(vel), _p(ngp), int(exact),
+                       _p(out), st.ctypes.data_as(_i32p))
+    return out, st
 
 
 def propagate_n_body(pos, vel, jd0, jd1, frame=FRAME_ECLIPTIC, center=10,

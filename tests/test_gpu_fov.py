@@ -27,14 +27,21 @@ def _population(n, seed):
     return np.concatenate([pm, pn], axis=1), np.concatenate([vm, vn], axis=1)
 
 
-def _fields(gpu, oracle_spk, pos, jds, seed, width=1.8):
-    """Fields pointed at chosen objects (so detections exist) and at random directions."""
+def _fields(gpu, oracle_spk, pos, jds, seed, width=1.8, vel=None):
+    """Fields pointed at chosen objects (so detections exist) and at random directions; with
+    ``vel`` the chosen object is followed to the field's epoch (two-body)."""
     rng = np.random.default_rng(seed)
     fovs = []
     for k, jd in enumerate(jds):
         obs = _observer(oracle_spk, jd)
         if k % 2 == 0:
-            target = pos[:, rng.integers(pos.shape[1])] - obs[:3]
+            i = rng.integers(pos.shape[1])
+            p = pos[:, i]
+            if vel is not None:
+                tp, _, _, _ = oracle_spk.propagate_two_body(pos[:, i:i + 1], vel[:, i:i + 1],
+                                                            np.array([EPOCH]), np.array([jd]))
+                p = tp[:, 0]
+            target = p - obs[:3]
         else:
             target = rng.normal(size=3)
         o = gpu.State("observer", jd, obs[:3], obs[3:], gpu.Frames.Ecliptic, 10)
@@ -81,12 +88,15 @@ def test_check_visible_vs_oracle(gpu, oracle_spk, offset_days):
 
 
 def test_fov_state_check_schedule_vs_oracle(gpu, oracle_spk):
-    """kete.fov_state_check chunking, big/small re-propagation and per-field results."""
+    """kete.fov_state_check chunking, big/small re-propagation and per-field results.  The
+    fields span 200 days, so both re-seeding branches of checks.rs:68-85 fire: the big-step
+    copy moves on once a chunk is 50 dt_limit (150 d) from it, and the small-step population
+    restarts from the big-step copy while it is 25 dt_limit (75 d) or more away."""
     n = 1500
     pos, vel = _population(n, 21)
     rng = np.random.default_rng(22)
-    jds = np.sort(EPOCH + rng.uniform(0.0, 40.0, 30))
-    fovs = _fields(gpu, oracle_spk, pos, jds, 23, width=4.0)
+    jds = np.sort(EPOCH + rng.uniform(0.0, 200.0, 45))
+    fovs = _fields(gpu, oracle_spk, pos, jds, 23, width=4.0, vel=vel)
     states = [gpu.State(f"o{i}", EPOCH, pos[:, i], vel[:, i]) for i in range(n)]
     res = gpu.fov_state_check(states, fovs, dt_limit=3.0)
     got = {}
@@ -110,14 +120,17 @@ def test_fov_state_check_schedule_vs_oracle(gpu, oracle_spk):
         return [op, ov, p[2] & (st == 0), target]
 
     n_fields = 0
+    reseeds = resets = 0
     for chunk in chunks:
         jd_mean = (chunk[-1].jd + chunk[0].jd) / 2.0
         if abs(jd_mean - big_jd) >= dt_limit * 50:
             big_jd = jd_mean
             big = prop(big, jd)
+            reseeds += 1
         if abs(jd_mean - jd) >= dt_limit:
             if abs(jd - big_jd) >= dt_limit * 25:
                 cur = [big[0].copy(), big[1].copy(), big[2].copy(), big[3]]
+                resets += 1
             jd = jd_mean
             cur = prop(cur, jd)
         idx = np.nonzero(cur[2])[0]
@@ -135,4 +148,5 @@ def test_fov_state_check_schedule_vs_oracle(gpu, oracle_spk):
                 assert np.abs(g[d].pos - ref[d][1:4]).max() < 1e-9
             n_fields += bool(ref)
     assert n_fields >= 5
+    assert reseeds >= 1 and resets >= 1, (reseeds, resets)
     assert len(res) == sum(1 for f in fovs if id(f) in got)
