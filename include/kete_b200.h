@@ -348,7 +348,10 @@ int kete_b200_fp64_probe(int64_t iters, double* tflops, float* ms);
  * registers / 3 blocks per SM, 2 = 128 / 4), plus 3 for the form whose eighth lane
  * evaluates the step end during each corrector iteration, plus 6 (with the step-end lane)
  * for the form whose lane groups start their steps together and reuse the bodies' positions
- * across a step's corrector iterations; default 7; nodes_refill: 1 = persistent grid whose
+ * across a step's corrector iterations; 9 and 10 (168 / 128 registers) for the form that
+ * keeps that cache but lets the four objects of a warp step independently, the whole warp
+ * sharing each round's ephemeris-record evaluations; default 7; nodes_refill: 1 = persistent
+ * grid whose
  * lane groups take objects from a queue as they finish; thread_block: block size of the
  * one-object-per-thread kernel. */
 int kete_b200_set_launch_config(int nodes_variant, int nodes_refill, int thread_block);
@@ -360,7 +363,8 @@ int kete_b200_set_launch_config(int nodes_variant, int nodes_refill, int thread_
  * without end: an object that has not arrived after max_steps attempts gets status
  * KETE_B200_TIMEOUT and a NaN state, and the kernel returns normally.  0 restores the
  * defaults (2^20 attempts per object; 2^24 per batch for system integration); at most
- * KETE_B200_STEP_LIMIT_MAX. */
+ * KETE_B200_STEP_LIMIT_MAX.  The sensitivity and adjoint passes bound their rounds by 12 per
+ * attempt instead of counting attempts. */
 #define KETE_B200_STEP_LIMIT_MAX (1 << 24)
 int kete_b200_set_step_limit(int64_t max_steps);
 

@@ -671,6 +671,8 @@ struct Stager {
 int nodes_variant_for(int variant, int n_force) {
     if (variant < 6) return variant;
     const FastPlan& P = n_force == g_eph.n_force_planets ? g_eph.fast_planets : g_eph.fast_all;
+    if (variant >= 9)  // pooled: the uncached step-end form of the same register budget
+        return (!P.ok || pool_plan_doubles(P) > POOL_CACHE_DOUBLES) ? variant - 5 : variant;
     if (!P.ok || fast_plan_cache_doubles(P) > EPH_CACHE) return variant - 3;
     return variant;
 }
@@ -1517,7 +1519,7 @@ int kete_b200_fov_check_visible(int64_t n_obj, const double* pos, const double* 
 }
 
 int kete_b200_set_launch_config(int nodes_variant, int nodes_refill, int thread_block) {
-    if (nodes_variant < 0 || nodes_variant > 8 || thread_block < 32 || thread_block > 1024 ||
+    if (nodes_variant < 0 || nodes_variant > 10 || thread_block < 32 || thread_block > 1024 ||
         thread_block % 32)
         return set_error(KETE_B200_E_ARGUMENT, "bad launch configuration");
     std::lock_guard<std::mutex> lk(g_mu);

@@ -97,6 +97,18 @@ struct FastPlan {
     FastItem item[MAX_ITEMS];
 };
 
+// Body cache of the warp-pooled node kernel (radau_pool.cuh), doubles per lane: position and
+// velocity of the first n_vel items, positions of every other item but padding (centres
+// included: the bodies chained to them add the centre's position when the force terms read
+// them).  The planets need 39.
+constexpr int POOL_CACHE_DOUBLES = 40;
+inline __host__ __device__ int pool_plan_doubles(const FastPlan& P) {
+    int k = 6 * P.n_vel;
+    for (int it = P.n_vel; it < P.n_items; ++it)
+        if (P.item[it].role != -2) k += 3;
+    return k;
+}
+
 // Doubles a lane's body-position cache needs for a fast plan (SpkForceT::fast_positions):
 // position and velocity of the first n_vel bodies, positions of the other force bodies.
 inline __host__ __device__ int fast_plan_cache_doubles(const FastPlan& P) {

@@ -213,22 +213,16 @@ struct SpkForceT {
     int32_t min_id;
 
     // One body's contribution (GravParams::add_acceleration, gravity.rs:171-216, plus the
-    // non-gravitational term relative to the Sun, acceleration.rs:161-165).  VEL = false
-    // serves the bodies whose velocity does not enter the force (no relativistic or
-    // non-gravitational term): bv is then not read.
+    // non-gravitational term relative to the Sun, acceleration.rs:161-165), given the relative
+    // position rp and velocity rv, r2 = |rp|^2 and ir = rsqrt(r2).  VEL = false serves the
+    // bodies whose velocity does not enter the force (no relativistic or non-gravitational
+    // term): rv is then not read.  Callers that evaluate several bodies compute their
+    // reciprocal square roots together (independent chains) before summing the terms in the
+    // reference's order.
     template <bool VEL = true>
-    __device__ __forceinline__ int body(const ForceEntry& fe, bool exact, const double x[3],
-                                        const double v[3], const double bp[3], const double bv[3],
-                                        double& acc0, double& acc1, double& acc2) {
-        const double rp[3] = {x[0] - bp[0], x[1] - bp[1], x[2] - bp[2]};
-        double rv[3] = {0.0, 0.0, 0.0};
-        if (VEL) {
-            rv[0] = v[0] - bv[0];
-            rv[1] = v[1] - bv[1];
-            rv[2] = v[2] - bv[2];
-        }
-        const double r2 = rp[0] * rp[0] + rp[1] * rp[1] + rp[2] * rp[2];
-        const double ir = rsqrt(r2);
+    __device__ __forceinline__ int body_terms(const ForceEntry& fe, bool exact, const double rp[3],
+                                              const double rv[3], double r2, double ir,
+                                              double& acc0, double& acc1, double& acc2) {
         const double r = r2 * ir;
         const double ir3 = ir * ir * ir;
         if (exact) {
@@ -287,6 +281,24 @@ struct SpkForceT {
             acc2 += rp[2] * coef * (z_squared - 3.0);
         }
         return ST_OK;
+    }
+
+    // body_terms for the body at bp (velocity bv) seen from (x, v).  Distances use one
+    // reciprocal square root per body: r = r2 * rsqrt(r2) and r^-3 = rsqrt(r2)^3 replace the
+    // reference's sqrt and 1/(r*r*r) (a few ulp apart).
+    template <bool VEL = true>
+    __device__ __forceinline__ int body(const ForceEntry& fe, bool exact, const double x[3],
+                                        const double v[3], const double bp[3], const double bv[3],
+                                        double& acc0, double& acc1, double& acc2) {
+        const double rp[3] = {x[0] - bp[0], x[1] - bp[1], x[2] - bp[2]};
+        double rv[3] = {0.0, 0.0, 0.0};
+        if (VEL) {
+            rv[0] = v[0] - bv[0];
+            rv[1] = v[1] - bv[1];
+            rv[2] = v[2] - bv[2];
+        }
+        const double r2 = rp[0] * rp[0] + rp[1] * rp[1] + rp[2] * rp[2];
+        return body_terms<VEL>(fe, exact, rp, rv, r2, rsqrt(r2), acc0, acc1, acc2);
     }
 
     // Fast path: the host-verified window where every body's first segment covers t and all
@@ -419,6 +431,9 @@ struct SpkForceT {
         }
     }
 
+    // The velocity items two at a time and the other force bodies three at a time: the
+    // relative positions and reciprocal square roots of a batch are formed together
+    // (independent dependency chains), then the terms are summed in eval_fast's order.
     __device__ __forceinline__ int fast_forces(const FastPlan& P, bool exact, const double x[3],
                                                const double v[3], const double* cache, int stride,
                                                double out[3]) {
@@ -426,26 +441,59 @@ struct SpkForceT {
         const int n_vel = P.n_vel;
         int k = 0;
 #pragma unroll 1
-        for (int it = 0; it < n_vel; ++it, k += 6) {
-            const FastItem& A = P.item[it];
-            const double bp[3] = {cache[k * stride], cache[(k + 1) * stride], cache[(k + 2) * stride]};
-            const double bv[3] = {cache[(k + 3) * stride], cache[(k + 4) * stride],
-                                  cache[(k + 5) * stride]};
-            const ForceEntry fe{A.mass, A.radius, 0, A.kind, A.naif_id, 0};
-            const int rc = body<true>(fe, exact, x, v, bp, bv, acc0, acc1, acc2);
-            if (rc != ST_OK) return rc;
+        for (int it = 0; it < n_vel; it += 2) {
+            const int nb = it + 1 < n_vel ? 2 : 1;
+            double rp[2][3], rv[2][3], r2[2], ir[2];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int kh = h < nb ? k + 6 * h : k;
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    rp[h][c] = x[c] - cache[(kh + c) * stride];
+                    rv[h][c] = v[c] - cache[(kh + 3 + c) * stride];
+                }
+                r2[h] = rp[h][0] * rp[h][0] + rp[h][1] * rp[h][1] + rp[h][2] * rp[h][2];
+                ir[h] = rsqrt(r2[h]);
+            }
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                if (h < nb) {
+                    const FastItem& A = P.item[it + h];
+                    const ForceEntry fe{A.mass, A.radius, 0, A.kind, A.naif_id, 0};
+                    const int rc = body_terms<true>(fe, exact, rp[h], rv[h], r2[h], ir[h], acc0,
+                                                    acc1, acc2);
+                    if (rc != ST_OK) return rc;
+                }
+            }
+            k += 6 * nb;
         }
         const double zero[3] = {0.0, 0.0, 0.0};
         const int n_items = P.n_items;
 #pragma unroll 1
-        for (int it = n_vel; it < n_items; ++it) {
-            const FastItem& I = P.item[it];
-            if (I.role < 0) continue;
-            const double bp[3] = {cache[k * stride], cache[(k + 1) * stride], cache[(k + 2) * stride]};
-            k += 3;
-            const ForceEntry fe{I.mass, I.radius, 0, I.kind, I.naif_id, 0};
-            const int rc = body<false>(fe, exact, x, v, bp, zero, acc0, acc1, acc2);
-            if (rc != ST_OK) return rc;
+        for (int it = n_vel; it < n_items; it += 3) {
+            double rp[3][3], r2[3], ir[3];
+            bool use[3];
+#pragma unroll
+            for (int h = 0; h < 3; ++h) {
+                use[h] = it + h < n_items && P.item[it + h].role >= 0;
+                if (use[h]) {
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) rp[h][c] = x[c] - cache[(k + c) * stride];
+                    k += 3;
+                    r2[h] = rp[h][0] * rp[h][0] + rp[h][1] * rp[h][1] + rp[h][2] * rp[h][2];
+                    ir[h] = rsqrt(r2[h]);
+                }
+            }
+#pragma unroll
+            for (int h = 0; h < 3; ++h) {
+                if (use[h]) {
+                    const FastItem& I = P.item[it + h];
+                    const ForceEntry fe{I.mass, I.radius, 0, I.kind, I.naif_id, 0};
+                    const int rc = body_terms<false>(fe, exact, rp[h], zero, r2[h], ir[h], acc0,
+                                                     acc1, acc2);
+                    if (rc != ST_OK) return rc;
+                }
+            }
         }
         out[0] = acc0;
         out[1] = acc1;

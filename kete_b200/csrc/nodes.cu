@@ -1,10 +1,14 @@
-// nodes.cu -- host launchers of the node-parallel Radau kernel (radau_nodes.cuh): every
-// register-cap / step-end / warp-synchronous instantiation the tuner chooses from.  Its own
-// translation unit so the instantiations compile in parallel with the other kernels.
+// nodes.cu -- host launchers of the node-parallel Radau kernels (radau_nodes.cuh and the
+// warp-pooled form of radau_pool.cuh): every register-cap / step-end / warp-synchronous /
+// pooled instantiation the tuner chooses from.  Its own translation unit so the
+// instantiations compile in parallel with the other kernels.
+#include <atomic>
+
 #include "common.cuh"
 #include "forces.cuh"
 #include "internal.h"
 #include "radau_nodes.cuh"
+#include "radau_pool.cuh"
 
 namespace kb {
 KB_CONSTANT_UPLOADER(nodes)
@@ -15,9 +19,13 @@ namespace kb {
 // Node-parallel Radau: 8 lanes per object.  With a.queue == null each group integrates one
 // object (grid covers n groups); with a queue the grid is persistent and groups refill.
 // variant: 0 = no register cap, 1 = >= 3 blocks/SM (168 registers), 2 = >= 4 blocks/SM;
-// +3: the step-end lane form (exact evaluations taken from lane 7, see radau_nodes.cuh).
+// +3: the step-end lane form (exact evaluations taken from lane 7, see radau_nodes.cuh);
+// 6-8: the step-end form with warp-synchronous steps and the per-lane ephemeris cache;
+// 9, 10: the warp-pooled record evaluations (radau_pool.cuh) at 168 / 128 registers.
 static const void* nodes_kernel_ptr(int variant) {
     switch (variant) {
+        case 9: return (const void*)nbody_pool_kernel<3>;
+        case 10: return (const void*)nbody_pool_kernel<4>;
         case 1: return (const void*)nbody_nodes_kernel<3, false>;
         case 2: return (const void*)nbody_nodes_kernel<4, false>;
         case 3: return (const void*)nbody_nodes_kernel<1, true>;
@@ -30,11 +38,37 @@ static const void* nodes_kernel_ptr(int variant) {
     }
 }
 
+static int dyn_smem(int variant) { return variant >= 9 ? POOL_DYN_SMEM : 0; }
+
+// The pooled kernels keep their body cache in dynamic shared memory above the 48 KB static
+// limit: allow it once per device (a function attribute, not a stream operation).
+static int allow_dyn_smem(int variant) {
+    static std::atomic<unsigned long long> done[2];
+    if (variant < 9) return 0;
+    int dev = 0;
+    int rc = cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    if (rc) return rc;
+    const unsigned long long bit = 1ull << (dev & 63);
+    auto& d = done[variant - 9];
+    if (d.load() & bit) return 0;
+    if ((rc = cuda_check(cudaFuncSetAttribute(nodes_kernel_ptr(variant),
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              dyn_smem(variant)),
+                         "pooled kernel shared memory")))
+        return rc;
+    d.fetch_or(bit);
+    return 0;
+}
+
 int launch_nbody_nodes(const NBodyArgs& a, int variant, int grid, cudaStream_t stream) {
     if (a.n <= 0) return 0;
     const int block = NODES_BLOCK;
     if (grid <= 0) grid = (int)((a.n * NODE_G + block - 1) / block);
+    int rc = allow_dyn_smem(variant);
+    if (rc) return rc;
     switch (variant) {
+        case 9: nbody_pool_kernel<3><<<grid, block, POOL_DYN_SMEM, stream>>>(a); break;
+        case 10: nbody_pool_kernel<4><<<grid, block, POOL_DYN_SMEM, stream>>>(a); break;
         case 1: nbody_nodes_kernel<3, false><<<grid, block, 0, stream>>>(a); break;
         case 2: nbody_nodes_kernel<4, false><<<grid, block, 0, stream>>>(a); break;
         case 3: nbody_nodes_kernel<1, true><<<grid, block, 0, stream>>>(a); break;
@@ -55,8 +89,9 @@ int nodes_grid_size(int variant, int* grid) {
     if (rc) return rc;
     if ((rc = cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attr")))
         return rc;
+    if ((rc = allow_dyn_smem(variant))) return rc;
     if ((rc = cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                             &per_sm, nodes_kernel_ptr(variant), NODES_BLOCK, 0),
+                             &per_sm, nodes_kernel_ptr(variant), NODES_BLOCK, dyn_smem(variant)),
                          "occupancy")))
         return rc;
     *grid = sms * (per_sm > 0 ? per_sm : 1);

@@ -32,6 +32,7 @@ enum Phase : int {
     PH_DONE = 3,
     PH_WAIT = 4,      // WS: step accepted, the next one starts with the warp's other groups
     PH_FINISHED = 5,  // WS: no object left for this group
+    PH_STORE = 6,     // pooled form: the object is finished, its outcome stored next round
 };
 
 __device__ __forceinline__ void nodes_store(const NBodyArgs& a, int64_t i, int rc, const double x[3],
@@ -127,7 +128,7 @@ __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_nodes_kernel(NBodyArg
     int phase = PH_DONE;
     double t = 0.0, tf = 0.0, h = 0.0, next_h = 0.0;
     double x[3], v[3], acc[3];
-    int iter = 0, failures = 0;
+    int iter = 0, failures = 0, attempts = 0;
     RadauCounters cnt;
     SpkForce F;
     F.n_force = a.n_force;
@@ -169,6 +170,7 @@ __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_nodes_kernel(NBodyArg
         cnt = RadauCounters();
         iter = 0;
         failures = 0;
+        attempts = 0;
         rc = ST_OK;
         const bool finite = isfinite(x[0]) && isfinite(x[1]) && isfinite(x[2]) &&
                             isfinite(v[0]) && isfinite(v[1]) && isfinite(v[2]) && isfinite(t);
@@ -196,6 +198,7 @@ __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_nodes_kernel(NBodyArg
             __syncwarp(gmask);
         }
         iter = 0;
+        ++attempts;
         phase = PH_ITER;
     };
 
@@ -225,7 +228,9 @@ __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_nodes_kernel(NBodyArg
             if (__all_sync(0xffffffffu, phase == PH_FINISHED)) break;
             if (phase == PH_WAIT || phase == PH_DONE || phase == PH_FINISHED) continue;
         }
-        if (phase != PH_DONE && ++obj_rounds > max_obj_rounds) {
+        // the step loop's bound: step attempts (kete_b200_set_step_limit), and rounds as a
+        // second guard
+        if (phase != PH_DONE && (++obj_rounds > max_obj_rounds || attempts > a.max_loops)) {
             finish(ST_TIMEOUT);
             continue;
         }

@@ -5,9 +5,10 @@ The node-parallel Radau kernel comes in three register budgets (no cap, 168 regi
 local memory), each with or without the step-end lane (variants 3-5: the eighth lane
 evaluates the step end during every corrector iteration instead of a separate round;
 variants 6-8 add warp-synchronous step starts with the bodies' positions cached across a
-step's corrector iterations) and
-in two grid forms (one lane group per object, or a persistent grid
-whose groups take the next object from a queue).  Which is fastest depends on the object
+step's corrector iterations; variants 9 and 10, at 168 and 128 registers, keep the cache but
+let the warp's four objects step independently and share every round's ephemeris-record
+evaluations across all 32 lanes) and in two grid forms (one lane group per object, or a
+persistent grid whose groups take the next object from a queue).  Which is fastest depends on the object
 count and the spread of their step counts, so it is measured: ``autotune`` times every
 configuration on the caller's own inputs (device arrays) and installs the fastest.
 """
@@ -22,8 +23,8 @@ from . import _lib
 from .propagation import propagate_n_body_arrays
 
 CONFIGS = [dict(mode=_lib.MODE_NODES, variant=v, refill=r) for v, r in
-           itertools.product((0, 1, 2, 3, 4, 5, 6, 7, 8), (0, 1))] + [dict(mode=_lib.MODE_THREAD,
-                                                                 variant=0, refill=0)]
+           itertools.product((0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10), (0, 1))] + [
+               dict(mode=_lib.MODE_THREAD, variant=0, refill=0)]
 _current = dict(mode=_lib.MODE_NODES, variant=7, refill=0, thread_block=128)
 
 

@@ -22,9 +22,10 @@ pytestmark = pytest.mark.gpu
 EPOCH = synthetic.EPOCH
 TIMEOUT = 7
 
-# the product configuration (warp-synchronous cached node kernel, persistent grid with
-# refill, objects in work order), the same without refill, and the plain thread form
+# the warp-synchronous cached node kernel (persistent grid with refill, objects in work
+# order; and one object per group), the warp-pooled forms, and the plain thread form
 FORMS = (dict(mode=2, variant=7, refill=1), dict(mode=2, variant=7, refill=0),
+         dict(mode=2, variant=9, refill=1), dict(mode=2, variant=10, refill=1),
          dict(mode=1, variant=0, refill=0))
 
 

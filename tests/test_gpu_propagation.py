@@ -117,7 +117,8 @@ def test_spk_states_vs_oracle(gpu, oracle_spk):
 CONFIGS = (dict(mode=1, variant=0, refill=0), dict(mode=2, variant=0, refill=0),
            dict(mode=2, variant=2, refill=1), dict(mode=2, variant=3, refill=1),
            dict(mode=2, variant=5, refill=0), dict(mode=2, variant=7, refill=1),
-           dict(mode=2, variant=6, refill=0))
+           dict(mode=2, variant=6, refill=0), dict(mode=2, variant=9, refill=1),
+           dict(mode=2, variant=10, refill=0))
 MODES = CONFIGS
 
 
@@ -150,7 +151,8 @@ def _compare_nbody(gpu, oracle, pos, vel, jd0, jd1, ng=None, frame=2, center=10,
 @pytest.mark.parametrize("refill", [0, 1])
 def test_warp_synchronous_forms_match(gpu, refill):
     """Variants 6-8 change only when each group's next step starts and reuse the bodies'
-    positions across a step's iterations.  The cached positions are rounded to doubles
+    positions across a step's iterations; variants 9 and 10 reuse them too, with the records
+    evaluated by the whole warp for whichever lanes need them.  The cached positions are rounded to doubles
     before the force terms read them, where the uncached path may fuse the last multiply
     into the difference, so results agree with the same register budget without caching to
     rounding: statuses equal, positions within the 1e-9 AU parity bar, step counts equal
@@ -165,12 +167,13 @@ def test_warp_synchronous_forms_match(gpu, refill):
     jd0 = EPOCH + rng.uniform(-30.0, 30.0, n)
     jd1 = EPOCH + rng.uniform(-400.0, 400.0, n)
     out = {}
-    for variant in (3, 4, 5, 6, 7, 8):
+    for variant in (3, 4, 5, 6, 7, 8, 9, 10):
         _set(gpu, dict(mode=2, variant=variant, refill=refill))
         out[variant] = gpu.propagate_n_body_arrays(pos, vel, jd0, jd1, nongrav=ng, mode=2,
                                                    with_details=True)
     tune.set_config()
-    for base, ws in ((3, 6), (4, 7), (5, 8)):
+    # the pooled forms (9, 10) against the uncached step-end forms of their register budgets
+    for base, ws in ((3, 6), (4, 7), (5, 8), (4, 9), (5, 10)):
         p0, v0, s0, d0 = out[base]
         p1, v1, s1, d1 = out[ws]
         assert np.array_equal(s0, s1)
