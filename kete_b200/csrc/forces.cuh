@@ -431,9 +431,6 @@ struct SpkForceT {
         }
     }
 
-    // The velocity items two at a time and the other force bodies three at a time: the
-    // relative positions and reciprocal square roots of a batch are formed together
-    // (independent dependency chains), then the terms are summed in eval_fast's order.
     __device__ __forceinline__ int fast_forces(const FastPlan& P, bool exact, const double x[3],
                                                const double v[3], const double* cache, int stride,
                                                double out[3]) {
@@ -441,59 +438,26 @@ struct SpkForceT {
         const int n_vel = P.n_vel;
         int k = 0;
 #pragma unroll 1
-        for (int it = 0; it < n_vel; it += 2) {
-            const int nb = it + 1 < n_vel ? 2 : 1;
-            double rp[2][3], rv[2][3], r2[2], ir[2];
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int kh = h < nb ? k + 6 * h : k;
-#pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    rp[h][c] = x[c] - cache[(kh + c) * stride];
-                    rv[h][c] = v[c] - cache[(kh + 3 + c) * stride];
-                }
-                r2[h] = rp[h][0] * rp[h][0] + rp[h][1] * rp[h][1] + rp[h][2] * rp[h][2];
-                ir[h] = rsqrt(r2[h]);
-            }
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                if (h < nb) {
-                    const FastItem& A = P.item[it + h];
-                    const ForceEntry fe{A.mass, A.radius, 0, A.kind, A.naif_id, 0};
-                    const int rc = body_terms<true>(fe, exact, rp[h], rv[h], r2[h], ir[h], acc0,
-                                                    acc1, acc2);
-                    if (rc != ST_OK) return rc;
-                }
-            }
-            k += 6 * nb;
+        for (int it = 0; it < n_vel; ++it, k += 6) {
+            const FastItem& A = P.item[it];
+            const double bp[3] = {cache[k * stride], cache[(k + 1) * stride], cache[(k + 2) * stride]};
+            const double bv[3] = {cache[(k + 3) * stride], cache[(k + 4) * stride],
+                                  cache[(k + 5) * stride]};
+            const ForceEntry fe{A.mass, A.radius, 0, A.kind, A.naif_id, 0};
+            const int rc = body<true>(fe, exact, x, v, bp, bv, acc0, acc1, acc2);
+            if (rc != ST_OK) return rc;
         }
         const double zero[3] = {0.0, 0.0, 0.0};
         const int n_items = P.n_items;
 #pragma unroll 1
-        for (int it = n_vel; it < n_items; it += 3) {
-            double rp[3][3], r2[3], ir[3];
-            bool use[3];
-#pragma unroll
-            for (int h = 0; h < 3; ++h) {
-                use[h] = it + h < n_items && P.item[it + h].role >= 0;
-                if (use[h]) {
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) rp[h][c] = x[c] - cache[(k + c) * stride];
-                    k += 3;
-                    r2[h] = rp[h][0] * rp[h][0] + rp[h][1] * rp[h][1] + rp[h][2] * rp[h][2];
-                    ir[h] = rsqrt(r2[h]);
-                }
-            }
-#pragma unroll
-            for (int h = 0; h < 3; ++h) {
-                if (use[h]) {
-                    const FastItem& I = P.item[it + h];
-                    const ForceEntry fe{I.mass, I.radius, 0, I.kind, I.naif_id, 0};
-                    const int rc = body_terms<false>(fe, exact, rp[h], zero, r2[h], ir[h], acc0,
-                                                     acc1, acc2);
-                    if (rc != ST_OK) return rc;
-                }
-            }
+        for (int it = n_vel; it < n_items; ++it) {
+            const FastItem& I = P.item[it];
+            if (I.role < 0) continue;
+            const double bp[3] = {cache[k * stride], cache[(k + 1) * stride], cache[(k + 2) * stride]};
+            k += 3;
+            const ForceEntry fe{I.mass, I.radius, 0, I.kind, I.naif_id, 0};
+            const int rc = body<false>(fe, exact, x, v, bp, zero, acc0, acc1, acc2);
+            if (rc != ST_OK) return rc;
         }
         out[0] = acc0;
         out[1] = acc1;

@@ -158,9 +158,9 @@ __device__ __forceinline__ void pool_records(unsigned M, int warp_lane, int warp
 }
 
 // The force at (x, v) from a lane's cached body states, summed in the fast plan's order
-// (eval_fast's): the velocity items two at a time, then the others three at a time, the
-// chained bodies offset by the centre kept before them; the relative positions and reciprocal
-// square roots of a batch are formed together (independent dependency chains).
+// (eval_fast's): the velocity items, then the others, with the chained bodies offset by the
+// centre kept before them.  One body at a time: the kernel is bound by its registers, and
+// forming several bodies' terms together spills more than it hides.
 __device__ __forceinline__ int pool_forces(const FastPlan& P, SpkForce& F, bool exact,
                                            const double x[3], const double v[3],
                                            const double* cache, double out[3]) {
@@ -168,71 +168,36 @@ __device__ __forceinline__ int pool_forces(const FastPlan& P, SpkForce& F, bool 
     const int n_vel = P.n_vel;
     int k = 0;
 #pragma unroll 1
-    for (int it = 0; it < n_vel; it += 2) {
-        const int nb = it + 1 < n_vel ? 2 : 1;
-        double rp[2][3], rv[2][3], r2[2], ir[2];
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int kh = h < nb ? k + 6 * h : k;
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                rp[h][c] = x[c] - cache[(kh + c) * NODES_BLOCK];
-                rv[h][c] = v[c] - cache[(kh + 3 + c) * NODES_BLOCK];
-            }
-            r2[h] = rp[h][0] * rp[h][0] + rp[h][1] * rp[h][1] + rp[h][2] * rp[h][2];
-            ir[h] = rsqrt(r2[h]);
-        }
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            if (h < nb) {
-                const FastItem& A = P.item[it + h];
-                const ForceEntry fe{A.mass, A.radius, 0, A.kind, A.naif_id, 0};
-                const int rc = F.body_terms<true>(fe, exact, rp[h], rv[h], r2[h], ir[h], acc0,
-                                                  acc1, acc2);
-                if (rc != ST_OK) return rc;
-            }
-        }
-        k += 6 * nb;
+    for (int it = 0; it < n_vel; ++it, k += 6) {
+        const FastItem& A = P.item[it];
+        const double bp[3] = {cache[k * NODES_BLOCK], cache[(k + 1) * NODES_BLOCK],
+                              cache[(k + 2) * NODES_BLOCK]};
+        const double bv[3] = {cache[(k + 3) * NODES_BLOCK], cache[(k + 4) * NODES_BLOCK],
+                              cache[(k + 5) * NODES_BLOCK]};
+        const ForceEntry fe{A.mass, A.radius, 0, A.kind, A.naif_id, 0};
+        const int rc = F.body<true>(fe, exact, x, v, bp, bv, acc0, acc1, acc2);
+        if (rc != ST_OK) return rc;
     }
     const double zero[3] = {0.0, 0.0, 0.0};
     double cp[3] = {0.0, 0.0, 0.0};
     const int n_items = P.n_items;
 #pragma unroll 1
-    for (int it = n_vel; it < n_items; it += 3) {
-        double rp[3][3], r2[3], ir[3];
-        bool use[3];
-#pragma unroll
-        for (int h = 0; h < 3; ++h) {
-            use[h] = false;
-            if (it + h >= n_items) continue;
-            const FastItem& I = P.item[it + h];
-            if (I.role == -2) continue;
-            double bp[3] = {cache[k * NODES_BLOCK], cache[(k + 1) * NODES_BLOCK],
-                            cache[(k + 2) * NODES_BLOCK]};
-            k += 3;
-            if (I.role < 0) {
-                cp[0] = bp[0]; cp[1] = bp[1]; cp[2] = bp[2];
-                continue;
-            }
-            if (I.chained) {
-                bp[0] += cp[0]; bp[1] += cp[1]; bp[2] += cp[2];
-            }
-            use[h] = true;
-#pragma unroll
-            for (int c = 0; c < 3; ++c) rp[h][c] = x[c] - bp[c];
-            r2[h] = rp[h][0] * rp[h][0] + rp[h][1] * rp[h][1] + rp[h][2] * rp[h][2];
-            ir[h] = rsqrt(r2[h]);
+    for (int it = n_vel; it < n_items; ++it) {
+        const FastItem& I = P.item[it];
+        if (I.role == -2) continue;
+        double bp[3] = {cache[k * NODES_BLOCK], cache[(k + 1) * NODES_BLOCK],
+                        cache[(k + 2) * NODES_BLOCK]};
+        k += 3;
+        if (I.role < 0) {
+            cp[0] = bp[0]; cp[1] = bp[1]; cp[2] = bp[2];
+            continue;
         }
-#pragma unroll
-        for (int h = 0; h < 3; ++h) {
-            if (use[h]) {
-                const FastItem& I = P.item[it + h];
-                const ForceEntry fe{I.mass, I.radius, 0, I.kind, I.naif_id, 0};
-                const int rc = F.body_terms<false>(fe, exact, rp[h], zero, r2[h], ir[h], acc0,
-                                                   acc1, acc2);
-                if (rc != ST_OK) return rc;
-            }
+        if (I.chained) {
+            bp[0] += cp[0]; bp[1] += cp[1]; bp[2] += cp[2];
         }
+        const ForceEntry fe{I.mass, I.radius, 0, I.kind, I.naif_id, 0};
+        const int rc = F.body<false>(fe, exact, x, v, bp, zero, acc0, acc1, acc2);
+        if (rc != ST_OK) return rc;
     }
     out[0] = acc0;
     out[1] = acc1;
@@ -291,6 +256,12 @@ static __device__ __noinline__ ChainedState pool_change_center(bool inward, doub
 // Dynamic shared memory of the pooled kernel: the body cache.
 constexpr int POOL_DYN_SMEM = POOL_CACHE_DOUBLES * NODES_BLOCK * (int)sizeof(double);
 
+// Per-group state in shared memory (doubles): the object's epoch, target epoch, step, previous
+// step, position, velocity and acceleration at the epoch.  Every lane of a group needs the
+// same values; keeping them out of the lanes' registers leaves the registers to the hot loop.
+constexpr int ST_T = 0, ST_TF = 1, ST_H = 2, ST_HP = 3, ST_X = 4, ST_V = 7, ST_A = 10;
+constexpr int ST_ROW = 13;
+
 // MINB: minimum resident blocks per SM requested from the compiler (3: 168 registers,
 // 4: 128); the host picks the instantiation.  With a.queue the grid is persistent and groups
 // take objects from the queue; without, each group integrates one object.
@@ -301,6 +272,7 @@ __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_pool_kernel(NBodyArgs
     __shared__ double s_b[NODES_BLOCK / NODE_G][21];
     __shared__ double s_e[NODES_BLOCK / NODE_G][NODE_G * 3];
     __shared__ double s_cmp[NODES_BLOCK / NODE_G][6];
+    __shared__ double s_st[NODES_BLOCK / NODE_G][ST_ROW];
     __shared__ double s_te[NODES_BLOCK];
     __shared__ int s_tgt[NODES_BLOCK];
     __shared__ PoolSrc s_src[MAX_ITEMS];
@@ -351,6 +323,7 @@ __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_pool_kernel(NBodyArgs
     double* sb = s_b[threadIdx.x / NODE_G];
     double* se = s_e[threadIdx.x / NODE_G];
     double* scmp = s_cmp[threadIdx.x / NODE_G];
+    double* st = s_st[threadIdx.x / NODE_G];
     const int comp = lane % 3;  // component this lane forms g and b for (lanes 0-2 publish)
     const double* nrow = s_node + (lane < 7 ? lane + 1 : 8) * NODE_ROW;
     const bool se_lane = lane == 7;
@@ -358,8 +331,6 @@ __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_pool_kernel(NBodyArgs
 
     int64_t obj = -1;
     int phase = PH_DONE;
-    double t = 0.0, tf = 0.0, h = 0.0, next_h = 0.0, h_prev = 0.0;
-    double x[3] = {0.0, 0.0, 0.0}, v[3] = {0.0, 0.0, 0.0}, acc[3] = {0.0, 0.0, 0.0};
     int iter = 0, failures = 0, attempts = 0;
     RadauCounters cnt;
     SpkForce F;
@@ -370,9 +341,9 @@ __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_pool_kernel(NBodyArgs
     F.impact_id = 0;
     F.min_dist = 1e300;
     F.min_id = 0;
-    int rc = ST_OK;
     double cache_t = __longlong_as_double(0x7ff8000000000000LL);  // nothing cached yet
     bool first = true;
+    int outcome = ST_OK;  // outcome of a finished object, stored at the top of the next round
 
     auto fetch = [&]() -> bool {
         int64_t k;
@@ -386,11 +357,26 @@ __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_pool_kernel(NBodyArgs
         first = false;
         if (k >= a.n) return false;
         obj = a.order ? a.order[k] : k;
-        const int64_t n = a.n;
-        t = a.jd0[obj];
-        tf = a.jd1[obj];
-        x[0] = a.pos[obj]; x[1] = a.pos[n + obj]; x[2] = a.pos[2 * n + obj];
-        v[0] = a.vel[obj]; v[1] = a.vel[n + obj]; v[2] = a.vel[2 * n + obj];
+        int frc = ST_OK;
+        if (lane == 0) {
+            const int64_t n = a.n;
+            const double t0 = a.jd0[obj];
+            double3 p = make_double3(a.pos[obj], a.pos[n + obj], a.pos[2 * n + obj]);
+            double3 v = make_double3(a.vel[obj], a.vel[n + obj], a.vel[2 * n + obj]);
+            const bool finite = isfinite(p.x) && isfinite(p.y) && isfinite(p.z) &&
+                                isfinite(v.x) && isfinite(v.y) && isfinite(v.z) && isfinite(t0);
+            if (!finite) frc = ST_VALUE_ERROR;
+            if (frc == ST_OK && (a.chain.len > 0 || a.frame == FRAME_ECLIPTIC)) {
+                const ChainedState s = pool_change_center(true, t0, a.frame, a.chain, p, v);
+                frc = s.rc;
+                p = s.p;
+                v = s.v;
+            }
+            st[ST_T] = t0;
+            st[ST_TF] = a.jd1[obj];
+            st[ST_X] = p.x; st[ST_X + 1] = p.y; st[ST_X + 2] = p.z;
+            st[ST_V] = v.x; st[ST_V + 1] = v.y; st[ST_V + 2] = v.z;
+        }
         if (lane < 7) {
             sb[lane] = 0.0;
             sb[7 + lane] = 0.0;
@@ -406,40 +392,26 @@ __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_pool_kernel(NBodyArgs
         iter = 0;
         failures = 0;
         attempts = 0;
-        rc = ST_OK;
-        const bool finite = isfinite(x[0]) && isfinite(x[1]) && isfinite(x[2]) &&
-                            isfinite(v[0]) && isfinite(v[1]) && isfinite(v[2]) && isfinite(t);
-        if (!finite) rc = ST_VALUE_ERROR;
-        if (rc == ST_OK && (a.chain.len > 0 || a.frame == FRAME_ECLIPTIC)) {
-            const ChainedState s = pool_change_center(true, t, a.frame, a.chain,
-                                                      make_double3(x[0], x[1], x[2]),
-                                                      make_double3(v[0], v[1], v[2]));
-            rc = s.rc;
-            x[0] = s.p.x; x[1] = s.p.y; x[2] = s.p.z;
-            v[0] = s.v.x; v[1] = s.v.y; v[2] = s.v.z;
-        }
-        phase = PH_EXACT_INIT;
+        outcome = __shfl_sync(gmask, frc, 0, NODE_G);
+        phase = outcome == ST_OK ? PH_EXACT_INIT : PH_STORE;
         __syncwarp(gmask);
         return true;
     };
 
-    // an object's outcome is recorded here and stored at the top of the next round (one
-    // store site keeps the loop's state in registers)
-    int outcome = ST_OK;
     auto finish = [&](int code) {
         outcome = code;
         phase = PH_STORE;
     };
 
-    // step start: |h| >= MIN_STEP, then truncate to the final time (radau.rs:187-190,214-216);
-    // after an accepted step the corrector starts from the predicted b (predict_b_row)
-    auto start_step = [&](bool predict) {
+    // step start with step h (every lane computes the same): |h| >= MIN_STEP, then truncate
+    // to the final time (radau.rs:187-190,214-216); after an accepted step the corrector
+    // starts from the predicted b (predict_b_row).  Lane 0 publishes the step.
+    auto start_step = [&](double h, double t, double tf, bool predict, double h_prev) {
         if (fabs(h) < 0.005) h = copysign(0.005, h);
         if (fabs(t - tf) <= fabs(h)) h = tf - t;
-        if (predict) {
-            if (lane < 3) predict_b_row(sb + 7 * lane, h / h_prev);
-            __syncwarp(gmask);
-        }
+        if (predict && lane < 3) predict_b_row(sb + 7 * lane, h / h_prev);
+        if (lane == 0) st[ST_H] = h;
+        __syncwarp(gmask);
         iter = 0;
         ++attempts;
         phase = PH_ITER;
@@ -448,23 +420,27 @@ __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_pool_kernel(NBodyArgs
     int obj_rounds = 0;
     const int max_obj_rounds = a.max_loops * 11;
     for (;;) {
-        if (phase == PH_STORE) {
-            int code = outcome;
-            if (code == ST_OK && (a.chain.len > 0 || a.frame == FRAME_ECLIPTIC)) {
-                const ChainedState s = pool_change_center(false, tf, a.frame, a.chain,
-                                                          make_double3(x[0], x[1], x[2]),
-                                                          make_double3(v[0], v[1], v[2]));
-                code = s.rc;
-                x[0] = s.p.x; x[1] = s.p.y; x[2] = s.p.z;
-                v[0] = s.v.x; v[1] = s.v.y; v[2] = s.v.z;
+        if (phase == PH_STORE) {  // the finished object's outcome (lane 0 stores)
+            if (lane == 0) {
+                int code = outcome;
+                double3 p = make_double3(st[ST_X], st[ST_X + 1], st[ST_X + 2]);
+                double3 v = make_double3(st[ST_V], st[ST_V + 1], st[ST_V + 2]);
+                if (code == ST_OK && (a.chain.len > 0 || a.frame == FRAME_ECLIPTIC)) {
+                    const ChainedState s = pool_change_center(false, st[ST_TF], a.frame, a.chain,
+                                                              p, v);
+                    code = s.rc;
+                    p = s.p;
+                    v = s.v;
+                }
+                const double xs[3] = {p.x, p.y, p.z}, vs[3] = {v.x, v.y, v.z};
+                nodes_store(a, obj, code, xs, vs, F, st[ST_T], cnt);
             }
-            if (lane == 0) nodes_store(a, obj, code, x, v, F, t, cnt);
+            __syncwarp(gmask);  // st is read before the next object overwrites it
             phase = PH_DONE;
         }
         if (phase == PH_DONE) {  // take the next object (group-collective)
             obj_rounds = 0;
             if (!fetch()) phase = PH_FINISHED;
-            else if (rc != ST_OK) finish(rc);
         }
         // every lane of the warp stays in the loop for the pool's collectives until all
         // four groups have run out of objects
@@ -481,14 +457,15 @@ __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_pool_kernel(NBodyArgs
         double te = 0.0, xe[3] = {0.0, 0.0, 0.0}, ve[3] = {0.0, 0.0, 0.0};
         if (active) {
             if (!iter_round) {
-                te = t;
+                te = st[ST_T];
 #pragma unroll
                 for (int c = 0; c < 3; ++c) {
-                    xe[c] = x[c];
-                    ve[c] = v[c];
+                    xe[c] = st[ST_X + c];
+                    ve[c] = st[ST_V + c];
                 }
             } else {
                 const double f = nrow[14], frac2 = nrow[15];
+                const double h = st[ST_H];
                 const double h2 = h * h;
 #pragma unroll
                 for (int c = 0; c < 3; ++c) {
@@ -499,10 +476,11 @@ __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_pool_kernel(NBodyArgs
                         bw += nrow[k] * bck;
                         bu += nrow[7 + k] * bck;
                     }
-                    xe[c] = x[c] + f * v[c] * h + frac2 * h2 * (acc[c] / 2.0 + bw);
-                    ve[c] = v[c] + f * h * (acc[c] + bu);
+                    const double ac = st[ST_A + c];
+                    xe[c] = st[ST_X + c] + f * st[ST_V + c] * h + frac2 * h2 * (ac / 2.0 + bw);
+                    ve[c] = st[ST_V + c] + f * h * (ac + bu);
                 }
-                te = t + f * h;
+                te = st[ST_T] + f * h;
             }
         }
         const bool fast = active && use_pool && te >= plan.lo && te <= plan.hi;
@@ -549,23 +527,23 @@ __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_pool_kernel(NBodyArgs
             finish(erc);
             continue;
         }
-        if (!iter_round) {  // the initial exact evaluation
+        if (!iter_round) {  // the initial exact evaluation (every lane evaluated one point)
             cnt.exact++;
-            acc[0] = ev[0];
-            acc[1] = ev[1];
-            acc[2] = ev[2];
+            const double t = st[ST_T], tf = st[ST_TF];
+            __syncwarp(gmask);
+            if (lane < 3) st[ST_A + lane] = ev[lane == 0 ? 0 : (lane == 1 ? 1 : 2)];
             if (fabs(tf - t) < 1e-10) {
+                __syncwarp(gmask);
                 finish(ST_OK);
                 continue;
             }
-            h = copysign(0.1, tf - t);
             failures = 0;
-            start_step(false);
+            start_step(copysign(0.1, tf - t), t, tf, false, 0.0);
             continue;
         }
         // ---- corrector iteration: exchange the 7 node evaluations, form g and b ----
         // (radau.rs:292-313).  Lanes 0-2 each own one component; every lane then reads the
-        // new b for the convergence test and the state update.
+        // new b for the convergence test.
         cnt.iterations++;
         se[3 * lane + 0] = ev[0];
         se[3 * lane + 1] = ev[1];
@@ -573,7 +551,7 @@ __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_pool_kernel(NBodyArgs
         const double b6_old0 = sb[6], b6_old1 = sb[13], b6_old2 = sb[20];
         __syncwarp(gmask);
         {
-            const double ac = comp == 0 ? acc[0] : (comp == 1 ? acc[1] : acc[2]);
+            const double ac = st[ST_A + comp];
             double g[7];
 #pragma unroll
             for (int j = 1; j < 8; ++j) {
@@ -600,11 +578,12 @@ __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_pool_kernel(NBodyArgs
                                   fabs(b62 - b6_old2) / fem2);
         ++iter;
         if (ratio < 1e-14) {
-            const double h2 = h * h;
-            // x += dx, v += dv with compensated (Kahan) summation
-            double ncx[3], ncv[3];
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
+            const double h = st[ST_H], t = st[ST_T], tf = st[ST_TF];
+            __syncwarp(gmask);  // every lane has read the step before lane 0 replaces it
+            if (lane < 3) {
+                // x += dx, v += dv with compensated (Kahan) summation; lane c owns component c
+                const int c = lane;
+                const double h2 = h * h;
                 double dw = 0.0, du = 0.0;
 #pragma unroll
                 for (int k = 0; k < 7; ++k) {
@@ -612,32 +591,31 @@ __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_pool_kernel(NBodyArgs
                     dw += bck * c_tab.w[k];
                     du += bck * c_tab.u[k];
                 }
-                const double dx = v[c] * h + h2 * (acc[c] * 0.5 + dw);
-                const double dv = h * (acc[c] + du);
+                const double xc = st[ST_X + c], vc = st[ST_V + c], ac = st[ST_A + c];
+                const double dx = vc * h + h2 * (ac * 0.5 + dw);
+                const double dv = h * (ac + du);
                 const double yx = dx - scmp[c], yv = dv - scmp[3 + c];
-                const double tx = x[c] + yx, tv = v[c] + yv;
-                ncx[c] = (tx - x[c]) - yx;
-                ncv[c] = (tv - v[c]) - yv;
-                x[c] = tx;
-                v[c] = tv;
+                const double tx = xc + yx, tv = vc + yv;
+                scmp[c] = (tx - xc) - yx;
+                scmp[3 + c] = (tv - vc) - yv;
+                st[ST_X + c] = tx;
+                st[ST_V + c] = tv;
+                // the step-end lane's evaluation is the exact evaluation of the new state
+                st[ST_A + c] = se[21 + c];
             }
-            __syncwarp(gmask);  // every lane has read the old compensations
-            if (lane < 3) {
-                scmp[lane] = lane == 0 ? ncx[0] : (lane == 1 ? ncx[1] : ncx[2]);
-                scmp[3 + lane] = lane == 0 ? ncv[0] : (lane == 1 ? ncv[1] : ncv[2]);
-            }
-            t += h;
             const double mb6 = fmax(fmax(fabs(b60), fabs(b61)), fabs(b62));
             const double r = pow(1e-6 * fmax(fmax(fem0, fem1), fem2) / mb6, 1.0 / 7.0);
-            next_h = h * clampd(r, 0.25, 4.0);
-            // the step-end lane's evaluation is the exact evaluation of the new state
+            const double next_h = h * clampd(r, 0.25, 4.0);
+            const double tn = t + h;
+            if (lane == 0) {
+                st[ST_T] = tn;
+                st[ST_HP] = h;
+                st[ST_H] = next_h;
+            }
             const int se_rc = __shfl_sync(gmask, erc, 7, NODE_G);
             F.min_dist = __shfl_sync(gmask, F.min_dist, 7, NODE_G);
             F.min_id = __shfl_sync(gmask, F.min_id, 7, NODE_G);
             F.impact_id = __shfl_sync(gmask, F.impact_id, 7, NODE_G);
-            acc[0] = se[21];
-            acc[1] = se[22];
-            acc[2] = se[23];
             __syncwarp(gmask);
             cnt.exact++;
             if (se_rc != ST_OK) {
@@ -645,14 +623,12 @@ __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_pool_kernel(NBodyArgs
                 continue;
             }
             cnt.steps++;
-            h_prev = h;
-            h = next_h;
-            if (fabs(t - tf) < 1e-12) {
+            if (fabs(tn - tf) < 1e-12) {
                 finish(ST_OK);
                 continue;
             }
             failures = 0;
-            start_step(true);
+            start_step(next_h, tn, tf, true, h);
             continue;
         }
         if (se_lane) {  // iteration not converged: forget the step-end lane's record
@@ -662,12 +638,13 @@ __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_pool_kernel(NBodyArgs
         __syncwarp(gmask);
         if (iter >= 10) {  // step failed to converge (radau.rs:345) -> retry smaller
             failures += 1;
-            h *= 0.7;
             if (failures > 10) {
                 finish(ST_CONVERGENCE);
                 continue;
             }
-            start_step(false);
+            const double h = st[ST_H] * 0.7, t = st[ST_T], tf = st[ST_TF];
+            __syncwarp(gmask);  // read before lane 0 replaces the step
+            start_step(h, t, tf, false, 0.0);
         }
     }
 }
