@@ -225,16 +225,15 @@ struct SpkForceT {
                                               double& acc0, double& acc1, double& acc2) {
         const double r = r2 * ir;
         const double ir3 = ir * ir * ir;
-        if (exact) {
-            if (r <= fe.radius) {
-                impact_id = fe.naif_id;
-                return ST_IMPACT;
-            }
-            if (fe.kind != FK_SUN && r < min_dist) {
-                min_dist = r;
-                min_id = fe.naif_id;
-            }
+        // exact evaluations only: impacts and the closest approach to a non-Sun body (as
+        // selects, not branches: the flag differs between the lanes of a warp)
+        if (exact && r <= fe.radius) {
+            impact_id = fe.naif_id;
+            return ST_IMPACT;
         }
+        const bool closer = exact && fe.kind != FK_SUN && r < min_dist;
+        min_dist = closer ? r : min_dist;
+        min_id = closer ? fe.naif_id : min_id;
         const double mass = fe.mass;
         const double kk = mass * ir3;
         acc0 -= rp[0] * kk;

@@ -283,8 +283,9 @@ namespace kb {
 // the orbit.  With a persistent grid the groups that finish early pick up the small ones
 // and the tail is short; with one group per object, neighbours in a warp get similar work,
 // so the warp-synchronous forms' groups wait less for each other.  Work is bucketed on a
-// log2 scale (eighth-octave buckets from 2^-8 to 2^7 radians); within a bucket the order is
-// whatever the atomics give -- it does not affect any object's result.
+// log2 scale (quarter-octave classes from 2^-8 to 2^7 radians, each split by the direction
+// of integration); within a bucket the order is whatever the atomics give -- it does not
+// affect any object's result.
 //
 // Scratch layout (ints): [0] object queue, [1..ORDER_BUCKETS] bucket histogram, then the
 // bucket cursors, then order[n] from int offset ORDER_SCRATCH_HEADER.
@@ -301,8 +302,14 @@ __device__ __forceinline__ int work_bucket(int64_t i, int64_t n, const double* _
     const double mean_motion = inv_a > 0.0 ? sqrt(GMS * inv_a * inv_a * inv_a) : sqrt(GMS / (r * r * r));
     const double work = span * mean_motion;
     if (!(work > 0.0) || !isfinite(work)) return ORDER_BUCKETS - 1;  // no work, NaN last
-    const int b = (int)floor(log2(work) * 8.0) + 64;
-    return ORDER_BUCKETS - 1 - (b < 0 ? 0 : (b > ORDER_BUCKETS - 1 ? ORDER_BUCKETS - 1 : b));
+    // quarter-octave work classes, most work first; within a class the objects integrated
+    // forwards in time come before those integrated backwards, so that neighbours in the
+    // order (the lane groups of a warp, the groups of a block) also move through the
+    // ephemeris in the same direction and share more of its records
+    constexpr int CLASSES = ORDER_BUCKETS / 2;
+    const int b = (int)floor(log2(work) * 4.0) + 32;
+    const int cls = CLASSES - 1 - (b < 0 ? 0 : (b > CLASSES - 1 ? CLASSES - 1 : b));
+    return 2 * cls + (jd1 < jd0 ? 1 : 0);
 }
 
 __global__ void order_hist_kernel(int64_t n, const double* __restrict__ pos,
