@@ -124,7 +124,7 @@ WORKLOADS["thermal_wise_1m"] = ("thermal model, FRM with the four WISE bands and
                                 "lognormal median 0.14 sigma_ln 0.6, H U(8,20), G 0.15, "
                                 "emissivity 0.9), 2048-facet sphere")
 DEFAULT_N["thermal_wise_1m"] = 1_000_000
-# ncu sm__pipe_fp64_cycles_active of the FRM WISE kernel (profiles/thermal_frm_wise_20k.md)
+# ncu sm__pipe_fp64_cycles_active of the FRM WISE kernel (one capture, 20k geometries)
 THERMAL_FP64_PIPE = 0.564
 WORKLOADS["stm_cov_1m"] = ("two-body state-transition matrices with covariance propagation, {n} "
                            "main-belt states, per-object spans U(-1000, 1000) d, one 6x6 "
@@ -1024,8 +1024,8 @@ def run_survey(args, world, rank, local):
                      "chunk_ms": fov_ms, "bytes_algorithmic": fov_bytes,
                      "note": "time of one chunk's fov_check_visible call (prefilter, n-body "
                              "branch if any, result copy-back); the chain's dominant kernel is "
-                             "the node kernel of the chunk re-propagations (about 22 of the 24 s; "
-                             "its roofline: profiles/nbody_nodes_kernel_10k.md)"},
+                             "the node kernel of the chunk re-propagations (about 22 of the 24 s), "
+                             "whose roofline the N-body workloads report"},
         "cpu_baseline": {"value": len(idx) * F / cpu_s, "unit": "object-fields/s",
                          "cores": os.cpu_count(), "kind": "port",
                          "sample": f"seeded {len(idx)}-object subsample of the population, full "
@@ -1396,7 +1396,7 @@ def run_thermal(args, world, rank, local):
                      "frac": None, "traffic": None, "fp64_pipe_active_ncu": THERMAL_FP64_PIPE,
                      "note": "one exp per seen facet and band dominates and has no fixed flop "
                              "count; the FP64 pipe is busy 56 % of the kernel's cycles with "
-                             "instruction issue the limit (profiles/thermal_frm_wise_20k.md)"},
+                             "instruction issue the limit (ncu, 20k geometries)"},
         "neatm_same_inputs": {"ms_per_step": 1e3 * t_neatm / args.steps,
                               "value": world * n * args.steps / t_neatm, "unit": "geometries/s"},
         "cpu_baseline": {"value": k / cpu_s, "unit": "geometries/s", "cores": os.cpu_count(),
@@ -1529,7 +1529,7 @@ def run_stm(args, world, rank, local):
                      "frac": (achieved / peak) if peak else None, "traffic": None,
                      "bytes_per_object": STM_BYTES_PER_OBJECT,
                      "note": "algorithmic bytes over the kernel time; the dual-number leaf "
-                             "Jacobians make it FP64/latency-bound (profiles/two_body_stm_1m.md)"},
+                             "Jacobians make it FP64/latency-bound (ncu: 31.6% FP64 pipe)"},
         "cpu_baseline": {"value": k / cpu_s, "unit": "objects/s", "cores": 1, "kind": "port",
                          "sample": f"the first {k} objects, one thread"},
         "e2e": {"value": world * n / e2e_s, "unit": "objects/s",

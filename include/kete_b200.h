@@ -327,9 +327,13 @@ int kete_b200_frm(int64_t n, const double* sun2obj, const double* sun2obs, const
  * KETE_B200_NOALLOC_MAX_OBJECTS is rejected with KETE_B200_E_ARGUMENT.
  * All array arguments are device pointers on the current device; the call only enqueues
  * work on `stream`.  The loaded SPK must already be resident on the device (load it after
- * kete_b200_init, or make one regular call first).  The first call on each device looks up
- * the array's device address (make it before any stream capture).  Calls that overlap on
- * the GPU share the array and race: serialize them. */
+ * kete_b200_init, or make one regular call first).  kete_b200_init loads the library's
+ * kernels and the array on the device it prepares and looks up the array's device address,
+ * so calls there load and allocate nothing; on a device it has not prepared the first call
+ * does that lookup (and the lazy module load it implies), so make it before any stream
+ * capture.  Calls that overlap on the GPU share the array and race, and the call reads the
+ * ephemeris table and launch configuration before it enqueues: serialize it with other
+ * calls, SPK loads and kete_b200_set_launch_config. */
 #define KETE_B200_NOALLOC_MAX_OBJECTS 1048576
 int kete_b200_propagate_n_body_noalloc(int64_t n, const double* pos, const double* vel,
                                        const double* jd0, const double* jd1, int frame,
@@ -339,7 +343,11 @@ int kete_b200_propagate_n_body_noalloc(int64_t n, const double* pos, const doubl
                                        double* min_dist, int32_t* counters, void* stream);
 
 /* --- diagnostics (no counterpart in the reference) ------------------------------------
- * FP64 pipe throughput of the current device, measured with independent DFMA chains
+ * Device allocations (cudaMalloc) the library has made since it was loaded: staging
+ * buffers that grow to a call's size, the ephemeris pool, facet tables, probes. */
+int64_t kete_b200_device_allocations(void);
+
+/* FP64 pipe throughput of the current device, measured with independent DFMA chains
  * (the FP64 roofline denominator).  Synchronous; ms may be NULL. */
 int kete_b200_fp64_probe(int64_t iters, double* tflops, float* ms);
 

@@ -545,7 +545,7 @@ static int ensure_tables(DevState& ds) {
             f[3 * N_FACETS + idx] = std::cos(lat);
             f[4 * N_FACETS + idx] = std::sin(lat);
         }
-        if ((rc = cuda_check(cudaMalloc(&ds.facets, f.size() * sizeof(double)), "cudaMalloc facets")))
+        if ((rc = cuda_check(counted_malloc((void**)&ds.facets, f.size() * sizeof(double)), "cudaMalloc facets")))
             return rc;
         if ((rc = cuda_check(cudaMemcpy(ds.facets, f.data(), f.size() * sizeof(double),
                                         cudaMemcpyHostToDevice),
@@ -571,7 +571,7 @@ static int ensure_device(DevState*& out) {
             if (ds.pool) cudaFree(ds.pool);
             ds.pool = nullptr;
             ds.pool_cap = 0;
-            if ((rc = cuda_check(cudaMalloc(&ds.pool, bytes), "cudaMalloc ephemeris pool"))) return rc;
+            if ((rc = cuda_check(counted_malloc((void**)&ds.pool, bytes), "cudaMalloc ephemeris pool"))) return rc;
             ds.pool_cap = bytes;
         }
         if (bytes && (rc = cuda_check(cudaMemcpy(ds.pool, g_pool_host.data(), bytes, cudaMemcpyHostToDevice),
@@ -595,7 +595,7 @@ static int staging(DevState& ds, size_t k, size_t bytes, void** p) {
         b.first = nullptr;
         b.second = 0;
         const size_t want = bytes < 256 ? 256 : bytes;
-        int rc = cuda_check(cudaMalloc(&b.first, want), "cudaMalloc staging buffer");
+        int rc = cuda_check(counted_malloc((void**)&b.first, want), "cudaMalloc staging buffer");
         if (rc) return rc;
         b.second = want;
     }
@@ -663,11 +663,10 @@ struct Stager {
     }
 };
 
-// Everything the allocation-free entry point needs, read under the lock without allocating:
-// the ephemeris must already be resident on the current device.
-// The node-kernel variant to launch for a force list: the warp-synchronous variants (6-8)
-// only pay off with the body-position cache, so a plan that does not fit it (or no fast plan)
-// runs their uncached twins (3-5), which integrate identically.
+// The node-kernel variant to launch for a force list: the cached variants (6-8 warp-
+// synchronous, 9-10 warp-pooled) only pay off with the body-position cache, so a plan that
+// does not fit it (or no fast plan) runs the uncached step-end twins (3-5), which integrate
+// identically.
 int nodes_variant_for(int variant, int n_force) {
     if (variant < 6) return variant;
     const FastPlan& P = n_force == g_eph.n_force_planets ? g_eph.fast_planets : g_eph.fast_all;
@@ -677,6 +676,8 @@ int nodes_variant_for(int variant, int n_force) {
     return variant;
 }
 
+// Everything the allocation-free entry point needs, read under the lock without allocating:
+// the ephemeris must already be resident on the current device.
 int noalloc_snapshot(int include_asteroids, int64_t center, NBodyArgs& a, LaunchConfig& cfg) {
     std::lock_guard<std::mutex> lk(g_mu);
     if (!g_eph.loaded) return set_error(KETE_B200_E_NO_EPHEMERIS, "no SPK loaded");
@@ -716,9 +717,16 @@ int kete_b200_init(int device) {
     if (rc) return rc;
     DevState* ds;
     if ((rc = ensure_device(ds))) return rc;
+    // load the kernels and resolve the fixed scratch of the allocation-free entry point now,
+    // so that its calls on this device load no module (which could allocate) themselves
+    if ((rc = preload_nodes_kernels())) return rc;
+    if ((rc = preload_order_kernels())) return rc;
+    if ((rc = noalloc_prepare())) return rc;
     g_device_ready = true;
     return 0;
 }
+
+int64_t kete_b200_device_allocations(void) { return g_device_allocations.load(); }
 
 int kete_b200_spk_load_buffer(const uint8_t* bytes, int64_t n_bytes) {
     if (!bytes || n_bytes <= 0) return set_error(KETE_B200_E_ARGUMENT, "empty SPK buffer");

@@ -18,6 +18,15 @@ struct EphemConst;
 int set_error(int code, const std::string& msg);
 int cuda_check(cudaError_t e, const char* what);
 extern std::atomic<int64_t> g_kernel_launches;  // kernels.cu
+// device allocations the library has made since it was loaded (kete_b200_device_allocations)
+extern std::atomic<int64_t> g_device_allocations;  // kernels.cu
+
+// cudaMalloc counted in g_device_allocations
+inline cudaError_t counted_malloc(void** p, size_t bytes) {
+    const cudaError_t e = cudaMalloc(p, bytes);
+    if (e == cudaSuccess) g_device_allocations.fetch_add(1, std::memory_order_relaxed);
+    return e;
+}
 
 // every launch helper adds the kernels it enqueued when it checks the launch
 inline int launched(int kernels, const char* what) {
@@ -68,6 +77,12 @@ int launch_covariance(int64_t n, int rows, int cols, const double* phi, const do
 int launch_nbody_thread(const NBodyArgs& a, int block, cudaStream_t stream);
 int launch_nbody_nodes(const NBodyArgs& a, int variant, int grid, cudaStream_t stream);
 int nodes_grid_size(int variant, int* grid);
+// load the node kernels and the processing-order kernels into the current context (module
+// loading is lazy: done here, it does not happen inside a later call)
+int preload_nodes_kernels();
+int preload_order_kernels();
+// resolve the allocation-free entry point's scratch address on the current device
+int noalloc_prepare();
 int launch_span_order(int64_t n, const double* pos, const double* vel, const double* jd0,
                       const double* jd1, int* scratch,
                       cudaStream_t stream);

@@ -18,6 +18,7 @@ namespace kb {
 // Kernels launched by this library since it was loaded (kete_b200_kernel_launches): every
 // launch helper below adds the kernels it enqueued when it checks the launch.
 std::atomic<int64_t> g_kernel_launches{0};
+std::atomic<int64_t> g_device_allocations{0};
 
 KB_CONSTANT_UPLOADER(kernels)
 
@@ -250,7 +251,7 @@ int fp64_probe(int64_t iters, double* tflops, float* ms_out) {
     if ((rc = cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attr")))
         return rc;
     double* d_out = nullptr;
-    if ((rc = cuda_check(cudaMalloc(&d_out, sizeof(double)), "cudaMalloc probe"))) return rc;
+    if ((rc = cuda_check(counted_malloc((void**)&d_out, sizeof(double)), "cudaMalloc probe"))) return rc;
     const int block = 256, grid = sms * 8;
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
@@ -346,6 +347,15 @@ __global__ void order_scatter_kernel(int64_t n, const double* __restrict__ pos,
         const int p = atomicAdd(&scratch[1 + ORDER_BUCKETS + b], 1);
         if (p >= 0 && p < n) order[p] = (int32_t)i;
     }
+}
+
+int preload_order_kernels() {
+    cudaFuncAttributes fa;
+    int rc = 0;
+    for (const void* f : {(const void*)order_hist_kernel, (const void*)order_scan_kernel,
+                          (const void*)order_scatter_kernel})
+        if ((rc = cuda_check(cudaFuncGetAttributes(&fa, f), "load ordering kernels"))) return rc;
+    return 0;
 }
 
 // Zero the header, histogram the work, scan, scatter.  scratch must hold

@@ -10,14 +10,18 @@
 // variant keeps that scratch in a fixed array of device memory reserved in the library
 // image instead.
 //
-// The fixed array is a file-scope __device__ object: every GPU that loads the library holds
-// it (KETE_B200_NOALLOC_MAX_OBJECTS * 4 + 1024 bytes, 4 MiB + 1 KiB) until the process
-// exits.  Host code cannot use the array's name as a device address, so on the first call
-// on each device the address is looked up with cudaGetSymbolAddress (with that device
-// current) and cached per device; that first call should therefore come before any stream
-// capture.  All calls share the one array: calls whose work overlaps on the GPU (different
-// streams, or different host threads) race on it and must be serialized by the caller.
-// The header that must start at zero (queue, histogram, cursors) is cleared by every call.
+// The fixed array is a file-scope __device__ object of KETE_B200_NOALLOC_MAX_OBJECTS * 4 +
+// 1024 bytes (4 MiB + 1 KiB).  CUDA loads modules lazily, so a device holds the array from
+// the moment its module is loaded until the process exits: kete_b200_init loads it (and the
+// kernels this entry point launches) on the device it prepares, and looks the array's
+// device address up there with cudaGetSymbolAddress -- host code cannot use the array's name
+// as a device address.  A device that kete_b200_init has not prepared gets the same lookup,
+// with the module loading it implies, on its first call here, which should then come before
+// any stream capture.  All calls share the one array: calls whose work overlaps on the GPU
+// (different streams, or different host threads) race on it and must be serialized by the
+// caller, as must a concurrent SPK load or kete_b200_set_launch_config on another thread
+// (the call reads the ephemeris table and launch configuration, then enqueues).  The header
+// that must start at zero (queue, histogram, cursors) is cleared by every call.
 #include <cstring>
 #include <mutex>
 
@@ -54,6 +58,11 @@ static int noalloc_scratch(int** out) {
     }
     *out = g_noalloc_ptr[dev];
     return 0;
+}
+
+int noalloc_prepare() {
+    int* p = nullptr;
+    return noalloc_scratch(&p);
 }
 
 }  // namespace kb

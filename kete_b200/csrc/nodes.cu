@@ -82,6 +82,17 @@ int launch_nbody_nodes(const NBodyArgs& a, int variant, int grid, cudaStream_t s
     return launched(1, "nbody_nodes_kernel launch");
 }
 
+int preload_nodes_kernels() {
+    cudaFuncAttributes fa;
+    int rc = 0;
+    for (int v = 0; v <= 10; ++v) {
+        if ((rc = cuda_check(cudaFuncGetAttributes(&fa, nodes_kernel_ptr(v)), "load node kernels")))
+            return rc;
+        if ((rc = allow_dyn_smem(v))) return rc;
+    }
+    return 0;
+}
+
 // Resident grid for the persistent (refill) form: blocks per SM from the occupancy API.
 int nodes_grid_size(int variant, int* grid) {
     int dev = 0, sms = 0, per_sm = 0;

@@ -148,8 +148,10 @@ def frm_arrays(sun2obj, sun2obs, h_mag, g_param, diam, vis_albedo, emissivity, b
 def neatm_flux(sun2obj, sun2obs, v_albedo, g_param, beaming, diameter, wavelength,
                emissivity=0.9):
     """kete.flux.neatm_flux (src/kete/rust/flux/common.rs:223-261): NEATM thermal flux in
-    Jy of one object at one wavelength (nm).  Array arguments (sun2obj/sun2obs (3, n) or
-    (n, 3), parameters scalar or (n,)) return an (n,) array, computed on the GPU."""
+    Jy of one object at one wavelength (nm).  Array arguments (sun2obj/sun2obs (3, n), one
+    column per object, parameters scalar or (n,)) return an (n,) array, computed on the GPU.
+    An (n, 3) array with n != 3 is accepted and read one row per object; a 3 x 3 array is
+    always read as three columns."""
     return _single_band_thermal("neatm", sun2obj, sun2obs, v_albedo, g_param, diameter,
                                 wavelength, emissivity, beaming)
 
@@ -162,7 +164,8 @@ def frm_flux(sun2obj, sun2obs, v_albedo, g_param, diameter, wavelength, emissivi
 
 
 def _as_3n(v):
-    """(3,) -> (3, 1); (3, n) as given; (n, 3) transposed."""
+    """(3,) -> (3, 1); (3, n) as given, one column per object (a 3 x 3 array included); an
+    (n, 3) array with n != 3 transposed."""
     a = np.asarray(v, dtype=np.float64)
     if a.ndim == 1:
         return a.reshape(3, 1)

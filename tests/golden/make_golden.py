@@ -72,4 +72,8 @@ def main(root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("KETE_REFERENCE_ROOT")
+    if not root:
+        sys.exit("usage: make_golden.py <path to the kete reference checkout> "
+                 "(or set KETE_REFERENCE_ROOT)")
+    main(root)

@@ -46,4 +46,8 @@ def main(src):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/docs/data/20000042.bsp")
+    path = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("KETE_REFERENCE_BSP")
+    if not path:
+        sys.exit("usage: make_spk_fixtures.py <path to the reference's docs/data/20000042.bsp> "
+                 "(or set KETE_REFERENCE_BSP)")
+    main(path)

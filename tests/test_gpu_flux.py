@@ -162,3 +162,14 @@ def test_single_band_thermal_functions(gpu, oracle):
         o = oracle.frm_total_flux(s2obj_n[:, i], s2obs_n[:, i], h, 0.15, 2.0, 0.1, 0.9,
                                   [22000.0], [0.0])
         assert abs(fa[i] / o["thermal_fluxes"][0] - 1) < 1e-12
+
+
+def test_thermal_functions_three_objects_are_columns(gpu):
+    """A 3 x 3 sun2obj / sun2obs is three objects, one column each (not three rows)."""
+    s2obj_n, s2obs_n = _geometries(3, 17)
+    for fn, args in ((gpu.flux.neatm_flux, (0.1, 0.15, 1.2, 2.0, 12000.0)),
+                     (gpu.flux.frm_flux, (0.1, 0.15, 2.0, 12000.0))):
+        batch = fn(np.ascontiguousarray(s2obj_n), np.ascontiguousarray(s2obs_n), *args)
+        single = [fn(s2obj_n[:, i].copy(), s2obs_n[:, i].copy(), *args) for i in range(3)]
+        assert batch.shape == (3,)
+        assert np.allclose(batch, single, rtol=1e-14, atol=0.0)

@@ -63,7 +63,7 @@ def test_radau_basic_two_body(oracle, goldens):
 
 
 def test_radau_matches_kepler(oracle):
-    """Radau + central force against the closed-form solution (SURVEY pin 2)."""
+    """Radau + central force against the closed-form two-body solution."""
     from kete_b200 import synthetic
 
     pos, vel = synthetic.main_belt(20, seed=5)
@@ -219,7 +219,7 @@ def test_hg_zero_phase(oracle):
 
 
 def test_spk_roundtrip(oracle_spk):
-    """Re-reading the written SPK returns the fitted planet states (SURVEY pin 4)."""
+    """Re-reading the written SPK returns the fitted planet states."""
     from kete_b200 import synthetic
 
     for body in (10, 1, 2, 3, 4, 5, 6, 7, 8, 399, 301):

@@ -18,7 +18,8 @@ from kete_b200 import synthetic
 AU_KM = 149597870.7
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 SUBSET = os.path.join(GOLDEN, "spk_type21_subset.bsp")
-FULL = "/root/reference/docs/data/20000042.bsp"
+# the full JPL file the fixture was cut from, when a reference checkout is named
+FULL = os.environ.get("KETE_REFERENCE_BSP", "")
 
 
 def _load(oracle, *paths):
@@ -57,7 +58,8 @@ def test_type21_outside_coverage(oracle):
     assert rc == 3  # DAFLimits
 
 
-@pytest.mark.skipif(not os.path.exists(FULL), reason="the reference's type-21 file is absent")
+@pytest.mark.skipif(not FULL or not os.path.exists(FULL),
+                    reason="KETE_REFERENCE_BSP does not name the reference's type-21 file")
 def test_type21_subset_matches_full_file(oracle):
     _, _, _, _, _, s0, s1 = _records(SUBSET)
     jds = np.linspace(s0 + 10.0, s1 - 10.0, 97) / 86400.0 + 2451545.0

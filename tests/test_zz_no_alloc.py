@@ -28,6 +28,7 @@ def _bind(lib):
         ctypes.c_int64, v, v, v, v, ctypes.c_int, ctypes.c_int64, ctypes.c_int, v, v, v, v, v, v,
         v, v, ctypes.c_int, ctypes.c_int, v]
     lib.kete_b200_last_error.restype = ctypes.c_char_p
+    lib.kete_b200_device_allocations.restype = ctypes.c_int64
     return lib
 
 
@@ -57,6 +58,7 @@ def test_noalloc_matches_regular_entry_point(gpu):
                                         2, 1, stream)
     assert rc == 0, lib.kete_b200_last_error()
     torch.cuda.synchronize()
+    allocations = lib.kete_b200_device_allocations()
     for call in range(2):  # the shared scratch must be reset correctly on every call
         op, ov, os_ = outputs()
         rc = lib.kete_b200_propagate_n_body_noalloc(
@@ -72,6 +74,8 @@ def test_noalloc_matches_regular_entry_point(gpu):
         assert err[ok].max() < TOL_AU, (call, err[ok].max())
         verr = (ov - rv).abs().max(dim=0).values.cpu().numpy()
         assert verr[ok].max() < TOL_AU, (call, verr[ok].max())
+        # the library allocated no device memory for either call
+        assert lib.kete_b200_device_allocations() == allocations, call
 
 
 def test_noalloc_rejects_more_objects_than_its_scratch(gpu):
