@@ -376,6 +376,13 @@ int kete_b200_set_launch_config(int nodes_variant, int nodes_refill, int thread_
 #define KETE_B200_STEP_LIMIT_MAX (1 << 24)
 int kete_b200_set_step_limit(int64_t max_steps);
 
+/* Form of the N-body forward sensitivities (kete_b200_propagate_n_body_stm and the N-body
+ * covariance propagation built on it; no counterpart in the reference): 0 (default) = eight
+ * lanes per object, each corrector node's force Jacobian taken once per step attempt at its
+ * last iteration's point; 1 = one object per thread, every iteration's Jacobian at its own
+ * points.  The two agree to about 1e-8 relative. */
+int kete_b200_set_sensitivity_form(int form);
+
 /* Number of kernels this library has enqueued since it was loaded (no counterpart in the
  * reference): read it before and after a call to count the call's GPU launches. */
 int64_t kete_b200_kernel_launches(void);

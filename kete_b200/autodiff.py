@@ -46,6 +46,15 @@ def _bind():
     return L
 
 
+def set_sensitivity_form(form: int = 0):
+    """Form of the forward sensitivities (kete_b200_set_sensitivity_form): 0 = eight lanes per
+    object with each node's Jacobian taken once per step attempt (default); 1 = one object
+    per thread with every corrector iteration's Jacobian at its own points."""
+    L = _lib.lib()
+    L.kete_b200_set_sensitivity_form.argtypes = [ctypes.c_int]
+    _lib.check(L.kete_b200_set_sensitivity_form(int(form)))
+
+
 def propagate_n_body_stm_arrays(pos, vel, jd0, epochs, frame=Frames.Ecliptic, center=10,
                                 include_asteroids=False, nongrav=None):
     """States at each epoch and their sensitivities.

@@ -179,6 +179,7 @@ __device__ __forceinline__ void sens_rounds(SensGroup& G, SpkForce& F, Policy& P
                 G.predict = false;
             } else {
                 P.end_attempt(G, true);
+                if (G.phase == SP_DONE) return;  // the policy failed the object
                 G.h_prev = G.h;
                 G.predict = true;
                 G.h = G.next_h;
@@ -249,6 +250,7 @@ __device__ __forceinline__ void sens_rounds(SensGroup& G, SpkForce& F, Policy& P
         __syncwarp(gmask);
         if (G.iter >= 10) {  // not converged: retry with a smaller step (radau.rs:199-210)
             P.end_attempt(G, false);
+            if (G.phase == SP_DONE) return;  // the policy failed the object
             G.predict = false;
             G.failures += 1;
             G.h *= 0.7;

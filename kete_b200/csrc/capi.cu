@@ -1212,7 +1212,7 @@ int kete_b200_propagate_n_body_stm(int64_t n, const double* pos, const double* v
     a.status = S.out(status, (size_t)n);
     a.max_loops = g_launch.max_loops;
     if (S.rc) return S.rc;
-    if ((rc = launch_nbody_stm(a, st))) return rc;
+    if ((rc = launch_nbody_stm(a, g_launch.sens_form, st))) return rc;
     return S.finish();
 }
 
@@ -1534,6 +1534,13 @@ int kete_b200_set_launch_config(int nodes_variant, int nodes_refill, int thread_
     g_launch.nodes_variant = nodes_variant;
     g_launch.nodes_refill = nodes_refill ? 1 : 0;
     g_launch.thread_block = thread_block;
+    return 0;
+}
+
+int kete_b200_set_sensitivity_form(int form) {
+    if (form != 0 && form != 1) return set_error(KETE_B200_E_ARGUMENT, "sensitivity form is 0 or 1");
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_launch.sens_form = form;
     return 0;
 }
 

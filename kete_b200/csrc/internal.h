@@ -96,6 +96,7 @@ struct LaunchConfig {
     // has not reached its target after this many step attempts returns ST_TIMEOUT
     int max_loops = 1 << 20;
     int max_loops_long = 1 << 24;  // system integration (every batch's whole span)
+    int sens_form = 0;  // forward sensitivities: 0 node-parallel, 1 one object per thread
 };
 LaunchConfig& launch_config();
 int noalloc_snapshot(int include_asteroids, int64_t center, NBodyArgs& a, LaunchConfig& cfg);
@@ -124,7 +125,8 @@ struct StmArgs {
     int32_t* status;
     int max_loops;
 };
-int launch_nbody_stm(const StmArgs& a, cudaStream_t stream);
+// form: 0 = node-parallel (8 lanes per object), 1 = one object per thread
+int launch_nbody_stm(const StmArgs& a, int form, cudaStream_t stream);
 
 // reverse-mode gradients: checkpointed forward pass and adjoint pass (adjoint.cuh)
 constexpr int SENS_STRIDE = 36;       // doubles per checkpoint / attempt record

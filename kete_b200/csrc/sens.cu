@@ -1,9 +1,12 @@
-// sens.cu -- N-body forward sensitivities: the variational form (nbody_stm_kernel, every
-// force term in dual numbers from tangent.cuh) and its host launcher.
+// sens.cu -- N-body forward sensitivities: the node-parallel form (nbody_stm_nodes_kernel,
+// stm_nodes.cuh) and the one-object-per-thread form (nbody_stm_kernel, every force term in
+// dual numbers from tangent.cuh, the Jacobian of every corrector iteration at its own
+// points), with their host launcher.
 #include "common.cuh"
 #include "forces.cuh"
 #include "internal.h"
 #include "radau.cuh"
+#include "stm_nodes.cuh"
 #include "tangent.cuh"
 
 namespace kb {
@@ -244,10 +247,22 @@ __global__ void __launch_bounds__(64) nbody_stm_kernel(StmArgs a) {
     a.status[i] = rc;
 }
 
-int launch_nbody_stm(const StmArgs& a, cudaStream_t stream) {
+int launch_nbody_stm(const StmArgs& a, int form, cudaStream_t stream) {
     if (a.n <= 0) return 0;
-    nbody_stm_kernel<<<(unsigned)((a.n + 63) / 64), 64, 0, stream>>>(a);
-    return launched(1, "nbody_stm_kernel launch");
+    if (form == 1) {  // one object per thread
+        nbody_stm_kernel<<<(unsigned)((a.n + 63) / 64), 64, 0, stream>>>(a);
+        return launched(1, "nbody_stm_kernel launch");
+    }
+    // node-parallel: tangents in dynamic shared memory above the 48 KB static limit (a
+    // function attribute, set on every launch: it is not a stream operation)
+    int rc = cuda_check(cudaFuncSetAttribute(nbody_stm_nodes_kernel<1>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             STM_DYN_SMEM),
+                        "sensitivity kernel shared memory");
+    if (rc) return rc;
+    const int64_t grid = (a.n * SG + STM_BLOCK - 1) / STM_BLOCK;
+    nbody_stm_nodes_kernel<1><<<(unsigned)grid, STM_BLOCK, STM_DYN_SMEM, stream>>>(a);
+    return launched(1, "nbody_stm_nodes_kernel launch");
 }
 
 }  // namespace kb

@@ -20,6 +20,17 @@ EPOCH = synthetic.EPOCH
 EPOCHS = EPOCH + np.array([60.0, 250.0, 730.0])
 
 
+@pytest.fixture(params=[0, 1], ids=["nodes", "thread"])
+def form(request, gpu):
+    """Both forms of the forward sensitivities: eight lanes per object (default) and one
+    object per thread."""
+    from kete_b200.autodiff import set_sensitivity_form
+
+    set_sensitivity_form(request.param)
+    yield request.param
+    set_sensitivity_form(0)
+
+
 def _population(n_neo=6, n_comet=4, seed=77):
     pos_n, vel_n = synthetic.neo(n_neo, seed=seed)
     pos_c, vel_c = synthetic.neo(n_comet, seed=seed + 1)
@@ -35,7 +46,7 @@ def _population(n_neo=6, n_comet=4, seed=77):
     return pos, vel, ng
 
 
-def test_stm_states_match_oracle_chain(gpu, oracle_spk):
+def test_stm_states_match_oracle_chain(gpu, form, oracle_spk):
     from kete_b200.autodiff import propagate_n_body_stm_arrays
 
     pos, vel, ng = _population()
@@ -73,7 +84,7 @@ def _richardson(f, d):
     return (4.0 * D1 - D2) / 3.0
 
 
-def test_stm_vs_finite_differences(gpu):
+def test_stm_vs_finite_differences(gpu, form):
     from kete_b200.autodiff import propagate_n_body_stm_arrays
 
     pos, vel, ng = _population()
@@ -94,7 +105,7 @@ def test_stm_vs_finite_differences(gpu):
         assert err.max() < 1e-5, (p, err.max())
 
 
-def test_stm_identity_at_start_and_frames(gpu):
+def test_stm_identity_at_start_and_frames(gpu, form):
     """An epoch equal to the start gives the identity (A columns zero), in either frame."""
     from kete_b200.autodiff import propagate_n_body_stm_arrays
     from kete_b200.state import Frames
@@ -111,7 +122,7 @@ def test_stm_identity_at_start_and_frames(gpu):
         assert np.abs(s[0, 0:3] - pos).max() < 1e-13
 
 
-def test_stm_failure_is_nan(gpu):
+def test_stm_failure_is_nan(gpu, form):
     from kete_b200.autodiff import propagate_n_body_stm_arrays
 
     pos, vel, ng = _population(2, 0)
@@ -171,3 +182,26 @@ def test_radec_loss_gradient_through_autograd(gpu, method):
                 fd = _richardson(loss_at, deltas[which])
                 tol = 2e-5 * max(abs(g[j]), np.abs(g).max() * 1e-3)
                 assert abs(fd - g[j]) <= tol, (which, j, fd, g[j])
+
+
+def test_stm_forms_agree(gpu):
+    """The node-parallel form (each node's Jacobian once per attempt, at its last corrector
+    iteration's point) against the one-object-per-thread form (every iteration's Jacobian at
+    its own points): per object, epoch and direction, 1e-7 of the column's largest entry."""
+    from kete_b200.autodiff import propagate_n_body_stm_arrays, set_sensitivity_form
+
+    pos, vel, ng = _population(24, 8, seed=13)
+    n = pos.shape[1]
+    jd0 = np.full(n, EPOCH)
+    out = {}
+    try:
+        for f in (0, 1):
+            set_sensitivity_form(f)
+            out[f] = propagate_n_body_stm_arrays(pos, vel, jd0, EPOCHS, nongrav=ng)
+    finally:
+        set_sensitivity_form(0)
+    (s0, m0, st0), (s1, m1, st1) = out[0], out[1]
+    assert (st0 == 0).all() and (st1 == 0).all()
+    assert np.abs(s0 - s1).max() < 1e-10  # the same trajectories, to rounding
+    err = np.abs(m0 - m1).max(axis=1) / np.abs(m1).max(axis=1)  # (K, 8, n)
+    assert err.max() < 1e-7, err.max()
