@@ -117,9 +117,11 @@ struct StmNodesPolicy {
     __device__ void end_attempt(SensGroup& G, bool converged) {
         __syncwarp(gmask);
         const double h = G.h, h2 = h * h;
-        // node Jacobians at the last corrector iteration's points
+        // node Jacobians at the last corrector iteration's points (lanes 0-6) and, after an
+        // accepted step, the Jacobian at the new state (lane 7) in the same round
         double J[18], jp[6];
         bool ok = true;
+        if (lane == 7 && converged) ok = jacobian(G.t, G.x, G.v, J, jp);
         if (lane < 7) {
             const double f = nrow[14], frac2 = nrow[15];
             double xe[3], ve[3];
@@ -143,6 +145,21 @@ struct StmNodesPolicy {
             G.phase = SP_DONE;
             return;
         }
+        if (lane == 7 && converged) {  // lane 7 publishes J' (in the dE area, free until used)
+#pragma unroll
+            for (int i = 0; i < 18; ++i) ts[STM_DE + i] = J[i];
+#pragma unroll
+            for (int i = 0; i < 6; ++i) ts[STM_DE + 18 + i] = jp[i];
+        }
+        __syncwarp(gmask);
+        double Jn[18], jpn[6];  // J' in every lane, read before the dE area is reused
+        if (converged) {
+#pragma unroll
+            for (int i = 0; i < 18; ++i) Jn[i] = ts[STM_DE + i];
+#pragma unroll
+            for (int i = 0; i < 6; ++i) jpn[i] = ts[STM_DE + 18 + i];
+        }
+        __syncwarp(gmask);
         // the M corrector iterations, linearised
         const int M = G.iter;
         for (int m = 0; m < M; ++m) {
@@ -215,17 +232,8 @@ struct StmNodesPolicy {
                 ts[STM_DV + 8 * c + p] = dv + h * (da + du);
             }
         }
-        // da' from the Jacobian at the accepted state (every lane evaluates it; the lane's
-        // cache holds the bodies at the new epoch after the exact evaluation)
-        double J2[18], jp2[6];
-        ok = jacobian(G.t, G.x, G.v, J2, jp2);
-        __syncwarp(gmask);
-        if (!__all_sync(gmask, ok)) {
-            G.rc = ST_DAF_LIMITS;
-            G.phase = SP_DONE;
-            return;
-        }
-        tangent_acc(J2, jp2);
+        // da' from the Jacobian at the accepted state
+        tangent_acc(Jn, jpn);
         __syncwarp(gmask);
     }
 
