@@ -978,6 +978,16 @@ def run_survey(args, world, rank, local):
     torch.cuda.synchronize()
     fov_ms = e0.elapsed_time(e1) / reps
     fov_bytes = n * 57 + sub.numel() * 8
+    # one more pass of the chain with its stages timed apart (device synchronized around
+    # each stage): the N-body re-propagations, the field checks, the magnitudes
+    stages = {}
+    ff_s, oo_s, ss_s = fov_state_check_arrays(P, V, EPOCH, TB, SURVEY_DT_LIMIT, False, G,
+                                              stage_times=stages)
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    survey_magnitudes(ff_s, oo_s, ss_s, table, h, pv)
+    torch.cuda.synchronize()
+    stages["magnitudes"] = time.perf_counter() - t
     peaks = measured_peaks()
     if rank != 0:
         return
@@ -1016,16 +1026,21 @@ def run_survey(args, world, rank, local):
                    "launch": launch,
                    "l2": "inputs (the population's states) larger than L2",
                    "parallelism": f"replicas x{world} (objects independent)"},
-        "roofline": {"bound": "hbm", "kernel": "fov_prefilter_kernel (one chunk)",
+        "stages_s": {"nbody_repropagation": stages.get("propagate"),
+                     "field_checks": stages.get("check"), "magnitudes": stages.get("magnitudes"),
+                     "note": "one extra pass of the chain with the device synchronized around "
+                             "each stage"},
+        "roofline": {"bound": "hbm", "kernel": "fov_screen_kernel + fov_pairs_kernel (one chunk)",
                      "achieved": fov_bytes / (fov_ms * 1e-3) / 1e9, "peak": peaks.get("hbm_gbs"),
                      "unit": "GB/s",
                      "frac": (fov_bytes / (fov_ms * 1e-3) / 1e9) / peaks["hbm_gbs"]
                      if peaks.get("hbm_gbs") else None, "traffic": None,
                      "chunk_ms": fov_ms, "bytes_algorithmic": fov_bytes,
-                     "note": "time of one chunk's fov_check_visible call (prefilter, n-body "
-                             "branch if any, result copy-back); the chain's dominant kernel is "
-                             "the node kernel of the chunk re-propagations (about 22 of the 24 s), "
-                             "whose roofline the N-body workloads report"},
+                     "note": "time of one chunk's fov_check_visible call (linear screen, "
+                             "two-body pass, n-body branch if any, result copy-back); the "
+                             "chain's dominant kernel is the node kernel of the chunk "
+                             "re-propagations (stages_s), whose roofline the N-body workloads "
+                             "report"},
         "cpu_baseline": {"value": len(idx) * F / cpu_s, "unit": "object-fields/s",
                          "cores": os.cpu_count(), "kind": "port",
                          "sample": f"seeded {len(idx)}-object subsample of the population, full "

@@ -383,6 +383,12 @@ int kete_b200_set_step_limit(int64_t max_steps);
  * points.  The two agree to about 1e-8 relative. */
 int kete_b200_set_sensitivity_form(int form);
 
+/* Form of the field checks (kete_b200_fov_check_visible and the schedule built on it; no
+ * counterpart in the reference): 0 (default) = a first-order linear screen of every
+ * (object, field) pair, then the two-body light-time solve on the pairs that pass, one
+ * thread each; 1 = both in one pass, one thread per object.  Same results. */
+int kete_b200_set_fov_form(int form);
+
 /* Number of kernels this library has enqueued since it was loaded (no counterpart in the
  * reference): read it before and after a call to count the call's GPU launches. */
 int64_t kete_b200_kernel_launches(void);

@@ -1460,29 +1460,41 @@ int kete_b200_fov_check_visible(int64_t n_obj, const double* pos, const double* 
     a.out_obj = S.out(out_obj, (size_t)capacity);
     a.out_state = S.out(out_state, 7 * (size_t)capacity);
     if (S.rc) return S.rc;
-    // scratch: counters and the n-body candidate list (grown and re-run on overflow)
+    // scratch: counters, the n-body candidate list and the screened-pair list (grown and
+    // re-run on overflow)
     void* cnt = nullptr;
-    if ((rc = staging(*ds, 20, 2 * sizeof(unsigned long long), &cnt))) return rc;
+    if ((rc = staging(*ds, 20, 3 * sizeof(unsigned long long), &cnt))) return rc;
     a.counters = (unsigned long long*)cnt;
+    const bool two_pass = g_launch.fov_form == 0;
     int64_t cand_cap = std::max<int64_t>(1024, n_obj / 16);
-    unsigned long long h[2] = {0, 0};
+    int64_t pair_cap = std::max<int64_t>(4096, n_obj / 4);
+    unsigned long long h[3] = {0, 0, 0};
     for (int attempt = 0; attempt < 3; ++attempt) {
-        void *cf = nullptr, *co = nullptr;
+        void *cf = nullptr, *co = nullptr, *pf = nullptr, *po = nullptr;
         if ((rc = staging(*ds, 21, (size_t)cand_cap * sizeof(int32_t), &cf))) return rc;
         if ((rc = staging(*ds, 22, (size_t)cand_cap * sizeof(int32_t), &co))) return rc;
+        if (two_pass) {
+            if ((rc = staging(*ds, 30, (size_t)pair_cap * sizeof(int32_t), &pf))) return rc;
+            if ((rc = staging(*ds, 31, (size_t)pair_cap * sizeof(int32_t), &po))) return rc;
+        }
         a.cand_fov = (int32_t*)cf;
         a.cand_obj = (int32_t*)co;
         a.cand_capacity = cand_cap;
-        if ((rc = cuda_check(cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned long long), st), "clear counters")))
+        a.pair_fov = (int32_t*)pf;
+        a.pair_obj = (int32_t*)po;
+        a.pair_capacity = two_pass ? pair_cap : 0;
+        if ((rc = cuda_check(cudaMemsetAsync(cnt, 0, 3 * sizeof(unsigned long long), st), "clear counters")))
             return rc;
-        if ((rc = launch_fov_prefilter(a, st))) return rc;
+        if ((rc = two_pass ? launch_fov_screen(a, st) : launch_fov_prefilter(a, st))) return rc;
         if ((rc = cuda_check(cudaMemcpyAsync(h, cnt, sizeof h, cudaMemcpyDeviceToHost, st), "read counters")))
             return rc;
         if ((rc = cuda_check(cudaStreamSynchronize(st), "stream synchronize"))) return rc;
-        if ((int64_t)h[1] <= cand_cap) break;
-        cand_cap = (int64_t)h[1] + 1024;
+        if ((int64_t)h[1] <= cand_cap && (!two_pass || (int64_t)h[2] <= pair_cap)) break;
+        cand_cap = std::max<int64_t>(cand_cap, (int64_t)h[1] + 1024);
+        pair_cap = std::max<int64_t>(pair_cap, (int64_t)h[2] + 4096);
         if (attempt == 2) return set_error(KETE_B200_E_CUDA, "candidate list kept overflowing");
     }
+    if (two_pass && (rc = launch_fov_pairs(a, (int64_t)h[2], st))) return rc;
     const int64_t m = (int64_t)h[1];
     if (m > 0) {
         // n-body branch (fov_like.rs:90-108): Radau every candidate to its field's epoch
@@ -1517,9 +1529,10 @@ int kete_b200_fov_check_visible(int64_t n_obj, const double* pos, const double* 
         if ((rc = launch_nbody_nodes(nb, nodes_variant_for(g_launch.nodes_variant, nb.n_force), 0, st)))
             return rc;
         if ((rc = launch_fov_finish(a, m, (double*)op, (double*)ov, (int32_t*)os, st))) return rc;
-        if ((rc = cuda_check(cudaMemcpyAsync(h, cnt, sizeof h, cudaMemcpyDeviceToHost, st), "read counters")))
-            return rc;
     }
+    // the visible count after the last pass that emits (two-body pairs, n-body finish)
+    if ((rc = cuda_check(cudaMemcpyAsync(h, cnt, sizeof h, cudaMemcpyDeviceToHost, st), "read counters")))
+        return rc;
     if ((rc = S.finish())) return rc;
     if ((rc = cuda_check(cudaStreamSynchronize(st), "stream synchronize"))) return rc;
     *n_visible = (int64_t)h[0];
@@ -1534,6 +1547,13 @@ int kete_b200_set_launch_config(int nodes_variant, int nodes_refill, int thread_
     g_launch.nodes_variant = nodes_variant;
     g_launch.nodes_refill = nodes_refill ? 1 : 0;
     g_launch.thread_block = thread_block;
+    return 0;
+}
+
+int kete_b200_set_fov_form(int form) {
+    if (form != 0 && form != 1) return set_error(KETE_B200_E_ARGUMENT, "field-check form is 0 or 1");
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_launch.fov_form = form;
     return 0;
 }
 

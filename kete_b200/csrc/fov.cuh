@@ -141,6 +141,102 @@ __global__ void __launch_bounds__(128) fov_prefilter_kernel(FovArgs a) {
     }
 }
 
+// Appends (f, i) for every lane of the warp with `take` set, one atomic per warp.
+__device__ __forceinline__ void fov_append_pair(const FovArgs& a, bool take, int f, int64_t i) {
+    const unsigned active = __activemask();
+    const unsigned want = __ballot_sync(active, take);
+    if (!want) return;
+    const int leader = __ffs(want) - 1;
+    const int lane = threadIdx.x & 31;
+    unsigned long long base = 0;
+    if (lane == leader) base = atomicAdd(&a.counters[2], (unsigned long long)__popc(want));
+    base = __shfl_sync(active, base, leader);
+    if (take) {
+        const unsigned long long k = base + __popc(want & ((1u << lane) - 1u));
+        if ((int64_t)k < a.pair_capacity) {
+            a.pair_fov[k] = f;
+            a.pair_obj[k] = (int32_t)i;
+        }
+    }
+}
+
+// Two-pass form of fov_prefilter_kernel.  First pass: one thread per object over tiles of
+// fields, the first-order linear screen of check_linear only (a few dozen uniform FP64
+// operations per pair); the pairs that pass are appended to a list.  Fields at least
+// dt_limit away from the object's epoch take check_visible's n-body branch here as in
+// fov_prefilter_kernel (its two-body screen in place), which the fov_state_check schedule
+// never reaches.  The second pass (fov_pairs_kernel) runs the two-body light-time solve on the
+// listed pairs only, one thread per pair, so the solve's Newton iterations no longer leave the
+// lanes of screened-out pairs idle.
+__global__ void __launch_bounds__(128) fov_screen_kernel(FovArgs a) {
+    __shared__ double s_f[FOV_TILE * FOV_STRIDE];
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool active = i < a.n_obj && (a.valid == nullptr || a.valid[i]);
+    double pos[3] = {0, 0, 0}, vel[3] = {0, 0, 0}, jd = 0.0;
+    if (active) {
+        pos[0] = a.pos[i]; pos[1] = a.pos[a.n_obj + i]; pos[2] = a.pos[2 * a.n_obj + i];
+        vel[0] = a.vel[i]; vel[1] = a.vel[a.n_obj + i]; vel[2] = a.vel[2 * a.n_obj + i];
+        jd = a.jd[i];
+    }
+    for (int64_t base = 0; base < a.n_fov; base += FOV_TILE) {
+        const int nt = (int)((a.n_fov - base) < FOV_TILE ? (a.n_fov - base) : FOV_TILE);
+        __syncthreads();
+        for (int q = threadIdx.x; q < nt * FOV_STRIDE; q += blockDim.x) {
+            const int f = q / FOV_STRIDE, c = q % FOV_STRIDE;
+            s_f[q] = a.fov[(int64_t)c * a.n_fov + base + f];
+        }
+        __syncthreads();
+        for (int t = 0; t < nt; ++t) {
+            const double* f = s_f + t * FOV_STRIDE;
+            bool take = false;
+            if (active) {
+                const double dvx = vel[0] - f[4], dvy = vel[1] - f[5], dvz = vel[2] - f[6];
+                const double max_dist = norm3(dvx, dvy, dvz) * a.dt_limit * 2.0;
+                if (fabs(jd - f[0]) < a.dt_limit) {
+                    // check_linear: first-order light delay, straight-line motion
+                    const double rel0 = pos[0] - f[1], rel1 = pos[1] - f[2], rel2 = pos[2] - f[3];
+                    const double dt = f[0] - jd - norm3(rel0, rel1, rel2) * C_AU_PER_DAY_INV;
+                    const double nrel[3] = {pos[0] + vel[0] * dt - f[1],
+                                            pos[1] + vel[1] * dt - f[2],
+                                            pos[2] + vel[2] * dt - f[3]};
+                    double dist;
+                    take = patch_contains(f, nrel, dist) || !(dist > max_dist);
+                } else {
+                    double dist, fin[7];
+                    bool inside;
+                    if (fov_two_body(f, jd, pos, vel, inside, dist, fin) == ST_OK &&
+                        (inside || !(dist > max_dist))) {
+                        const unsigned long long k = atomicAdd(&a.counters[1], 1ULL);
+                        if ((int64_t)k < a.cand_capacity) {
+                            a.cand_fov[k] = (int32_t)(base + t);
+                            a.cand_obj[k] = (int32_t)i;
+                        }
+                    }
+                }
+            }
+            fov_append_pair(a, take, (int)(base + t), i);
+        }
+    }
+}
+
+// Second pass: check_two_body for every screened pair (one thread per pair); visible pairs
+// are emitted as in fov_prefilter_kernel.
+__global__ void __launch_bounds__(128) fov_pairs_kernel(FovArgs a, int64_t m) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= m) return;
+    const int f = a.pair_fov[k];
+    const int64_t i = a.pair_obj[k];
+    double fcol[FOV_STRIDE];
+#pragma unroll
+    for (int c = 0; c < FOV_STRIDE; ++c) fcol[c] = a.fov[(int64_t)c * a.n_fov + f];
+    const double pos[3] = {a.pos[i], a.pos[a.n_obj + i], a.pos[2 * a.n_obj + i]};
+    const double vel[3] = {a.vel[i], a.vel[a.n_obj + i], a.vel[2 * a.n_obj + i]};
+    double dist, fin[7];
+    bool inside;
+    if (fov_two_body(fcol, a.jd[i], pos, vel, inside, dist, fin) == ST_OK && inside)
+        fov_emit(a, f, i, fin);
+}
+
 // Gather the n-body candidates' states (object state, target epoch = observer epoch).
 __global__ void fov_gather_kernel(FovArgs a, int64_t m, double* __restrict__ gpos,
                                   double* __restrict__ gvel, double* __restrict__ gjd0,

@@ -22,12 +22,15 @@ struct FovArgs {
     double dt_limit;
     int64_t capacity;      // visible outputs
     int64_t cand_capacity; // n-body candidates
-    unsigned long long* counters;  // [0] visible, [1] n-body candidates
+    int64_t pair_capacity; // (field, object) pairs that pass the linear screen
+    unsigned long long* counters;  // [0] visible, [1] n-body candidates, [2] screened pairs
     int32_t* out_fov;
     int32_t* out_obj;
     double* out_state;     // 7 x capacity
     int32_t* cand_fov;
     int32_t* cand_obj;
+    int32_t* pair_fov;
+    int32_t* pair_obj;
 };
 
 }  // namespace kb

@@ -97,6 +97,7 @@ struct LaunchConfig {
     int max_loops = 1 << 20;
     int max_loops_long = 1 << 24;  // system integration (every batch's whole span)
     int sens_form = 0;  // forward sensitivities: 0 node-parallel, 1 one object per thread
+    int fov_form = 0;   // field checks: 0 linear screen + two-body pass, 1 one fused pass
 };
 LaunchConfig& launch_config();
 int noalloc_snapshot(int include_asteroids, int64_t center, NBodyArgs& a, LaunchConfig& cfg);
@@ -197,6 +198,8 @@ int launch_accel(const AccelArgs& a, bool vec, cudaStream_t stream);
 struct NeatmArgs;
 struct FovArgs;
 int launch_fov_prefilter(const FovArgs& a, cudaStream_t stream);
+int launch_fov_screen(const FovArgs& a, cudaStream_t stream);
+int launch_fov_pairs(const FovArgs& a, int64_t m, cudaStream_t stream);
 int launch_fov_gather(const FovArgs& a, int64_t m, double* gpos, double* gvel, double* gjd0,
                       double* gjd1, cudaStream_t stream);
 int launch_fov_contains(int64_t n_vec, const double* vec, int64_t n_fov, const double* fov,

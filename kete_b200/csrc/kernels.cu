@@ -590,6 +590,18 @@ int launch_fov_prefilter(const FovArgs& a, cudaStream_t stream) {
     return launched(1, "fov_prefilter_kernel launch");
 }
 
+int launch_fov_screen(const FovArgs& a, cudaStream_t stream) {
+    if (a.n_obj <= 0 || a.n_fov <= 0) return 0;
+    fov_screen_kernel<<<(unsigned)((a.n_obj + 127) / 128), 128, 0, stream>>>(a);
+    return launched(1, "fov_screen_kernel launch");
+}
+
+int launch_fov_pairs(const FovArgs& a, int64_t m, cudaStream_t stream) {
+    if (m <= 0) return 0;
+    fov_pairs_kernel<<<(unsigned)((m + 127) / 128), 128, 0, stream>>>(a, m);
+    return launched(1, "fov_pairs_kernel launch");
+}
+
 int launch_fov_gather(const FovArgs& a, int64_t m, double* gpos, double* gvel, double* gjd0,
                       double* gjd1, cudaStream_t stream) {
     if (m <= 0) return 0;

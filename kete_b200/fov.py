@@ -19,6 +19,7 @@ from __future__ import annotations
 
 import ctypes
 import math
+import time
 
 import numpy as np
 
@@ -345,6 +346,15 @@ def _bind():
     return L
 
 
+def set_fov_form(form: int = 0):
+    """Form of the field checks (kete_b200_set_fov_form): 0 = linear screen of every (object,
+    field) pair, then the two-body solve on the pairs that pass (default); 1 = one fused
+    pass.  Same results."""
+    L = _lib.lib()
+    L.kete_b200_set_fov_form.argtypes = [ctypes.c_int]
+    _lib.check(L.kete_b200_set_fov_form(int(form)))
+
+
 def fov_check_visible_arrays(pos, vel, jd, valid, fov_table, dt_limit=3.0,
                              include_asteroids=False, capacity=None):
     """Visibility of n objects (SoA (3, n) at epochs jd (n,), valid (n,) uint8 or None) in
@@ -399,7 +409,7 @@ def chunk_bounds(jds, dt_limit):
 
 
 def fov_state_check_arrays(pos, vel, jd, fov_table, dt_limit=3.0, include_asteroids=False,
-                           nongrav=None, on_chunk=None):
+                           nongrav=None, on_chunk=None, stage_times=None):
     """The fov_state_check schedule (src/kete/rust/fovs/checks.rs:24-110) on device arrays.
 
     pos/vel (3, n) heliocentric ecliptic torch CUDA tensors at the common epoch ``jd``;
@@ -408,7 +418,10 @@ def fov_state_check_arrays(pos, vel, jd, fov_table, dt_limit=3.0, include_astero
     chunk's mean epoch, re-seeded from a big-step copy every 25-50 dt_limit as the
     reference does; objects whose propagation fails are dropped from then on.  Returns
     (fov_index, obj_index, state7) numpy arrays over all fields, sorted by field then
-    object.  ``on_chunk(k0, k1)``, when given, is called after each chunk."""
+    object.  ``on_chunk(k0, k1)``, when given, is called after each chunk.  ``stage_times``,
+    when given (a dict), accumulates the seconds spent in the N-body re-propagations
+    ("propagate") and in the field checks ("check"), each measured with the device
+    synchronized on both sides."""
     import torch
 
     n = int(pos.shape[1])
@@ -427,12 +440,25 @@ def fov_state_check_arrays(pos, vel, jd, fov_table, dt_limit=3.0, include_astero
             return Pop(self.P.clone(), self.V.clone(), self.ok.clone(), self.t)
 
         def propagate(self, target):
+            t_start = _stage_start()
             jd0 = torch.full((n,), self.t, dtype=torch.float64, device=dev)
             jd1 = torch.full((n,), target, dtype=torch.float64, device=dev)
             P, V, st = propagate_n_body_arrays(self.P, self.V, jd0, jd1, Frames.Ecliptic, 10,
                                                include_asteroids, nongrav)
             self.P, self.V, self.t = P, V, target
             self.ok = self.ok & (st == 0)
+            _stage_end("propagate", t_start)
+
+    def _stage_start():
+        if stage_times is None:
+            return 0.0
+        torch.cuda.synchronize(dev)
+        return time.perf_counter()
+
+    def _stage_end(name, t_start):
+        if stage_times is not None:
+            torch.cuda.synchronize(dev)
+            stage_times[name] = stage_times.get(name, 0.0) + time.perf_counter() - t_start
 
     cur_jd = float(jd)
     big_jd = cur_jd
@@ -450,10 +476,12 @@ def fov_state_check_arrays(pos, vel, jd, fov_table, dt_limit=3.0, include_astero
                 cur = big.copy()
             cur_jd = jd_mean
             cur.propagate(cur_jd)
+        t_start = _stage_start()
         epochs = torch.full((n,), cur.t, dtype=torch.float64, device=dev)
         ff, oo, ss = fov_check_visible_arrays(cur.P, cur.V, epochs, cur.ok.to(torch.uint8),
                                               table[:, k0:k1].contiguous(), dt_limit,
                                               include_asteroids)
+        _stage_end("check", t_start)
         out_f.append(ff + k0)
         out_o.append(oo)
         out_s.append(ss)

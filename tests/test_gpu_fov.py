@@ -60,8 +60,17 @@ def _oracle_check(oracle_spk, fov, pos, vel, jd, dt_limit):
     return flags, out7
 
 
+@pytest.fixture(params=[0, 1], ids=["two_pass", "fused"])
+def fov_form(request, gpu):
+    """Both forms of the field check: linear screen then two-body pairs (default), and the
+    fused one-pass kernel."""
+    gpu.fov.set_fov_form(request.param)
+    yield request.param
+    gpu.fov.set_fov_form(0)
+
+
 @pytest.mark.parametrize("offset_days", [0.5, 4.0])
-def test_check_visible_vs_oracle(gpu, oracle_spk, offset_days):
+def test_check_visible_vs_oracle(gpu, oracle_spk, offset_days, fov_form):
     """Linear branch (|dt| < dt_limit) and n-body branch (|dt| >= dt_limit)."""
     n = 4000
     pos, vel = _population(n, 11)
@@ -150,3 +159,24 @@ def test_fov_state_check_schedule_vs_oracle(gpu, oracle_spk):
     assert n_fields >= 5
     assert reseeds >= 1 and resets >= 1, (reseeds, resets)
     assert len(res) == sum(1 for f in fovs if id(f) in got)
+
+
+def test_fov_forms_identical(gpu, oracle_spk):
+    """The two-pass and fused field checks run the same arithmetic on the same pairs: the
+    visible pairs and their states are identical."""
+    n = 20000
+    pos, vel = _population(n, 31)
+    jd_obj = np.full(n, EPOCH)
+    fovs = _fields(gpu, oracle_spk, pos, EPOCH + 0.3 + np.linspace(0, 2.0, 40), 32, width=3.0)
+    table = np.stack([f.ecliptic_column() for f in fovs], axis=1)
+    out = {}
+    try:
+        for form in (0, 1):
+            gpu.fov.set_fov_form(form)
+            out[form] = gpu.fov.fov_check_visible_arrays(pos, vel, jd_obj, None, table, 3.0)
+    finally:
+        gpu.fov.set_fov_form(0)
+    (f0, o0, s0), (f1, o1, s1) = out[0], out[1]
+    assert len(o0) > 20
+    assert np.array_equal(f0, f1) and np.array_equal(o0, o1)
+    assert np.array_equal(s0, s1)
