@@ -78,7 +78,14 @@ def flop_models(steps, iters, exact):
 
 # DRAM traffic of the node kernel from ncu captures (dram__bytes_read.sum +
 # dram__bytes_write.sum, one launch), per object, keyed by workload and launch configuration
-NODE_TRAFFIC = {}
+NODE_TRAFFIC = {
+    ("nbody_mixed_1m", 7, 1): {"bytes_per_object": (13_601_536 + 882_944) / 100_000,
+                               "fp64_pipe": 0.217,
+                               "captured": "one launch on a 100,000-object sample of the workload"},
+    ("nbody_mixed_1m", 9, 1): {"bytes_per_object": (13_523_968 + 951_296) / 100_000,
+                               "fp64_pipe": 0.241,
+                               "captured": "one launch on a 100,000-object sample of the workload"},
+}
 
 CLOSE_AU = 0.01  # objects whose closest planet approach is below this are reported apart
 
