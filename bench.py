@@ -140,6 +140,8 @@ DEFAULT_N["stm_cov_1m"] = 1_000_000
 # bytes each object moves: pos, vel, jd0, jd1, covariance in (8 x 44); pos, vel, STM,
 # covariance, status out (8 x 78 + 4)
 STM_BYTES_PER_OBJECT = 8 * 44 + 8 * 78 + 4
+WORKLOADS["adjoint_4k"] = ADJ_WORKLOAD
+DEFAULT_N["adjoint_4k"] = ADJ_N
 SPK21_ID = 20000042
 SURVEY_FIELDS, SURVEY_DT_LIMIT = 2000, 3.0
 
@@ -657,6 +659,11 @@ def run_gpu(args, world, rank, local):
     op, st_cpu, cpu_dt, cores = cpu_baseline(kind, pos[:, idx], vel[:, idx], jd0[idx], jd1[idx],
                                              None if ng is None else ng[:, idx], spk_bytes)
     cpu_units, _, _ = units_of(kind, jd0[idx], jd1[idx])
+    # the same oracle on one thread, over every tenth object of the sample
+    i1 = idx[::10]
+    _, _, cpu1_dt, _ = cpu_baseline(kind, pos[:, i1], vel[:, i1], jd0[i1], jd1[i1],
+                                    None if ng is None else ng[:, i1], spk_bytes, threads=1)
+    cpu1_units, _, _ = units_of(kind, jd0[i1], jd1[i1])
     gp = out[0][:, idx]
     gst = (out[2] if nbody else out[3])[idx]
     err = np.linalg.norm(gp - op, axis=0)
@@ -703,7 +710,10 @@ def run_gpu(args, world, rank, local):
                                     f"seeded 1% subsample ({len(idx)} objects, every 100th), "
                                     "rate per object-year") +
                                    ", oracle (C restatement of kete's FP64 path) with OpenMP on "
-                                   "all host cores"},
+                                   "all host cores",
+                         "one_thread": {"value": cpu1_units / cpu1_dt, "unit": unit, "cores": 1,
+                                        "sample": f"every tenth object of that sample "
+                                                  f"({len(i1)} objects)"}},
         "e2e": {"value": e2e_value, "unit": unit, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": args.steps * launches_per_step,
@@ -717,6 +727,38 @@ def run_gpu(args, world, rank, local):
         line["corrector_iterations_per_step"] = iters_total / max(steps_total, 1)
     if kind in ("nbody_mba_10k", "nbody_mixed_1m") and not args.no_adjoint:
         line["adjoint"] = adjoint_section(dev, max(1, args.warmup), max(1, min(args.steps, 3)))
+    print(json.dumps(line), flush=True)
+
+
+def run_adjoint(args, world, rank, local):
+    """The differentiation workload on its own: forward pass, checkpointed forward, adjoint
+    and forward sensitivities (the gradient-cost section of the default line)."""
+    import torch
+
+    import kete_b200
+    from kete_b200 import build, synthetic
+
+    build.build()
+    torch.cuda.set_device(local)
+    kete_b200.init(local)
+    td = tempfile.mkdtemp(prefix="kete_b200_bench_")
+    kete_b200.spice.kernel_reload([synthetic.write_synthetic_spk(os.path.join(td, "syn.bsp"))])
+    dev = torch.device("cuda", local)
+    sec = adjoint_section(dev, max(1, args.warmup), max(1, min(args.steps, 3)))
+    if rank != 0:
+        return
+    years = ADJ_N * ADJ_SPAN / 365.25
+    line = {
+        "metric": "reverse-mode gradient object-years/s (checkpointed forward + adjoint)",
+        "value": world * years / ((sec["checkpointed_forward_ms"] + sec["adjoint_ms"]) * 1e-3),
+        "unit": "object-years/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": sec["checkpointed_forward_ms"] + sec["adjoint_ms"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": ADJ_WORKLOAD, "n_objects": ADJ_N,
+                   "l2": "inputs resident; consecutive passes share the ephemeris in L2"},
+        "adjoint": sec,
+    }
     print(json.dumps(line), flush=True)
 
 
@@ -1608,6 +1650,8 @@ def main():
         run_thermal(args, world, rank, local)
     elif args.workload == "stm_cov_1m":
         run_stm(args, world, rank, local)
+    elif args.workload == "adjoint_4k":
+        run_adjoint(args, world, rank, local)
     else:
         run_gpu(args, world, rank, local)
         if world > 1:
