@@ -418,6 +418,70 @@ def run_reference_long(args):
     print(json.dumps(line), flush=True)
 
 
+def run_reference_adjoint(args):
+    """The gradient on the CPU oracle as kete offers it: the forward chain over the epochs
+    plus central differences in the 8 parameters (16 perturbed chains), on all host cores,
+    for a seeded sample of the differentiation workload's objects."""
+    from kete_b200 import synthetic
+    from oracle import oracle as O
+
+    pos, vel, ng, _, _, epochs, _ = adjoint_population(ADJ_N)
+    k = 64
+    sp, sv, sg = pos[:, :k].copy(), vel[:, :k].copy(), ng[:, :k].copy()
+    with tempfile.TemporaryDirectory() as td:
+        spk = synthetic.write_synthetic_spk(os.path.join(td, "syn.bsp"))
+        O.spk_reset()
+        O.spk_load_bytes(open(spk, "rb").read())
+
+    def chain(p, v, g):
+        t, m = EPOCH, p.shape[1]
+        for e in epochs:
+            p, v, _, _, _ = O.propagate_n_body(p, v, np.full(m, t), np.full(m, e), ng=g)
+            t = e
+        return p
+
+    steps = [1e-4] * 3 + [1e-6] * 3 + [5e-8, 5e-9]
+
+    def gradient():
+        chain(sp, sv, sg)
+        for q, d in enumerate(steps):
+            for s in (d, -d):
+                p, v, g = sp.copy(), sv.copy(), sg.copy()
+                if q < 3:
+                    p[q] += s
+                elif q < 6:
+                    v[q - 3] += s
+                else:
+                    g[q - 5] += s
+                chain(p, v, g)
+
+    for _ in range(args.warmup):
+        chain(sp[:, :4].copy(), sv[:, :4].copy(), sg[:, :4].copy())
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        gradient()
+    total = time.perf_counter() - t
+    value = k * ADJ_SPAN / 365.25 * args.steps / total
+    line = {
+        "impl": "reference",
+        "metric": "reverse-mode gradient object-years/s (checkpointed forward + adjoint)",
+        "value": value, "unit": "object-years/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": ADJ_WORKLOAD, "n_objects": ADJ_N,
+                   "l2": "inputs resident; consecutive passes share the ephemeris in L2"},
+        "cpu_baseline": {"value": value, "unit": "object-years/s", "cores": os.cpu_count(),
+                         "kind": "port",
+                         "sample": f"the first {k} objects per step: the forward chain and 16 "
+                                   "perturbed chains (central differences in the 8 "
+                                   "parameters), oracle on all host cores"},
+        "e2e": {"value": value, "unit": "object-years/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return
@@ -433,6 +497,8 @@ def run_reference(args, world, rank):
         return run_reference_thermal(args)
     if args.workload == "stm_cov_1m":
         return run_reference_stm(args)
+    if args.workload == "adjoint_4k":
+        return run_reference_adjoint(args)
     kind = args.workload
     n = args.n or DEFAULT_N[kind]
     pos, vel, jd0, jd1, ng = workload(n, kind=kind)
