@@ -225,6 +225,8 @@ __device__ __forceinline__ void sens_rounds(SensGroup& G, SpkForce& F, Policy& P
         const double ratio = fmax(fmax(fabs(b60 - b6_old0) / fem0, fabs(b61 - b6_old1) / fem1),
                                   fabs(b62 - b6_old2) / fem2);
         ++G.iter;
+        // the policy sees the points of an attempt's last iteration (converged or not)
+        if (ratio < 1e-14 || G.iter >= 10) P.last_iteration(G, te, xe, ve, lane);
         if (ratio < 1e-14) {
             const double h2 = G.h * G.h;
 #pragma unroll
@@ -313,6 +315,7 @@ struct SensForwardPolicy {
     }
     __device__ void attempt_predict(double) {}
     __device__ void iter_round(SensGroup&, double*, int) {}
+    __device__ void last_iteration(SensGroup&, double, const double*, const double*, int) {}
     __device__ void end_attempt(SensGroup&, bool) {}
     __device__ void segment_end(SensGroup& G) {
         const int64_t n = a->n;
@@ -439,6 +442,7 @@ struct SensReplayPolicy {
     __device__ void attempt_predict(double q) {
         if (lane == 0) rec[(size_t)(na - 1) * SENS_STRIDE + 34] = q;
     }
+    __device__ void last_iteration(SensGroup&, double, const double*, const double*, int) {}
     __device__ void iter_round(SensGroup&, double* b, int ln) {  // b of the previous iterate
         double* d = rec + (size_t)(na - 1) * SENS_STRIDE;
         if (ln < 7) {

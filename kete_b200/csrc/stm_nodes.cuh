@@ -15,7 +15,8 @@
 // where J_j (3 x 6) and jp_j (3 x 2) are the Jacobians of the force (dual numbers,
 // tangent.cuh) at node j's point of the attempt's last corrector iteration, for all M
 // iterations (the corrector has converged there to 1e-14 of |a| in b6), as the discrete
-// adjoint takes them; J' is taken at the accepted state.  Lane j < 7 owns node j + 1 and its
+// adjoint takes them -- evaluated in that iteration's round, while the lane's body cache
+// holds the node's time; J' is taken at the accepted state.  Lane j < 7 owns node j + 1 and its
 // Jacobian; lane p updates direction p of db and of the state tangents; all tangents of a
 // group live in shared memory.  The one-object-per-thread form (nbody_stm_kernel) takes every
 // iteration's Jacobian at that iteration's own points; the two agree to about 1e-8 relative.
@@ -32,10 +33,8 @@ namespace kb {
 constexpr int STM_BLOCK = SENS_BLOCK;   // 16 groups of 8 lanes
 constexpr int STM_GROUPS = STM_BLOCK / SG;
 // Tangent doubles per group in dynamic shared memory: dx, dv, da (3 x 8 each), db (3 x 8
-// rows of 7 coefficients), the node tangents dE (7 x 3 x 8), the attempt's start state
-// (x, v, a, t) and the b of its previous-to-last corrector iteration.
-constexpr int STM_DX = 0, STM_DV = 24, STM_DA = 48, STM_DB = 72, STM_DE = 240, STM_X0 = 408,
-              STM_T0 = 417, STM_BPREV = 418, STM_ROW = 439;
+// rows of 7 coefficients) and the node tangents dE (7 x 3 x 8).
+constexpr int STM_DX = 0, STM_DV = 24, STM_DA = 48, STM_DB = 72, STM_DE = 240, STM_ROW = 408;
 constexpr int STM_DYN_SMEM = STM_GROUPS * STM_ROW * (int)sizeof(double);
 
 struct StmNodesPolicy {
@@ -88,12 +87,6 @@ struct StmNodesPolicy {
             }
             tangent_acc(J, jp);
         }
-        if (lane < 3) {  // the attempt's start state
-            ts[STM_X0 + lane] = G.x[lane == 0 ? 0 : (lane == 1 ? 1 : 2)];
-            ts[STM_X0 + 3 + lane] = G.v[lane == 0 ? 0 : (lane == 1 ? 1 : 2)];
-            ts[STM_X0 + 6 + lane] = G.acc[lane == 0 ? 0 : (lane == 1 ? 1 : 2)];
-        }
-        if (lane == 3) ts[STM_T0] = G.t;
         __syncwarp(gmask);
         return true;
     }
@@ -106,40 +99,30 @@ struct StmNodesPolicy {
         __syncwarp(gmask);
     }
 
-    __device__ void iter_round(SensGroup&, double* b, int ln) {  // b of the previous iterate
-        if (ln < 7) {
-            ts[STM_BPREV + ln] = b[ln];
-            ts[STM_BPREV + 7 + ln] = b[7 + ln];
-            ts[STM_BPREV + 14 + ln] = b[14 + ln];
-        }
+    __device__ void iter_round(SensGroup&, double*, int) {}
+
+    // node j's Jacobian at its point of the attempt's last corrector iteration, while the
+    // lane's body cache still holds the node's time (kept in registers until end_attempt)
+    double Jl[18], jpl[6];
+    bool jl_ok;
+    __device__ void last_iteration(SensGroup&, double te, const double* xe, const double* ve,
+                                   int ln) {
+        jl_ok = true;
+        if (ln < 7) jl_ok = jacobian(te, xe, ve, Jl, jpl);
     }
 
     __device__ void end_attempt(SensGroup& G, bool converged) {
         __syncwarp(gmask);
         const double h = G.h, h2 = h * h;
-        // node Jacobians at the last corrector iteration's points (lanes 0-6) and, after an
-        // accepted step, the Jacobian at the new state (lane 7) in the same round
+        // node Jacobians at the last corrector iteration's points (lanes 0-6, taken in that
+        // round) and, after an accepted step, the Jacobian at the new state (lane 7)
         double J[18], jp[6];
-        bool ok = true;
+#pragma unroll
+        for (int i = 0; i < 18; ++i) J[i] = Jl[i];
+#pragma unroll
+        for (int i = 0; i < 6; ++i) jp[i] = jpl[i];
+        bool ok = jl_ok;
         if (lane == 7 && converged) ok = jacobian(G.t, G.x, G.v, J, jp);
-        if (lane < 7) {
-            const double f = nrow[14], frac2 = nrow[15];
-            double xe[3], ve[3];
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                double bw = 0.0, bu = 0.0;
-#pragma unroll
-                for (int kk = 0; kk < 7; ++kk) {
-                    const double bck = ts[STM_BPREV + 7 * c + kk];
-                    bw += nrow[kk] * bck;
-                    bu += nrow[7 + kk] * bck;
-                }
-                const double x0 = ts[STM_X0 + c], v0 = ts[STM_X0 + 3 + c], a0 = ts[STM_X0 + 6 + c];
-                xe[c] = x0 + f * v0 * h + frac2 * h2 * (a0 / 2.0 + bw);
-                ve[c] = v0 + f * h * (a0 + bu);
-            }
-            ok = jacobian(ts[STM_T0] + f * h, xe, ve, J, jp);  // the node's time, as evaluated
-        }
         if (!__all_sync(gmask, ok)) {
             G.rc = ST_DAF_LIMITS;
             G.phase = SP_DONE;
@@ -353,6 +336,7 @@ __global__ void __launch_bounds__(STM_BLOCK, MINB) nbody_stm_nodes_kernel(StmArg
     P.nrow = nrow;
     P.T = &T;
     P.C = &C;
+    P.jl_ok = true;
     sens_rotation(a.frame, P.R);
     {  // tangents of the initial state: d(equatorial state) / d(caller's state), A1, A2
         const int p = lane;

@@ -104,10 +104,11 @@ def test_close_approaches_reported_apart(gpu, oracle_spk):
     n = 400
     rng = np.random.default_rng(123)
     earth = np.stack([oracle_spk.spk_get_state(399, EPOCH + 30.0, 10, 2)[1]])[0]
-    # start 30 days before the encounter on the Earth's track, offset by 0.002-0.05 AU, with
-    # a relative velocity of ~0.01 AU/day: the straight-line approach passes near the Earth
-    rel_v = rng.normal(0.0, 0.01, (3, n))
-    miss = rng.uniform(0.002, 0.05, n) * rng.choice([-1.0, 1.0], n)
+    # start 30 days before the encounter on the Earth's track, offset by 0.001-0.03 AU, with
+    # a relative velocity of ~0.003 AU/day: the slow straight-line approach passes near the
+    # Earth and stays close for days, so the accepted steps sample the closest approach
+    rel_v = rng.normal(0.0, 0.003, (3, n))
+    miss = rng.uniform(0.001, 0.03, n) * rng.choice([-1.0, 1.0], n)
     p30 = earth[:3, None] + np.array([[1.0], [0.0], [0.0]]) * miss
     pos = p30 - 30.0 * (earth[3:, None] + rel_v)
     vel = earth[3:, None] + rel_v
@@ -116,7 +117,7 @@ def test_close_approaches_reported_apart(gpu, oracle_spk):
     op, ov, ost, _, _ = oracle_spk.propagate_n_body(pos, vel, jd0, jd1)
     p, v, st, det = gpu.propagate_n_body_arrays(pos, vel, jd0, jd1, with_details=True)
     close = det["min_dist"] < 0.01
-    assert close.sum() >= 20 and (~close).sum() >= 20
+    assert close.sum() >= 10 and (~close).sum() >= 10
     assert np.array_equal(st, ost)
     ok = (st == 0) & (ost == 0)
     err = np.linalg.norm(p - op, axis=0)
