@@ -35,7 +35,7 @@
 namespace kb {
 
 constexpr int SENS_BLOCK = 128;
-constexpr int SG = SENS_GROUP;  // lanes per object
+constexpr int SG = 8;  // lanes per object
 
 enum SensPhase : int { SP_BEGIN = 0, SP_EXACT_INIT = 1, SP_ITER = 2, SP_EXACT_STEP = 3, SP_PAUSE = 4, SP_DONE = 5 };
 
@@ -292,26 +292,6 @@ __device__ __forceinline__ void sens_rotation(int frame, double R[3][3]) {
     }
 }
 
-// Jacobian of the force at one point (dual numbers): J (3 x 6) = d a / d(x, v) and
-// jp (3 x 2) = d a / d(A1, A2).  Out of line: one copy serves every call site.
-static __device__ __noinline__ int sens_jacobian(TangentForce& T, double t, const double* x,
-                                          const double* v, double* J, double* jp, EphCache& C) {
-    double xx[3] = {x[0], x[1], x[2]}, vv[3] = {v[0], v[1], v[2]};
-    double ev[3], JJ[3][6], jj[3][2];
-    const FastPlan& plan = T.n_force == c_eph.n_force_planets ? c_eph.fast_planets : c_eph.fast_all;
-    const int rc = (C.on && t >= plan.lo && t <= plan.hi)
-                       ? T.eval_cached(plan, C, t, xx, vv, ev, JJ, jj)
-                       : T.eval(false, t, xx, vv, ev, JJ, jj);
-#pragma unroll
-    for (int r = 0; r < 3; ++r) {
-#pragma unroll
-        for (int c = 0; c < 6; ++c) J[6 * r + c] = JJ[r][c];
-        jp[2 * r] = jj[r][0];
-        jp[2 * r + 1] = jj[r][1];
-    }
-    return rc;
-}
-
 // ---------------------------------------------------------------------------------------
 // forward with checkpoints
 // ---------------------------------------------------------------------------------------
@@ -452,23 +432,6 @@ struct SensReplayPolicy {
     int na;       // attempts recorded
     int lane;
     double* sb;
-    // the force Jacobians of every recorded attempt (SENS_JAC doubles per lane): lane j < 7
-    // at node j + 1's point of the attempt's last corrector iteration, taken in that round
-    // while the lane's body cache holds the node's time; lane 7 at the accepted state
-    double* jac;
-    TangentForce* T;
-    EphCache* C;
-
-    __device__ void store_jacobian(double t, const double* x, const double* v) {
-        double J[18], jp[6];
-        const int rc = sens_jacobian(*T, t, x, v, J, jp, *C);
-        double* d = jac + ((size_t)(na - 1) * SG + lane) * SENS_JAC;
-#pragma unroll
-        for (int i = 0; i < 18; ++i) d[i] = J[i];
-#pragma unroll
-        for (int i = 0; i < 6; ++i) d[18 + i] = jp[i];
-        d[24] = (double)rc;
-    }
 
     __device__ bool begin_attempt(SensGroup& G) {
         sens_store_state(rec + (size_t)na * SENS_STRIDE, G, sb, lane, 0.0);
@@ -479,10 +442,7 @@ struct SensReplayPolicy {
     __device__ void attempt_predict(double q) {
         if (lane == 0) rec[(size_t)(na - 1) * SENS_STRIDE + 34] = q;
     }
-    __device__ void last_iteration(SensGroup&, double te, const double* xe, const double* ve,
-                                   int ln) {
-        if (ln < 7) store_jacobian(te, xe, ve);
-    }
+    __device__ void last_iteration(SensGroup&, double, const double*, const double*, int) {}
     __device__ void iter_round(SensGroup&, double* b, int ln) {  // b of the previous iterate
         double* d = rec + (size_t)(na - 1) * SENS_STRIDE;
         if (ln < 7) {
@@ -498,14 +458,32 @@ struct SensReplayPolicy {
             d[2] = (double)G.iter;
             d[3] = converged ? 1.0 : 0.0;
         }
-        // a' = F(x', v'): the cache holds the accepted epoch after the exact evaluation
-        if (lane == 7 && converged) store_jacobian(G.t, G.x, G.v);
     }
     __device__ void segment_end(SensGroup& G) {
         sens_store_state(rec + (size_t)na * SENS_STRIDE, G, sb, lane, 0.0);
         G.phase = SP_PAUSE;
     }
 };
+
+// Jacobian of the force at one point (dual numbers): J (3 x 6) = d a / d(x, v) and
+// jp (3 x 2) = d a / d(A1, A2).  Out of line: one copy serves every call site.
+static __device__ __noinline__ int sens_jacobian(TangentForce& T, double t, const double* x,
+                                          const double* v, double* J, double* jp, EphCache& C) {
+    double xx[3] = {x[0], x[1], x[2]}, vv[3] = {v[0], v[1], v[2]};
+    double ev[3], JJ[3][6], jj[3][2];
+    const FastPlan& plan = T.n_force == c_eph.n_force_planets ? c_eph.fast_planets : c_eph.fast_all;
+    const int rc = (C.on && t >= plan.lo && t <= plan.hi)
+                       ? T.eval_cached(plan, C, t, xx, vv, ev, JJ, jj)
+                       : T.eval(false, t, xx, vv, ev, JJ, jj);
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+#pragma unroll
+        for (int c = 0; c < 6; ++c) J[6 * r + c] = JJ[r][c];
+        jp[2 * r] = jj[r][0];
+        jp[2 * r + 1] = jj[r][1];
+    }
+    return rc;
+}
 
 template <int MINB>
 __global__ void __launch_bounds__(SENS_BLOCK, MINB) nbody_sens_backward_kernel(SensArgs a) {
@@ -536,7 +514,6 @@ __global__ void __launch_bounds__(SENS_BLOCK, MINB) nbody_sens_backward_kernel(S
     const int comp = lane % 3;
     const double* nrow = s_node + (lane < 7 ? lane + 1 : 7) * NODE_ROW_S;
     double* rec = a.rec + (size_t)obj * (SENS_CK_ATTEMPTS + 1) * SENS_STRIDE;
-    double* jac = a.jac + (size_t)obj * SENS_CK_ATTEMPTS * SG * SENS_JAC;
     const double* ck = a.ckpt + (size_t)obj * a.ckpt_cap * SENS_STRIDE;
 
     SpkForce F;
@@ -619,7 +596,7 @@ __global__ void __launch_bounds__(SENS_BLOCK, MINB) nbody_sens_backward_kernel(S
             }
             __syncwarp(gmask);
             G.phase = SP_BEGIN;
-            SensReplayPolicy P{rec, 0, lane, sb, jac, &T, &C};
+            SensReplayPolicy P{rec, 0, lane, sb};
             sens_rounds(G, F, P, nrow, sb, se, lane, comp, gmask, warp_lane, max_rounds, C);
             if (G.phase != SP_PAUSE) {
                 fail = G.rc != ST_OK ? G.rc : ST_TIMEOUT;
@@ -629,18 +606,36 @@ __global__ void __launch_bounds__(SENS_BLOCK, MINB) nbody_sens_backward_kernel(S
             // ---- transpose the attempts, last first ----
             for (int s = P.na - 1; s >= 0; --s) {
                 const double* r0 = rec + (size_t)s * SENS_STRIDE;
-                const double h = r0[1];
+                const double* r1 = r0 + SENS_STRIDE;
+                const double t0 = r0[0], h = r0[1];
                 const int M = (int)r0[2];
                 const bool conv = r0[3] != 0.0;
-                // the force Jacobians recorded by the replay (lane j < 7: node j + 1 at the
-                // last corrector iteration's point; lane 7: the accepted state)
+                double te, xe[3], ve[3];
+                if (lane < 7) {
+                    const double f = nrow[14], frac2 = nrow[15], h2 = h * h;
+#pragma unroll
+                    for (int q = 0; q < 3; ++q) {
+                        double bw = 0.0, bu = 0.0;
+#pragma unroll
+                        for (int kk = 0; kk < 7; ++kk) {
+                            const double bck = r0[13 + 7 * q + kk];
+                            bw += nrow[kk] * bck;
+                            bu += nrow[7 + kk] * bck;
+                        }
+                        xe[q] = r0[4 + q] + f * r0[7 + q] * h + frac2 * h2 * (r0[10 + q] / 2.0 + bw);
+                        ve[q] = r0[7 + q] + f * h * (r0[10 + q] + bu);
+                    }
+                    te = t0 + f * h;
+                } else {  // the step end x', v' (meaningful when the attempt converged)
+                    te = r1[0];
+#pragma unroll
+                    for (int q = 0; q < 3; ++q) {
+                        xe[q] = r1[4 + q];
+                        ve[q] = r1[7 + q];
+                    }
+                }
                 double J[18], jp[6];
-                const double* jd = jac + ((size_t)s * SG + lane) * SENS_JAC;
-#pragma unroll
-                for (int i = 0; i < 18; ++i) J[i] = jd[i];
-#pragma unroll
-                for (int i = 0; i < 6; ++i) jp[i] = jd[18 + i];
-                const int jrc = (int)jd[24];
+                const int jrc = sens_jacobian(T, te, xe, ve, J, jp, C);
                 const unsigned bad = __ballot_sync(gmask, jrc != ST_OK && (lane < 7 || conv));
                 if (bad) {
                     fail = ST_DAF_LIMITS;

@@ -1312,10 +1312,6 @@ int kete_b200_propagate_n_body_adjoint(int64_t n, int n_epochs, const double* ep
     if ((rc = staging(*ds, 33, (size_t)n * (SENS_CK_ATTEMPTS + 1) * SENS_STRIDE * sizeof(double), &rec)))
         return rc;
     a.rec = (double*)rec;
-    void* jac;
-    if ((rc = staging(*ds, 34, (size_t)n * SENS_CK_ATTEMPTS * SENS_GROUP * SENS_JAC * sizeof(double), &jac)))
-        return rc;
-    a.jac = (double*)jac;
     if ((rc = launch_sens_backward(a, st))) return rc;
     return S.finish();
 }

@@ -132,8 +132,6 @@ int launch_nbody_stm(const StmArgs& a, int form, cudaStream_t stream);
 // reverse-mode gradients: checkpointed forward pass and adjoint pass (adjoint.cuh)
 constexpr int SENS_STRIDE = 36;       // doubles per checkpoint / attempt record
 constexpr int SENS_CK_ATTEMPTS = 16;  // step attempts between checkpoints
-constexpr int SENS_JAC = 25;          // doubles per lane and attempt: J (18), jp (6), status
-constexpr int SENS_GROUP = 8;         // lanes per object in the sensitivity kernels
 struct SensArgs {
     int64_t n;
     const double* pos;  // 3 x n (forward)
@@ -155,8 +153,6 @@ struct SensArgs {
     double* out_grad;    // 8 x n: dL/d(pos0, vel0, A1, A2) (adjoint)
     int32_t* grad_status;  // n or null (adjoint)
     double* rec;         // n x (SENS_CK_ATTEMPTS + 1) x SENS_STRIDE scratch (adjoint)
-    double* jac;         // n x SENS_CK_ATTEMPTS x 8 x SENS_JAC scratch (adjoint): the force
-                         // Jacobians of each replayed attempt's nodes and step end
     int max_loops;
 };
 int launch_sens_forward(const SensArgs& a, cudaStream_t stream);
