@@ -37,6 +37,17 @@ int launch_sens_backward(const SensArgs& a, cudaStream_t stream) {
             return rc;
         opted[dev] = true;
     }
+    if (a.rec_all) {  // every block's replay first, one group per (object, block)
+        if ((rc = cuda_check(cudaFuncSetAttribute(nbody_sens_replay_kernel<1>,
+                                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                  cache_bytes),
+                             "cudaFuncSetAttribute")))
+            return rc;
+        const int64_t rthreads = a.n * (int64_t)a.ckpt_cap * SG;
+        nbody_sens_replay_kernel<1><<<(unsigned)((rthreads + SENS_BLOCK - 1) / SENS_BLOCK),
+                                      SENS_BLOCK, cache_bytes, stream>>>(a);
+        if ((rc = launched(1, "nbody_sens_replay_kernel launch"))) return rc;
+    }
     nbody_sens_backward_kernel<1><<<(unsigned)((threads + SENS_BLOCK - 1) / SENS_BLOCK), SENS_BLOCK, cache_bytes, stream>>>(a);
     return launched(1, "nbody_sens_backward_kernel launch");
 }

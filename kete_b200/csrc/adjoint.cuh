@@ -485,6 +485,92 @@ static __device__ __noinline__ int sens_jacobian(TangentForce& T, double t, cons
     return rc;
 }
 
+// Re-run checkpoint block `c` (its segment ends at tf) with the step code, recording every
+// attempt into rec (SENS_CK_ATTEMPTS + 1 records).  Returns ST_OK with the attempt count in na,
+// or the failure.
+__device__ __forceinline__ int sens_replay_block(const double* c, double tf, double* rec,
+                                                 SpkForce& F, const double* nrow, double* sb,
+                                                 double* se, int lane, int comp, unsigned gmask,
+                                                 int warp_lane, int max_rounds, EphCache& C,
+                                                 int& na) {
+    SensGroup G;
+    G.t = c[0];
+    G.h = c[1];
+    G.failures = (int)c[2];
+    G.tf = tf;
+    G.next_h = 0.0;
+    G.h_prev = c[34];
+    G.predict = c[34] != 0.0;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        G.x[q] = c[4 + q];
+        G.v[q] = c[7 + q];
+        G.acc[q] = c[10 + q];
+    }
+    G.iter = 0;
+    G.att = 0;
+    G.rc = ST_OK;
+    if (lane < 7) {
+        sb[lane] = c[13 + lane];
+        sb[7 + lane] = c[20 + lane];
+        sb[14 + lane] = c[27 + lane];
+    }
+    __syncwarp(gmask);
+    G.phase = SP_BEGIN;
+    SensReplayPolicy P{rec, 0, lane, sb};
+    sens_rounds(G, F, P, nrow, sb, se, lane, comp, gmask, warp_lane, max_rounds, C);
+    na = P.na;
+    __syncwarp(gmask);  // the records are complete and visible to the group
+    if (G.phase != SP_PAUSE) return G.rc != ST_OK ? G.rc : ST_TIMEOUT;
+    return ST_OK;
+}
+
+// The replays of every checkpoint block of every object at once, before the adjoint sweep:
+// a block's replay depends only on its checkpoint, so one group of 8 lanes per (object,
+// block) re-runs it in parallel and stores its attempt records (a.rec_all) and outcome
+// (a.rep_count: the attempt count, or -1 - status on failure) for the sweep to read.
+template <int MINB>
+__global__ void __launch_bounds__(SENS_BLOCK, MINB) nbody_sens_replay_kernel(SensArgs a) {
+    __shared__ double s_node[8 * NODE_ROW_S];
+    __shared__ double s_b[SENS_BLOCK / SG][21];
+    __shared__ double s_e[SENS_BLOCK / SG][SG * 3];
+    sens_load_nodes(s_node);
+    __syncthreads();
+    const int lane = threadIdx.x & (SG - 1);
+    const int warp_lane = threadIdx.x & 31;
+    const unsigned gmask = 0xFFu << (warp_lane & ~(SG - 1));
+    const int64_t item = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / SG;
+    const int64_t obj = item / a.ckpt_cap;
+    const int cb = (int)(item % a.ckpt_cap);
+    if (obj >= a.n || a.status[obj] != ST_OK || cb >= a.ckpt_count[obj]) return;
+    const int64_t n = a.n;
+    int k = 0;  // the epoch segment holding block cb
+    while (k + 1 < a.n_epochs && a.ckpt_seg[(int64_t)(k + 1) * n + obj] <= cb) ++k;
+    double* sb = s_b[threadIdx.x / SG];
+    double* se = s_e[threadIdx.x / SG];
+    const int comp = lane % 3;
+    const double* nrow = s_node + (lane < 7 ? lane + 1 : 7) * NODE_ROW_S;
+    SpkForce F;
+    F.n_force = a.n_force;
+    F.ng.base = a.nongrav ? a.nongrav + obj : nullptr;
+    F.ng.stride = n;
+    F.ng.kind = a.nongrav ? (int)a.nongrav[obj] : 0;
+    F.impact_id = 0;
+    F.min_dist = 1e300;
+    F.min_id = 0;
+    extern __shared__ double s_dyn[];
+    const FastPlan& plan = a.n_force == c_eph.n_force_planets ? c_eph.fast_planets : c_eph.fast_all;
+    EphCache C{s_dyn + threadIdx.x, SENS_BLOCK,
+               plan.ok && SpkForce::cached_doubles(plan) <= EPH_CACHE,
+               __longlong_as_double(0x7ff8000000000000LL)};
+    double* rec = a.rec_all + (size_t)item * (SENS_CK_ATTEMPTS + 1) * SENS_STRIDE;
+    const double* c = a.ckpt + ((size_t)obj * a.ckpt_cap + cb) * SENS_STRIDE;
+    int na = 0;
+    const int rc = sens_replay_block(c, a.epochs[k], rec, F, nrow, sb, se, lane, comp, gmask,
+                                     warp_lane, a.max_loops * 12, C, na);
+    if (lane == 0) a.rep_count[item] = rc == ST_OK ? na : -1 - rc;
+}
+
 template <int MINB>
 __global__ void __launch_bounds__(SENS_BLOCK, MINB) nbody_sens_backward_kernel(SensArgs a) {
     __shared__ double s_node[8 * NODE_ROW_S];
@@ -513,7 +599,7 @@ __global__ void __launch_bounds__(SENS_BLOCK, MINB) nbody_sens_backward_kernel(S
     double* stx = s_t[threadIdx.x / SG];
     const int comp = lane % 3;
     const double* nrow = s_node + (lane < 7 ? lane + 1 : 7) * NODE_ROW_S;
-    double* rec = a.rec + (size_t)obj * (SENS_CK_ATTEMPTS + 1) * SENS_STRIDE;
+    double* rec_own = a.rec + (size_t)obj * (SENS_CK_ATTEMPTS + 1) * SENS_STRIDE;
     const double* ck = a.ckpt + (size_t)obj * a.ckpt_cap * SENS_STRIDE;
 
     SpkForce F;
@@ -570,41 +656,29 @@ __global__ void __launch_bounds__(SENS_BLOCK, MINB) nbody_sens_backward_kernel(S
         const int c1 = k + 1 < a.n_epochs ? a.ckpt_seg[(int64_t)(k + 1) * n + obj] : n_ck;
         const double tf = a.epochs[k];
         for (int cb = c1 - 1; cb >= c0 && fail == ST_OK; --cb) {
-            // ---- re-run the block from its checkpoint ----
+            // ---- the block's attempt records: replayed up front, or re-run here ----
             const double* c = ck + (size_t)cb * SENS_STRIDE;
-            SensGroup G;
-            G.t = c[0];
-            G.h = c[1];
-            G.failures = (int)c[2];
-            G.tf = tf;
-            G.next_h = 0.0;
-            G.h_prev = c[34];
-            G.predict = c[34] != 0.0;
-#pragma unroll
-            for (int q = 0; q < 3; ++q) {
-                G.x[q] = c[4 + q];
-                G.v[q] = c[7 + q];
-                G.acc[q] = c[10 + q];
+            int na = 0;
+            double* rec = rec_own;
+            if (a.rec_all) {
+                const size_t item = (size_t)obj * a.ckpt_cap + cb;
+                rec = a.rec_all + item * (SENS_CK_ATTEMPTS + 1) * SENS_STRIDE;
+                const int cnt = a.rep_count[item];
+                if (cnt < 0) {
+                    fail = -1 - cnt;
+                    break;
+                }
+                na = cnt;
+            } else {
+                const int rrc = sens_replay_block(c, tf, rec, F, nrow, sb, se, lane, comp, gmask,
+                                                  warp_lane, max_rounds, C, na);
+                if (rrc != ST_OK) {
+                    fail = rrc;
+                    break;
+                }
             }
-            G.iter = 0;
-            G.att = 0;
-            G.rc = ST_OK;
-            if (lane < 7) {
-                sb[lane] = c[13 + lane];
-                sb[7 + lane] = c[20 + lane];
-                sb[14 + lane] = c[27 + lane];
-            }
-            __syncwarp(gmask);
-            G.phase = SP_BEGIN;
-            SensReplayPolicy P{rec, 0, lane, sb};
-            sens_rounds(G, F, P, nrow, sb, se, lane, comp, gmask, warp_lane, max_rounds, C);
-            if (G.phase != SP_PAUSE) {
-                fail = G.rc != ST_OK ? G.rc : ST_TIMEOUT;
-                break;
-            }
-            __syncwarp(gmask);  // the records are complete and visible to the group
             // ---- transpose the attempts, last first ----
-            for (int s = P.na - 1; s >= 0; --s) {
+            for (int s = na - 1; s >= 0; --s) {
                 const double* r0 = rec + (size_t)s * SENS_STRIDE;
                 const double* r1 = r0 + SENS_STRIDE;
                 const double t0 = r0[0], h = r0[1];

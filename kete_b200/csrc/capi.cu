@@ -1312,6 +1312,20 @@ int kete_b200_propagate_n_body_adjoint(int64_t n, int n_epochs, const double* ep
     if ((rc = staging(*ds, 33, (size_t)n * (SENS_CK_ATTEMPTS + 1) * SENS_STRIDE * sizeof(double), &rec)))
         return rc;
     a.rec = (double*)rec;
+    // the records of every checkpoint block, replayed in parallel before the sweep, when they
+    // fit a bounded scratch (else each block is re-run inside the sweep)
+    const size_t all_bytes =
+        (size_t)n * ckpt_capacity * (SENS_CK_ATTEMPTS + 1) * SENS_STRIDE * sizeof(double);
+    a.rec_all = nullptr;
+    a.rep_count = nullptr;
+    if (g_launch.adjoint_parallel_replay && all_bytes <= ADJOINT_REPLAY_BYTES) {
+        void *ra, *rn;
+        if ((rc = staging(*ds, 35, all_bytes, &ra)) ||
+            (rc = staging(*ds, 36, (size_t)n * ckpt_capacity * sizeof(int32_t), &rn)))
+            return rc;
+        a.rec_all = (double*)ra;
+        a.rep_count = (int32_t*)rn;
+    }
     if ((rc = launch_sens_backward(a, st))) return rc;
     return S.finish();
 }

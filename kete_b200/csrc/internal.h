@@ -98,7 +98,10 @@ struct LaunchConfig {
     int max_loops_long = 1 << 24;  // system integration (every batch's whole span)
     int sens_form = 0;  // forward sensitivities: 0 node-parallel, 1 one object per thread
     int fov_form = 0;   // field checks: 0 linear screen + two-body pass, 1 one fused pass
+    int adjoint_parallel_replay = 1;  // adjoint: replay every checkpoint block up front
 };
+// scratch bound of the adjoint's up-front replay (every block's attempt records)
+constexpr size_t ADJOINT_REPLAY_BYTES = size_t(8) << 30;
 LaunchConfig& launch_config();
 int noalloc_snapshot(int include_asteroids, int64_t center, NBodyArgs& a, LaunchConfig& cfg);
 int launch_radau_central(int64_t n, const double* pos, const double* vel, const double* t0,
@@ -153,6 +156,9 @@ struct SensArgs {
     double* out_grad;    // 8 x n: dL/d(pos0, vel0, A1, A2) (adjoint)
     int32_t* grad_status;  // n or null (adjoint)
     double* rec;         // n x (SENS_CK_ATTEMPTS + 1) x SENS_STRIDE scratch (adjoint)
+    double* rec_all;     // n x ckpt_cap x (SENS_CK_ATTEMPTS + 1) x SENS_STRIDE, or null: the
+                         // records of every block, replayed up front (adjoint)
+    int32_t* rep_count;  // n x ckpt_cap: attempts of each replayed block, -1 - status on failure
     int max_loops;
 };
 int launch_sens_forward(const SensArgs& a, cudaStream_t stream);
