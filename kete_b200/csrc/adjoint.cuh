@@ -35,7 +35,7 @@
 namespace kb {
 
 constexpr int SENS_BLOCK = 128;
-constexpr int SG = SENS_GROUP;  // lanes per object
+constexpr int SG = 8;  // lanes per object
 
 enum SensPhase : int { SP_BEGIN = 0, SP_EXACT_INIT = 1, SP_ITER = 2, SP_EXACT_STEP = 3, SP_PAUSE = 4, SP_DONE = 5 };
 
@@ -427,6 +427,44 @@ __global__ void __launch_bounds__(SENS_BLOCK, MINB) nbody_sens_forward_kernel(Se
 // ---------------------------------------------------------------------------------------
 // backward: re-run each checkpoint block, then transpose its attempts
 // ---------------------------------------------------------------------------------------
+struct SensReplayPolicy {
+    double* rec;  // SENS_CK_ATTEMPTS + 1 records
+    int na;       // attempts recorded
+    int lane;
+    double* sb;
+
+    __device__ bool begin_attempt(SensGroup& G) {
+        sens_store_state(rec + (size_t)na * SENS_STRIDE, G, sb, lane, 0.0);
+        if (na == SENS_CK_ATTEMPTS) return false;  // the block's end state is stored
+        na++;
+        return true;
+    }
+    __device__ void attempt_predict(double q) {
+        if (lane == 0) rec[(size_t)(na - 1) * SENS_STRIDE + 34] = q;
+    }
+    __device__ void last_iteration(SensGroup&, double, const double*, const double*, int) {}
+    __device__ void iter_round(SensGroup&, double* b, int ln) {  // b of the previous iterate
+        double* d = rec + (size_t)(na - 1) * SENS_STRIDE;
+        if (ln < 7) {
+            d[13 + ln] = b[ln];
+            d[20 + ln] = b[7 + ln];
+            d[27 + ln] = b[14 + ln];
+        }
+    }
+    __device__ void end_attempt(SensGroup& G, bool converged) {
+        if (lane == 0) {
+            double* d = rec + (size_t)(na - 1) * SENS_STRIDE;
+            d[1] = G.h;
+            d[2] = (double)G.iter;
+            d[3] = converged ? 1.0 : 0.0;
+        }
+    }
+    __device__ void segment_end(SensGroup& G) {
+        sens_store_state(rec + (size_t)na * SENS_STRIDE, G, sb, lane, 0.0);
+        G.phase = SP_PAUSE;
+    }
+};
+
 // Jacobian of the force at one point (dual numbers): J (3 x 6) = d a / d(x, v) and
 // jp (3 x 2) = d a / d(A1, A2).  Out of line: one copy serves every call site.
 static __device__ __noinline__ int sens_jacobian(TangentForce& T, double t, const double* x,
@@ -447,68 +485,6 @@ static __device__ __noinline__ int sens_jacobian(TangentForce& T, double t, cons
     return rc;
 }
 
-struct SensReplayPolicy {
-    double* rec;  // SENS_CK_ATTEMPTS + 1 records
-    int na;       // attempts recorded
-    int lane;
-    double* sb;
-    // optional (the up-front replay): the force Jacobians of every recorded attempt, SENS_JAC
-    // doubles per lane -- lane j < 7 at node j + 1's point of the attempt's last corrector
-    // iteration, taken in that round while the lane's body cache holds the node's time;
-    // lane 7 at the accepted state
-    double* jac = nullptr;
-    TangentForce* T = nullptr;
-    EphCache* C = nullptr;
-
-    __device__ void store_jacobian(double t, const double* x, const double* v) {
-        double J[18], jp[6];
-        const int rc = sens_jacobian(*T, t, x, v, J, jp, *C);
-        double* d = jac + ((size_t)(na - 1) * SG + lane) * SENS_JAC;
-#pragma unroll
-        for (int i = 0; i < 18; ++i) d[i] = J[i];
-#pragma unroll
-        for (int i = 0; i < 6; ++i) d[18 + i] = jp[i];
-        d[24] = (double)rc;
-    }
-
-    __device__ bool begin_attempt(SensGroup& G) {
-        sens_store_state(rec + (size_t)na * SENS_STRIDE, G, sb, lane, 0.0);
-        if (na == SENS_CK_ATTEMPTS) return false;  // the block's end state is stored
-        na++;
-        return true;
-    }
-    __device__ void attempt_predict(double q) {
-        if (lane == 0) rec[(size_t)(na - 1) * SENS_STRIDE + 34] = q;
-    }
-    __device__ void last_iteration(SensGroup&, double te, const double* xe, const double* ve,
-                                   int ln) {
-        if (jac && ln < 7) store_jacobian(te, xe, ve);
-    }
-    __device__ void iter_round(SensGroup&, double* b, int ln) {  // b of the previous iterate
-        double* d = rec + (size_t)(na - 1) * SENS_STRIDE;
-        if (ln < 7) {
-            d[13 + ln] = b[ln];
-            d[20 + ln] = b[7 + ln];
-            d[27 + ln] = b[14 + ln];
-        }
-    }
-    __device__ void end_attempt(SensGroup& G, bool converged) {
-        if (lane == 0) {
-            double* d = rec + (size_t)(na - 1) * SENS_STRIDE;
-            d[1] = G.h;
-            d[2] = (double)G.iter;
-            d[3] = converged ? 1.0 : 0.0;
-        }
-        // a' = F(x', v'): the cache holds the accepted epoch after the exact evaluation
-        if (jac && lane == 7 && converged) store_jacobian(G.t, G.x, G.v);
-    }
-    __device__ void segment_end(SensGroup& G) {
-        sens_store_state(rec + (size_t)na * SENS_STRIDE, G, sb, lane, 0.0);
-        G.phase = SP_PAUSE;
-    }
-};
-
-
 // Re-run checkpoint block `c` (its segment ends at tf) with the step code, recording every
 // attempt into rec (SENS_CK_ATTEMPTS + 1 records).  Returns ST_OK with the attempt count in na,
 // or the failure.
@@ -516,8 +492,7 @@ __device__ __forceinline__ int sens_replay_block(const double* c, double tf, dou
                                                  SpkForce& F, const double* nrow, double* sb,
                                                  double* se, int lane, int comp, unsigned gmask,
                                                  int warp_lane, int max_rounds, EphCache& C,
-                                                 int& na, double* jac = nullptr,
-                                                 TangentForce* T = nullptr) {
+                                                 int& na) {
     SensGroup G;
     G.t = c[0];
     G.h = c[1];
@@ -542,7 +517,7 @@ __device__ __forceinline__ int sens_replay_block(const double* c, double tf, dou
     }
     __syncwarp(gmask);
     G.phase = SP_BEGIN;
-    SensReplayPolicy P{rec, 0, lane, sb, jac, T, &C};
+    SensReplayPolicy P{rec, 0, lane, sb};
     sens_rounds(G, F, P, nrow, sb, se, lane, comp, gmask, warp_lane, max_rounds, C);
     na = P.na;
     __syncwarp(gmask);  // the records are complete and visible to the group
@@ -588,17 +563,11 @@ __global__ void __launch_bounds__(SENS_BLOCK, MINB) nbody_sens_replay_kernel(Sen
     EphCache C{s_dyn + threadIdx.x, SENS_BLOCK,
                plan.ok && SpkForce::cached_doubles(plan) <= EPH_CACHE,
                __longlong_as_double(0x7ff8000000000000LL)};
-    TangentForce T;
-    T.n_force = a.n_force;
-    T.ng = F.ng;
-    T.impact_id = 0;
-    T.min_dist = 1e300;
     double* rec = a.rec_all + (size_t)item * (SENS_CK_ATTEMPTS + 1) * SENS_STRIDE;
-    double* jac = a.jac_all ? a.jac_all + (size_t)item * SENS_CK_ATTEMPTS * SG * SENS_JAC : nullptr;
     const double* c = a.ckpt + ((size_t)obj * a.ckpt_cap + cb) * SENS_STRIDE;
     int na = 0;
     const int rc = sens_replay_block(c, a.epochs[k], rec, F, nrow, sb, se, lane, comp, gmask,
-                                     warp_lane, a.max_loops * 12, C, na, jac, &T);
+                                     warp_lane, a.max_loops * 12, C, na);
     if (lane == 0) a.rep_count[item] = rc == ST_OK ? na : -1 - rc;
 }
 
@@ -691,11 +660,9 @@ __global__ void __launch_bounds__(SENS_BLOCK, MINB) nbody_sens_backward_kernel(S
             const double* c = ck + (size_t)cb * SENS_STRIDE;
             int na = 0;
             double* rec = rec_own;
-            const double* jac_blk = nullptr;
             if (a.rec_all) {
                 const size_t item = (size_t)obj * a.ckpt_cap + cb;
                 rec = a.rec_all + item * (SENS_CK_ATTEMPTS + 1) * SENS_STRIDE;
-                if (a.jac_all) jac_blk = a.jac_all + item * SENS_CK_ATTEMPTS * SG * SENS_JAC;
                 const int cnt = a.rep_count[item];
                 if (cnt < 0) {
                     fail = -1 - cnt;
@@ -742,17 +709,7 @@ __global__ void __launch_bounds__(SENS_BLOCK, MINB) nbody_sens_backward_kernel(S
                     }
                 }
                 double J[18], jp[6];
-                int jrc;
-                if (jac_blk) {  // taken by the up-front replay at the same points
-                    const double* jd = jac_blk + ((size_t)s * SG + lane) * SENS_JAC;
-#pragma unroll
-                    for (int i = 0; i < 18; ++i) J[i] = jd[i];
-#pragma unroll
-                    for (int i = 0; i < 6; ++i) jp[i] = jd[18 + i];
-                    jrc = (lane < 7 || conv) ? (int)jd[24] : ST_OK;
-                } else {
-                    jrc = sens_jacobian(T, te, xe, ve, J, jp, C);
-                }
+                const int jrc = sens_jacobian(T, te, xe, ve, J, jp, C);
                 const unsigned bad = __ballot_sync(gmask, jrc != ST_OK && (lane < 7 || conv));
                 if (bad) {
                     fail = ST_DAF_LIMITS;
