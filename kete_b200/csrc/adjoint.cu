@@ -22,33 +22,31 @@ int launch_sens_backward(const SensArgs& a, cudaStream_t stream) {
     if (a.n <= 0) return 0;
     const int64_t threads = a.n * SG;
     // the per-lane ephemeris cache takes the block past the 48 KB of shared memory a kernel
-    // gets without opting in: opt in once per device
+    // gets without opting in (a function attribute, not a stream operation)
     constexpr int cache_bytes = EPH_CACHE * SENS_BLOCK * (int)sizeof(double);
-    static bool opted[64] = {};
-    int dev = 0;
-    int rc = cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
-    if (rc) return rc;
-    if (dev < 0 || dev >= 64) return cuda_check(cudaErrorInvalidDevice, "device index");
-    if (!opted[dev]) {
-        if ((rc = cuda_check(cudaFuncSetAttribute(nbody_sens_backward_kernel<1>,
+    int rc = 0;
+    const unsigned grid = (unsigned)((threads + SENS_BLOCK - 1) / SENS_BLOCK);
+    if (!a.rec_all) {  // the sweep re-runs each block itself
+        if ((rc = cuda_check(cudaFuncSetAttribute(nbody_sens_backward_kernel<1, true>,
                                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                   cache_bytes),
                              "cudaFuncSetAttribute")))
             return rc;
-        opted[dev] = true;
+        nbody_sens_backward_kernel<1, true><<<grid, SENS_BLOCK, cache_bytes, stream>>>(a);
+        return launched(1, "nbody_sens_backward_kernel launch");
     }
-    if (a.rec_all) {  // every block's replay first, one group per (object, block)
-        if ((rc = cuda_check(cudaFuncSetAttribute(nbody_sens_replay_kernel<1>,
-                                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+    // every block's replay first, one group per (object, block); then the sweep
+    for (const void* f : {(const void*)nbody_sens_replay_kernel<1>,
+                          (const void*)nbody_sens_backward_kernel<1, false>})
+        if ((rc = cuda_check(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                   cache_bytes),
                              "cudaFuncSetAttribute")))
             return rc;
-        const int64_t rthreads = a.n * (int64_t)a.ckpt_cap * SG;
-        nbody_sens_replay_kernel<1><<<(unsigned)((rthreads + SENS_BLOCK - 1) / SENS_BLOCK),
-                                      SENS_BLOCK, cache_bytes, stream>>>(a);
-        if ((rc = launched(1, "nbody_sens_replay_kernel launch"))) return rc;
-    }
-    nbody_sens_backward_kernel<1><<<(unsigned)((threads + SENS_BLOCK - 1) / SENS_BLOCK), SENS_BLOCK, cache_bytes, stream>>>(a);
+    const int64_t rthreads = a.n * (int64_t)a.ckpt_cap * SG;
+    nbody_sens_replay_kernel<1><<<(unsigned)((rthreads + SENS_BLOCK - 1) / SENS_BLOCK), SENS_BLOCK,
+                                  cache_bytes, stream>>>(a);
+    if ((rc = launched(1, "nbody_sens_replay_kernel launch"))) return rc;
+    nbody_sens_backward_kernel<1, false><<<grid, SENS_BLOCK, cache_bytes, stream>>>(a);
     return launched(1, "nbody_sens_backward_kernel launch");
 }
 

@@ -571,7 +571,10 @@ __global__ void __launch_bounds__(SENS_BLOCK, MINB) nbody_sens_replay_kernel(Sen
     if (lane == 0) a.rep_count[item] = rc == ST_OK ? na : -1 - rc;
 }
 
-template <int MINB>
+// REPLAY: the sweep re-runs each block itself (the records did not fit the up-front replay's
+// scratch); otherwise it reads the records nbody_sens_replay_kernel wrote, and carries no
+// step code (a smaller kernel with fewer registers).
+template <int MINB, bool REPLAY>
 __global__ void __launch_bounds__(SENS_BLOCK, MINB) nbody_sens_backward_kernel(SensArgs a) {
     __shared__ double s_node[8 * NODE_ROW_S];
     __shared__ double s_P[49];
@@ -660,7 +663,7 @@ __global__ void __launch_bounds__(SENS_BLOCK, MINB) nbody_sens_backward_kernel(S
             const double* c = ck + (size_t)cb * SENS_STRIDE;
             int na = 0;
             double* rec = rec_own;
-            if (a.rec_all) {
+            if (!REPLAY) {
                 const size_t item = (size_t)obj * a.ckpt_cap + cb;
                 rec = a.rec_all + item * (SENS_CK_ATTEMPTS + 1) * SENS_STRIDE;
                 const int cnt = a.rep_count[item];
