@@ -577,8 +577,7 @@ __global__ void __launch_bounds__(SENS_BLOCK, MINB) nbody_sens_replay_kernel(Sen
 // and the b of that iteration), lane 7 at the accepted state (the next record's start), each
 // written as J (18), jp (6) and the evaluation's status to a.jac_all.  The same points and the
 // same arithmetic as the sweep's own Jacobian rounds.
-template <int MINB>
-__global__ void __launch_bounds__(SENS_BLOCK, MINB) nbody_sens_jacobian_kernel(SensArgs a) {
+__global__ void __launch_bounds__(SENS_BLOCK) nbody_sens_jacobian_kernel(SensArgs a) {
     __shared__ double s_node[8 * NODE_ROW_S];
     sens_load_nodes(s_node);
     __syncthreads();
