@@ -35,12 +35,9 @@ int launch_sens_backward(const SensArgs& a, cudaStream_t stream) {
         nbody_sens_backward_kernel<1, true><<<grid, SENS_BLOCK, cache_bytes, stream>>>(a);
         return launched(1, "nbody_sens_backward_kernel launch");
     }
-    // every block's replay first, one group per (object, block); then, when their scratch was
-    // granted, every attempt's Jacobians, one thread per (attempt, lane); then the sweep
+    // every block's replay first, one group per (object, block); then the sweep
     for (const void* f : {(const void*)nbody_sens_replay_kernel<1>,
-                          (const void*)nbody_sens_jacobian_kernel,
-                          (const void*)nbody_sens_backward_kernel<1, false>,
-                          (const void*)nbody_sens_backward_kernel<1, false, true>})
+                          (const void*)nbody_sens_backward_kernel<1, false>})
         if ((rc = cuda_check(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                   cache_bytes),
                              "cudaFuncSetAttribute")))
@@ -49,15 +46,7 @@ int launch_sens_backward(const SensArgs& a, cudaStream_t stream) {
     nbody_sens_replay_kernel<1><<<(unsigned)((rthreads + SENS_BLOCK - 1) / SENS_BLOCK), SENS_BLOCK,
                                   cache_bytes, stream>>>(a);
     if ((rc = launched(1, "nbody_sens_replay_kernel launch"))) return rc;
-    if (a.jac_all) {
-        const int64_t jthreads = rthreads * SENS_CK_ATTEMPTS;
-        nbody_sens_jacobian_kernel<<<(unsigned)((jthreads + SENS_BLOCK - 1) / SENS_BLOCK),
-                                     SENS_BLOCK, cache_bytes, stream>>>(a);
-        if ((rc = launched(1, "nbody_sens_jacobian_kernel launch"))) return rc;
-        nbody_sens_backward_kernel<1, false, true><<<grid, SENS_BLOCK, cache_bytes, stream>>>(a);
-    } else {
-        nbody_sens_backward_kernel<1, false><<<grid, SENS_BLOCK, cache_bytes, stream>>>(a);
-    }
+    nbody_sens_backward_kernel<1, false><<<grid, SENS_BLOCK, cache_bytes, stream>>>(a);
     return launched(1, "nbody_sens_backward_kernel launch");
 }
 

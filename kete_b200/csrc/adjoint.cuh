@@ -35,7 +35,7 @@
 namespace kb {
 
 constexpr int SENS_BLOCK = 128;
-constexpr int SG = SENS_GROUP;  // lanes per object
+constexpr int SG = 8;  // lanes per object
 
 enum SensPhase : int { SP_BEGIN = 0, SP_EXACT_INIT = 1, SP_ITER = 2, SP_EXACT_STEP = 3, SP_PAUSE = 4, SP_DONE = 5 };
 
@@ -571,87 +571,10 @@ __global__ void __launch_bounds__(SENS_BLOCK, MINB) nbody_sens_replay_kernel(Sen
     if (lane == 0) a.rep_count[item] = rc == ST_OK ? na : -1 - rc;
 }
 
-// The force Jacobians of every replayed attempt at once, after nbody_sens_replay_kernel and
-// before the sweep: one thread per (object, block, attempt, lane), lane j < 7 at node j + 1's
-// point of the attempt's last corrector iteration (from the attempt's record: its start state
-// and the b of that iteration), lane 7 at the accepted state (the next record's start), each
-// written as J (18), jp (6) and the evaluation's status to a.jac_all.  The same points and the
-// same arithmetic as the sweep's own Jacobian rounds.
-__global__ void __launch_bounds__(SENS_BLOCK) nbody_sens_jacobian_kernel(SensArgs a) {
-    __shared__ double s_node[8 * NODE_ROW_S];
-    sens_load_nodes(s_node);
-    __syncthreads();
-    const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int lane = (int)(gid % SG);
-    const int64_t att = gid / SG;  // (item, s)
-    const int s = (int)(att % SENS_CK_ATTEMPTS);
-    const int64_t item = att / SENS_CK_ATTEMPTS;
-    const int64_t obj = item / a.ckpt_cap;
-    if (obj >= a.n || a.status[obj] != ST_OK) return;
-    const int cb = (int)(item % a.ckpt_cap);
-    if (cb >= a.ckpt_count[obj]) return;
-    const int na = a.rep_count[item];
-    if (s >= na) return;
-    const double* r0 = a.rec_all + ((size_t)item * (SENS_CK_ATTEMPTS + 1) + s) * SENS_STRIDE;
-    const double* r1 = r0 + SENS_STRIDE;
-    const double h = r0[1];
-    const bool conv = r0[3] != 0.0;
-    double* d = a.jac_all + ((size_t)att * SG + lane) * SENS_JAC;
-    if (lane == 7 && !conv) {  // no accepted state: nothing to differentiate
-        d[24] = (double)ST_OK;
-        return;
-    }
-    const double* nrow = s_node + (lane < 7 ? lane + 1 : 7) * NODE_ROW_S;
-    double te, xe[3], ve[3];
-    if (lane < 7) {
-        const double f = nrow[14], frac2 = nrow[15], h2 = h * h;
-#pragma unroll
-        for (int q = 0; q < 3; ++q) {
-            double bw = 0.0, bu = 0.0;
-#pragma unroll
-            for (int kk = 0; kk < 7; ++kk) {
-                const double bck = r0[13 + 7 * q + kk];
-                bw += nrow[kk] * bck;
-                bu += nrow[7 + kk] * bck;
-            }
-            xe[q] = r0[4 + q] + f * r0[7 + q] * h + frac2 * h2 * (r0[10 + q] / 2.0 + bw);
-            ve[q] = r0[7 + q] + f * h * (r0[10 + q] + bu);
-        }
-        te = r0[0] + f * h;
-    } else {
-        te = r1[0];
-#pragma unroll
-        for (int q = 0; q < 3; ++q) {
-            xe[q] = r1[4 + q];
-            ve[q] = r1[7 + q];
-        }
-    }
-    TangentForce T;
-    T.n_force = a.n_force;
-    T.ng.base = a.nongrav ? a.nongrav + obj : nullptr;
-    T.ng.stride = a.n;
-    T.ng.kind = a.nongrav ? (int)a.nongrav[obj] : 0;
-    T.impact_id = 0;
-    T.min_dist = 1e300;
-    extern __shared__ double s_dyn[];
-    const FastPlan& plan = a.n_force == c_eph.n_force_planets ? c_eph.fast_planets : c_eph.fast_all;
-    EphCache C{s_dyn + threadIdx.x, SENS_BLOCK,
-               plan.ok && SpkForce::cached_doubles(plan) <= EPH_CACHE,
-               __longlong_as_double(0x7ff8000000000000LL)};
-    double J[18], jp[6];
-    const int rc = sens_jacobian(T, te, xe, ve, J, jp, C);
-#pragma unroll
-    for (int i = 0; i < 18; ++i) d[i] = J[i];
-#pragma unroll
-    for (int i = 0; i < 6; ++i) d[18 + i] = jp[i];
-    d[24] = (double)rc;
-}
-
 // REPLAY: the sweep re-runs each block itself (the records did not fit the up-front replay's
 // scratch); otherwise it reads the records nbody_sens_replay_kernel wrote, and carries no
-// step code (a smaller kernel with fewer registers).  JAC: the attempts' Jacobians come from
-// nbody_sens_jacobian_kernel (a.jac_all) instead of rounds of the sweep's own.
-template <int MINB, bool REPLAY, bool JAC = false>
+// step code (a smaller kernel with fewer registers).
+template <int MINB, bool REPLAY>
 __global__ void __launch_bounds__(SENS_BLOCK, MINB) nbody_sens_backward_kernel(SensArgs a) {
     __shared__ double s_node[8 * NODE_ROW_S];
     __shared__ double s_P[49];
@@ -789,19 +712,7 @@ __global__ void __launch_bounds__(SENS_BLOCK, MINB) nbody_sens_backward_kernel(S
                     }
                 }
                 double J[18], jp[6];
-                int jrc;
-                if (JAC) {  // from nbody_sens_jacobian_kernel, at the same points
-                    const double* jd =
-                        a.jac_all + ((((size_t)obj * a.ckpt_cap + cb) * SENS_CK_ATTEMPTS + s) * SG +
-                                     lane) * SENS_JAC;
-#pragma unroll
-                    for (int i = 0; i < 18; ++i) J[i] = jd[i];
-#pragma unroll
-                    for (int i = 0; i < 6; ++i) jp[i] = jd[18 + i];
-                    jrc = (int)jd[24];
-                } else {
-                    jrc = sens_jacobian(T, te, xe, ve, J, jp, C);
-                }
+                const int jrc = sens_jacobian(T, te, xe, ve, J, jp, C);
                 const unsigned bad = __ballot_sync(gmask, jrc != ST_OK && (lane < 7 || conv));
                 if (bad) {
                     fail = ST_DAF_LIMITS;

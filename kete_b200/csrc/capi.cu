@@ -1316,11 +1316,8 @@ int kete_b200_propagate_n_body_adjoint(int64_t n, int n_epochs, const double* ep
     // fit a bounded scratch (else each block is re-run inside the sweep)
     const size_t all_bytes =
         (size_t)n * ckpt_capacity * (SENS_CK_ATTEMPTS + 1) * SENS_STRIDE * sizeof(double);
-    const size_t jac_bytes =
-        (size_t)n * ckpt_capacity * SENS_CK_ATTEMPTS * SENS_GROUP * SENS_JAC * sizeof(double);
     a.rec_all = nullptr;
     a.rep_count = nullptr;
-    a.jac_all = nullptr;
     if (g_launch.adjoint_parallel_replay && all_bytes <= ADJOINT_REPLAY_BYTES) {
         void *ra, *rn;
         if ((rc = staging(*ds, 35, all_bytes, &ra)) ||
@@ -1328,12 +1325,6 @@ int kete_b200_propagate_n_body_adjoint(int64_t n, int n_epochs, const double* ep
             return rc;
         a.rec_all = (double*)ra;
         a.rep_count = (int32_t*)rn;
-        // and the attempts' Jacobians, evaluated in parallel, when they fit the bound too
-        if (all_bytes + jac_bytes <= ADJOINT_REPLAY_BYTES) {
-            void* ja;
-            if ((rc = staging(*ds, 37, jac_bytes, &ja))) return rc;
-            a.jac_all = (double*)ja;
-        }
     }
     if ((rc = launch_sens_backward(a, st))) return rc;
     return S.finish();

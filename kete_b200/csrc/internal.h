@@ -101,7 +101,7 @@ struct LaunchConfig {
     int adjoint_parallel_replay = 1;  // adjoint: replay every checkpoint block up front
 };
 // scratch bound of the adjoint's up-front replay (every block's attempt records)
-constexpr size_t ADJOINT_REPLAY_BYTES = size_t(16) << 30;
+constexpr size_t ADJOINT_REPLAY_BYTES = size_t(8) << 30;
 LaunchConfig& launch_config();
 int noalloc_snapshot(int include_asteroids, int64_t center, NBodyArgs& a, LaunchConfig& cfg);
 int launch_radau_central(int64_t n, const double* pos, const double* vel, const double* t0,
@@ -135,8 +135,6 @@ int launch_nbody_stm(const StmArgs& a, int form, cudaStream_t stream);
 // reverse-mode gradients: checkpointed forward pass and adjoint pass (adjoint.cuh)
 constexpr int SENS_STRIDE = 36;       // doubles per checkpoint / attempt record
 constexpr int SENS_CK_ATTEMPTS = 16;  // step attempts between checkpoints
-constexpr int SENS_JAC = 25;          // doubles per lane and attempt: J (18), jp (6), status
-constexpr int SENS_GROUP = 8;         // lanes per object in the sensitivity kernels
 struct SensArgs {
     int64_t n;
     const double* pos;  // 3 x n (forward)
@@ -161,8 +159,6 @@ struct SensArgs {
     double* rec_all;     // n x ckpt_cap x (SENS_CK_ATTEMPTS + 1) x SENS_STRIDE, or null: the
                          // records of every block, replayed up front (adjoint)
     int32_t* rep_count;  // n x ckpt_cap: attempts of each replayed block, -1 - status on failure
-    double* jac_all;     // n x ckpt_cap x SENS_CK_ATTEMPTS x 8 x SENS_JAC, or null: the force
-                         // Jacobians of every replayed attempt (adjoint)
     int max_loops;
 };
 int launch_sens_forward(const SensArgs& a, cudaStream_t stream);
