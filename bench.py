@@ -85,6 +85,9 @@ NODE_TRAFFIC = {
     ("nbody_mixed_1m", 9, 1): {"bytes_per_object": (13_523_968 + 951_296) / 100_000,
                                "fp64_pipe": 0.241,
                                "captured": "one launch on a 100,000-object sample of the workload"},
+    ("nbody_mixed_1m", 10, 1): {"bytes_per_object": (13_684_736 + 806_656) / 100_000,
+                                "fp64_pipe": 0.254,
+                                "captured": "one launch on a 100,000-object sample of the workload"},
 }
 
 CLOSE_AU = 0.01  # objects whose closest planet approach is below this are reported apart
@@ -573,7 +576,10 @@ def run_gpu(args, world, rank, local):
                                         d["vel"][:, sub].contiguous(),
                                         d["jd0"][sub].contiguous(), d["jd1"][sub].contiguous(),
                                         nongrav=(d["ng"][:, sub].contiguous() if "ng" in d
-                                                 else None))
+                                                 else None),
+                                        full=(None if n <= 200_000 else
+                                              (d["pos"], d["vel"], d["jd0"], d["jd1"],
+                                               d.get("ng"))))
         else:
             best = dict(mode=args.mode, variant=args.variant, refill=args.refill)
             tune.set_config(**best)
@@ -766,7 +772,9 @@ def run_gpu(args, world, rank, local):
         "config": bench_config(kind, n),
         "launch": {"config": best, "autotune_sweep_ms": sweep,
                    "autotune_inputs": ("the workload" if n <= 200_000 else
-                                       "every 8th object of the workload"),
+                                       "every 8th object of the workload; the configurations "
+                                       "within 5% of its best (at most 3) re-timed on the "
+                                       "whole workload (_full)"),
                    "cuda_graph": graph is not None,
                    "parallelism": f"replicas x{world} (objects independent)"},
         "roofline": roof,
@@ -1036,14 +1044,15 @@ def run_survey(args, world, rank, local):
         return ff, oo, ss, v, mags
 
     # launch configuration of the chunk re-propagations, tuned on a 200k-object sample over
-    # one chunk's span (2 x dt_limit)
+    # one chunk's span (2 x dt_limit), the closest configurations re-timed on every object
     from kete_b200 import tune
 
     m = min(n, 200_000)
-    launch, _ = tune.autotune(P[:, :m].contiguous(), V[:, :m].contiguous(),
-                              torch.full((m,), EPOCH, dtype=torch.float64, device=dev),
-                              torch.full((m,), EPOCH + 2 * SURVEY_DT_LIMIT, dtype=torch.float64,
-                                         device=dev), nongrav=G[:, :m].contiguous())
+    span = lambda k, d: torch.full((k,), EPOCH + d, dtype=torch.float64, device=dev)
+    launch, _ = tune.autotune(P[:, :m].contiguous(), V[:, :m].contiguous(), span(m, 0.0),
+                              span(m, 2 * SURVEY_DT_LIMIT), nongrav=G[:, :m].contiguous(),
+                              full=(None if m == n else
+                                    (P, V, span(n, 0.0), span(n, 2 * SURVEY_DT_LIMIT), G)))
     for _ in range(args.warmup):
         chain(P, V)
     torch.cuda.synchronize()

@@ -35,15 +35,17 @@ int launch_sens_backward(const SensArgs& a, cudaStream_t stream) {
         nbody_sens_backward_kernel<1, true><<<grid, SENS_BLOCK, cache_bytes, stream>>>(a);
         return launched(1, "nbody_sens_backward_kernel launch");
     }
-    // every block's replay first, one group per (object, block); then the sweep
-    for (const void* f : {(const void*)nbody_sens_replay_kernel<1>,
+    // every block's replay first, one group per (object, block); then the sweep. The replay
+    // is throughput bound (n x blocks groups), so it is capped at 168 registers for 12
+    // resident warps per SM; the sweep is one partial wave and keeps the full register file.
+    for (const void* f : {(const void*)nbody_sens_replay_kernel<3>,
                           (const void*)nbody_sens_backward_kernel<1, false>})
         if ((rc = cuda_check(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                   cache_bytes),
                              "cudaFuncSetAttribute")))
             return rc;
     const int64_t rthreads = a.n * (int64_t)a.ckpt_cap * SG;
-    nbody_sens_replay_kernel<1><<<(unsigned)((rthreads + SENS_BLOCK - 1) / SENS_BLOCK), SENS_BLOCK,
+    nbody_sens_replay_kernel<3><<<(unsigned)((rthreads + SENS_BLOCK - 1) / SENS_BLOCK), SENS_BLOCK,
                                   cache_bytes, stream>>>(a);
     if ((rc = launched(1, "nbody_sens_replay_kernel launch"))) return rc;
     nbody_sens_backward_kernel<1, false><<<grid, SENS_BLOCK, cache_bytes, stream>>>(a);
