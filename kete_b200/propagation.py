@@ -59,6 +59,30 @@ def _alloc_like(template, shape, dtype):
     return np.empty(shape, dtype=dtype)
 
 
+def _out_array(given, template, shape, dtype, name):
+    """A caller's output array (checked: shape, dtype, contiguous, the inputs' side), or a new
+    one like ``template``."""
+    if given is None:
+        return _alloc_like(template, shape, dtype)
+    if not (isinstance(given, np.ndarray) or _lib._is_torch_cuda(given)):
+        raise ValueError(f"{name}: expected a numpy array or a CUDA tensor")
+    if tuple(given.shape) != tuple(shape):
+        raise ValueError(f"{name}: expected shape {tuple(shape)}, got {tuple(given.shape)}")
+    if _lib._is_torch_cuda(given) != _lib._is_torch_cuda(template):
+        raise ValueError(f"{name}: output and inputs must live on the same side")
+    if _lib._is_torch_cuda(given):
+        import torch
+
+        tdt = {np.float64: torch.float64, np.int32: torch.int32}[dtype]
+        if given.dtype != tdt or not given.is_contiguous():
+            raise ValueError(f"{name}: expected a contiguous {tdt} tensor")
+    elif (not isinstance(given, np.ndarray) or given.dtype != dtype
+          or not given.flags.c_contiguous):
+        raise ValueError(f"{name}: expected a C-contiguous numpy array of "
+                         f"{np.dtype(dtype).name}")
+    return given
+
+
 def propagate_two_body_arrays(pos, vel, jd0, jd1, observer_pos=None):
     """Two-body propagation of n Sun-centred states (SoA (3, n) arrays), object i from
     jd0[i] to jd1[i].  Returns (pos, vel, jd, status)."""
@@ -77,17 +101,21 @@ def propagate_two_body_arrays(pos, vel, jd0, jd1, observer_pos=None):
 
 def propagate_n_body_arrays(pos, vel, jd0, jd1, frame=Frames.Ecliptic, center=10,
                             include_asteroids=False, nongrav=None, mode=_lib.MODE_AUTO,
-                            with_details=False):
+                            with_details=False, out=None):
     """N-body Radau propagation of n states sharing ``frame`` and ``center``.
 
     pos/vel: (3, n); jd0/jd1: (n,); nongrav: None or (10, n) rows.  Returns
     (pos, vel, status) and, with ``with_details``, a dict with impact_id, impact_jd,
-    min_dist and counters (3, n: accepted steps, corrector iterations, exact evals)."""
+    min_dist and counters (3, n: accepted steps, corrector iterations, exact evals).
+    ``out``: None, or the (pos (3, n) float64, vel (3, n) float64, status (n,) int32) arrays
+    to write the results into, on the inputs' side (host arrays in pinned memory that a
+    caller reuses across calls are copied back at full bus speed)."""
     n = int(pos.shape[1])
     _lib.init()
-    out_p = _alloc_like(pos, (3, n), np.float64)
-    out_v = _alloc_like(pos, (3, n), np.float64)
-    st = _alloc_like(pos, (n,), np.int32)
+    o_p, o_v, o_s = out if out is not None else (None, None, None)
+    out_p = _out_array(o_p, pos, (3, n), np.float64, "out[0]")
+    out_v = _out_array(o_v, pos, (3, n), np.float64, "out[1]")
+    st = _out_array(o_s, pos, (n,), np.int32, "out[2]")
     det = None
     if with_details:
         det = dict(impact_id=_alloc_like(pos, (n,), np.int32),

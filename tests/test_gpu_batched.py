@@ -125,3 +125,49 @@ def test_close_approaches_reported_apart(gpu, oracle_spk):
     print(f"{int(close.sum())} of {n} within 0.01 AU of a planet: max |dpos| "
           f"{err[ok & close].max():.3e} AU, median {np.median(err[ok & close]):.3e} AU; "
           f"{int((err[ok & close] <= 1e-9).sum())} within 1e-9 AU")
+
+
+def test_output_arrays_and_tuner_finalists(gpu):
+    """``out=`` writes the results into the caller's arrays, on the host and on the device,
+    bit-identical to a call that allocates them; the tuner's finalist stage re-times the
+    closest configurations on the whole population and installs the fastest there."""
+    import torch
+    from kete_b200 import tune
+
+    pos, vel, ng, jd0, jd1 = _population(n=3000, seed=91)
+    jd1 = EPOCH + (jd1 - EPOCH) / 20.0  # spans of up to a quarter year keep the sweep short
+    n = pos.shape[1]
+    try:
+        tune.set_config(mode=2, variant=10, refill=1)
+        ref = gpu.propagate_n_body_arrays(pos, vel, jd0, jd1, nongrav=ng, mode=2)
+        out = (np.empty((3, n)), np.empty((3, n)), np.empty(n, dtype=np.int32))
+        got = gpu.propagate_n_body_arrays(pos, vel, jd0, jd1, nongrav=ng, mode=2, out=out)
+        for a, b, c in zip(ref, out, got):
+            assert c is b
+            assert np.array_equal(a, b)
+        T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+        dev = (T(pos), T(vel), T(jd0), T(jd1), T(ng))
+        dout = (torch.empty((3, n), dtype=torch.float64, device="cuda"),
+                torch.empty((3, n), dtype=torch.float64, device="cuda"),
+                torch.empty((n,), dtype=torch.int32, device="cuda"))
+        gpu.propagate_n_body_arrays(*dev[:4], nongrav=dev[4], mode=2, out=dout)
+        torch.cuda.synchronize()
+        for a, b in zip(ref, dout):
+            assert np.array_equal(a, b.cpu().numpy())
+        with pytest.raises(ValueError):  # wrong shape
+            gpu.propagate_n_body_arrays(pos, vel, jd0, jd1, nongrav=ng, mode=2,
+                                        out=(out[0][:, :10], out[1], out[2]))
+        with pytest.raises(ValueError):  # host outputs for device inputs
+            gpu.propagate_n_body_arrays(*dev[:4], nongrav=dev[4], mode=2, out=out)
+
+        sub = slice(0, None, 4)
+        best, times = tune.autotune(*(x[..., sub].contiguous() for x in dev[:4]),
+                                    nongrav=dev[4][:, sub].contiguous(), full=dev,
+                                    finalists=2, within=10.0)
+        full = {k: v for k, v in times.items() if k.endswith("_full")}
+        assert len(full) == 2
+        label = f"mode{best['mode']}_v{best['variant']}_r{best['refill']}_full"
+        assert times[label] == min(full.values())
+        assert {k: tune.current()[k] for k in best} == best
+    finally:
+        tune.set_config()

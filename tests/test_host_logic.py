@@ -84,3 +84,24 @@ def test_adjoint_wrapper_checks_shapes():
                        np.zeros(4, np.int32), np.zeros((3, 4), np.int32), np.zeros(4, np.int32))
     with pytest.raises(ValueError):
         A.propagate_n_body_adjoint(ck, np.zeros((3, 6, 4)))
+
+
+def test_output_arrays_are_checked():
+    """propagate_n_body_arrays(out=...): a caller's arrays are used as given when their shape,
+    dtype, layout and side fit, and refused otherwise (never silently copied)."""
+    from kete_b200.propagation import _out_array
+
+    tpl = np.zeros((3, 5))
+    given = np.empty((3, 5))
+    assert _out_array(given, tpl, (3, 5), np.float64, "out[0]") is given
+    fresh = _out_array(None, tpl, (3, 5), np.float64, "out[0]")
+    assert fresh.shape == (3, 5) and fresh.dtype == np.float64
+    st = _out_array(np.empty(5, dtype=np.int32), tpl, (5,), np.int32, "out[2]")
+    assert st.dtype == np.int32
+    for bad, shape, dtype in ((np.empty((3, 4)), (3, 5), np.float64),
+                              (np.empty((3, 5), dtype=np.float32), (3, 5), np.float64),
+                              (np.empty((5, 3)).T, (3, 5), np.float64),
+                              (np.empty(5, dtype=np.int64), (5,), np.int32),
+                              ([0.0] * 5, (5,), np.float64)):
+        with pytest.raises(ValueError):
+            _out_array(bad, tpl, shape, dtype, "out")
