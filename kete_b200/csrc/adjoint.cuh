@@ -526,9 +526,12 @@ __device__ __forceinline__ int sens_replay_block(const double* c, double tf, dou
 }
 
 // The replays of every checkpoint block of every object at once, before the adjoint sweep:
-// a block's replay depends only on its checkpoint, so one group of 8 lanes per (object,
-// block) re-runs it in parallel and stores its attempt records (a.rec_all) and outcome
-// (a.rep_count: the attempt count, or -1 - status on failure) for the sweep to read.
+// a block's replay depends only on its checkpoint, so groups of 8 lanes re-run the blocks in
+// parallel and store each block's attempt records (a.rec_all) and outcome (a.rep_count: the
+// attempt count, or -1 - status on failure) for the sweep to read.  The grid is persistent:
+// each group takes the next block from a queue (a.rep_first[n + 1]) in the dense order of
+// a.rep_first (sens_replay_offsets_kernel), so groups that finish early take more blocks
+// instead of leaving their thread block's other groups to run alone.
 template <int MINB>
 __global__ void __launch_bounds__(SENS_BLOCK, MINB) nbody_sens_replay_kernel(SensArgs a) {
     __shared__ double s_node[8 * NODE_ROW_S];
@@ -539,36 +542,51 @@ __global__ void __launch_bounds__(SENS_BLOCK, MINB) nbody_sens_replay_kernel(Sen
     const int lane = threadIdx.x & (SG - 1);
     const int warp_lane = threadIdx.x & 31;
     const unsigned gmask = 0xFFu << (warp_lane & ~(SG - 1));
-    const int64_t item = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / SG;
-    const int64_t obj = item / a.ckpt_cap;
-    const int cb = (int)(item % a.ckpt_cap);
-    if (obj >= a.n || a.status[obj] != ST_OK || cb >= a.ckpt_count[obj]) return;
     const int64_t n = a.n;
-    int k = 0;  // the epoch segment holding block cb
-    while (k + 1 < a.n_epochs && a.ckpt_seg[(int64_t)(k + 1) * n + obj] <= cb) ++k;
+    const int64_t total = a.rep_first[n];
+    int32_t* queue = a.rep_first + n + 1;
     double* sb = s_b[threadIdx.x / SG];
     double* se = s_e[threadIdx.x / SG];
     const int comp = lane % 3;
     const double* nrow = s_node + (lane < 7 ? lane + 1 : 7) * NODE_ROW_S;
-    SpkForce F;
-    F.n_force = a.n_force;
-    F.ng.base = a.nongrav ? a.nongrav + obj : nullptr;
-    F.ng.stride = n;
-    F.ng.kind = a.nongrav ? (int)a.nongrav[obj] : 0;
-    F.impact_id = 0;
-    F.min_dist = 1e300;
-    F.min_id = 0;
     extern __shared__ double s_dyn[];
     const FastPlan& plan = a.n_force == c_eph.n_force_planets ? c_eph.fast_planets : c_eph.fast_all;
-    EphCache C{s_dyn + threadIdx.x, SENS_BLOCK,
-               plan.ok && SpkForce::cached_doubles(plan) <= EPH_CACHE,
-               __longlong_as_double(0x7ff8000000000000LL)};
-    double* rec = a.rec_all + (size_t)item * (SENS_CK_ATTEMPTS + 1) * SENS_STRIDE;
-    const double* c = a.ckpt + ((size_t)obj * a.ckpt_cap + cb) * SENS_STRIDE;
-    int na = 0;
-    const int rc = sens_replay_block(c, a.epochs[k], rec, F, nrow, sb, se, lane, comp, gmask,
-                                     warp_lane, a.max_loops * 12, C, na);
-    if (lane == 0) a.rep_count[item] = rc == ST_OK ? na : -1 - rc;
+    for (;;) {
+        int q = 0;
+        if (lane == 0) q = atomicAdd(queue, 1);
+        const int64_t idx = __shfl_sync(gmask, q, 0, SG);
+        if (idx >= total) return;
+        // the object holding block idx: the last o with rep_first[o] <= idx
+        int64_t lo = 0, hi = n;  // rep_first[lo] <= idx < rep_first[hi]
+        while (hi - lo > 1) {
+            const int64_t mid = (lo + hi) >> 1;
+            if (a.rep_first[mid] <= idx) lo = mid;
+            else hi = mid;
+        }
+        const int64_t obj = lo;
+        const int cb = (int)(idx - a.rep_first[obj]);
+        const int64_t item = obj * a.ckpt_cap + cb;  // the sweep's layout of records and counts
+        int k = 0;  // the epoch segment holding block cb
+        while (k + 1 < a.n_epochs && a.ckpt_seg[(int64_t)(k + 1) * n + obj] <= cb) ++k;
+        SpkForce F;
+        F.n_force = a.n_force;
+        F.ng.base = a.nongrav ? a.nongrav + obj : nullptr;
+        F.ng.stride = n;
+        F.ng.kind = a.nongrav ? (int)a.nongrav[obj] : 0;
+        F.impact_id = 0;
+        F.min_dist = 1e300;
+        F.min_id = 0;
+        EphCache C{s_dyn + threadIdx.x, SENS_BLOCK,
+                   plan.ok && SpkForce::cached_doubles(plan) <= EPH_CACHE,
+                   __longlong_as_double(0x7ff8000000000000LL)};
+        double* rec = a.rec_all + (size_t)item * (SENS_CK_ATTEMPTS + 1) * SENS_STRIDE;
+        const double* c = a.ckpt + ((size_t)obj * a.ckpt_cap + cb) * SENS_STRIDE;
+        int na = 0;
+        const int rc = sens_replay_block(c, a.epochs[k], rec, F, nrow, sb, se, lane, comp, gmask,
+                                         warp_lane, a.max_loops * 12, C, na);
+        if (lane == 0) a.rep_count[item] = rc == ST_OK ? na : -1 - rc;
+        __syncwarp(gmask);  // sb, se and the cache are reused by the group's next block
+    }
 }
 
 // REPLAY: the sweep re-runs each block itself (the records did not fit the up-front replay's

@@ -1318,13 +1318,16 @@ int kete_b200_propagate_n_body_adjoint(int64_t n, int n_epochs, const double* ep
         (size_t)n * ckpt_capacity * (SENS_CK_ATTEMPTS + 1) * SENS_STRIDE * sizeof(double);
     a.rec_all = nullptr;
     a.rep_count = nullptr;
+    a.rep_first = nullptr;
     if (g_launch.adjoint_parallel_replay && all_bytes <= ADJOINT_REPLAY_BYTES) {
-        void *ra, *rn;
+        void *ra, *rn, *rf;
         if ((rc = staging(*ds, 35, all_bytes, &ra)) ||
-            (rc = staging(*ds, 36, (size_t)n * ckpt_capacity * sizeof(int32_t), &rn)))
+            (rc = staging(*ds, 36, (size_t)n * ckpt_capacity * sizeof(int32_t), &rn)) ||
+            (rc = staging(*ds, 34, ((size_t)n + 2) * sizeof(int32_t), &rf)))
             return rc;
         a.rec_all = (double*)ra;
         a.rep_count = (int32_t*)rn;
+        a.rep_first = (int32_t*)rf;
     }
     if ((rc = launch_sens_backward(a, st))) return rc;
     return S.finish();

@@ -159,6 +159,9 @@ struct SensArgs {
     double* rec_all;     // n x ckpt_cap x (SENS_CK_ATTEMPTS + 1) x SENS_STRIDE, or null: the
                          // records of every block, replayed up front (adjoint)
     int32_t* rep_count;  // n x ckpt_cap: attempts of each replayed block, -1 - status on failure
+    int32_t* rep_first;  // n + 2 (with rec_all): exclusive prefix sums of the blocks to replay
+                         // per object (the replay takes the blocks in this dense order), then
+                         // the replay's queue counter
     int max_loops;
 };
 int launch_sens_forward(const SensArgs& a, cudaStream_t stream);
