@@ -383,6 +383,13 @@ int kete_b200_set_step_limit(int64_t max_steps);
  * points.  The two agree to about 1e-8 relative. */
 int kete_b200_set_sensitivity_form(int form);
 
+/* Form of the adjoint pass's replays (kete_b200_propagate_n_body_adjoint; no counterpart in the
+ * reference): 0 (default) = every checkpoint block of every object re-run in one parallel
+ * launch before the sweep, when their records fit a bounded library scratch (8 GiB; else as
+ * 1); 1 = the sweep re-runs each block itself, just before transposing it.  Both give the same
+ * gradients bit for bit. */
+int kete_b200_set_adjoint_form(int form);
+
 /* Form of the field checks (kete_b200_fov_check_visible and the schedule built on it; no
  * counterpart in the reference): 0 (default) = a first-order linear screen of every
  * (object, field) pair, then the two-body light-time solve on the pairs that pass, one

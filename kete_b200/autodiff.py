@@ -55,6 +55,16 @@ def set_sensitivity_form(form: int = 0):
     _lib.check(L.kete_b200_set_sensitivity_form(int(form)))
 
 
+def set_adjoint_form(form: int = 0):
+    """Form of the adjoint pass's replays (kete_b200_set_adjoint_form): 0 = every checkpoint
+    block replayed in one parallel launch before the sweep (default, when the records fit the
+    library's bounded scratch); 1 = the sweep re-runs each block just before transposing it.
+    The gradients are identical."""
+    L = _lib.lib()
+    L.kete_b200_set_adjoint_form.argtypes = [ctypes.c_int]
+    _lib.check(L.kete_b200_set_adjoint_form(int(form)))
+
+
 def propagate_n_body_stm_arrays(pos, vel, jd0, epochs, frame=Frames.Ecliptic, center=10,
                                 include_asteroids=False, nongrav=None):
     """States at each epoch and their sensitivities.

@@ -1581,6 +1581,13 @@ int kete_b200_set_sensitivity_form(int form) {
     return 0;
 }
 
+int kete_b200_set_adjoint_form(int form) {
+    if (form != 0 && form != 1) return set_error(KETE_B200_E_ARGUMENT, "adjoint form is 0 or 1");
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_launch.adjoint_parallel_replay = form == 0;
+    return 0;
+}
+
 int kete_b200_set_step_limit(int64_t max_steps) {
     if (max_steps < 0 || max_steps > KETE_B200_STEP_LIMIT_MAX)
         return set_error(KETE_B200_E_ARGUMENT, "step limit out of range");
