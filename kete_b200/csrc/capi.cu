@@ -277,6 +277,9 @@ static void build_fast_plan(int n_force, FastPlan& P) {
         add(g_eph.force[b].slot, b);
     }
     P.n_vel = n;
+    P.sun_vel = -1;
+    for (int it = 0; it < n; ++it)
+        if (P.item[it].kind == FK_SUN) P.sun_vel = it;
     // the others in the reference's order, each centre before the first body chained to it
     int current_parent = -1;
     for (int b = 0; b < n_force && ok; ++b) {
@@ -676,9 +679,22 @@ int nodes_variant_for(int variant, int n_force) {
     return variant;
 }
 
+// The window a variant needs its objects' spans inside (the warp-pooled kernels: the fast
+// plan's), or [-inf, inf].
+void nodes_window(int variant, int n_force, double& lo, double& hi) {
+    const FastPlan& P = n_force == g_eph.n_force_planets ? g_eph.fast_planets : g_eph.fast_all;
+    lo = -INFINITY;
+    hi = INFINITY;
+    if (variant >= 9) {
+        lo = P.lo;
+        hi = P.hi;
+    }
+}
+
 // Everything the allocation-free entry point needs, read under the lock without allocating:
 // the ephemeris must already be resident on the current device.
-int noalloc_snapshot(int include_asteroids, int64_t center, NBodyArgs& a, LaunchConfig& cfg) {
+int noalloc_snapshot(int include_asteroids, int64_t center, NBodyArgs& a, LaunchConfig& cfg,
+                     NodesPlan& plan) {
     std::lock_guard<std::mutex> lk(g_mu);
     if (!g_eph.loaded) return set_error(KETE_B200_E_NO_EPHEMERIS, "no SPK loaded");
     int dev = 0;
@@ -696,6 +712,8 @@ int noalloc_snapshot(int include_asteroids, int64_t center, NBodyArgs& a, Launch
     a.n_force = n_force;
     cfg = g_launch;
     cfg.nodes_variant = nodes_variant_for(cfg.nodes_variant, n_force);
+    plan.general_variant = nodes_variant_for(7, n_force);
+    nodes_window(cfg.nodes_variant, n_force, plan.lo, plan.hi);
     return 0;
 }
 
@@ -932,22 +950,19 @@ int kete_b200_propagate_n_body(int64_t n, const double* pos, const double* vel, 
     if (mode == KETE_B200_MODE_THREAD) {
         if ((rc = launch_nbody_thread(a, g_launch.thread_block, st))) return rc;
     } else if (mode == KETE_B200_MODE_NODES || mode == KETE_B200_MODE_AUTO) {
-        int grid = 0;
         // objects in order of their work (span in orbital periods), most first; scratch holds
         // the queue counter, the work histogram and the processing order
         void* q = nullptr;
         if ((rc = staging(*ds, 31, (ORDER_SCRATCH_HEADER + (size_t)n) * sizeof(int), &q)))
             return rc;
-        if ((rc = launch_span_order(n, a.pos, a.vel, a.jd0, a.jd1, (int*)q, st))) return rc;
-        a.order = (const int32_t*)((int*)q + ORDER_SCRATCH_HEADER);
         const int variant = nodes_variant_for(g_launch.nodes_variant, a.n_force);
-        if (g_launch.nodes_refill) {  // persistent grid taking the next object from the queue
-            a.queue = (int*)q;
-            if ((rc = nodes_grid_size(variant, &grid))) return rc;
-            const int64_t need = (n * 8 + 127) / 128;
-            if (grid > need) grid = (int)need;
-        }
-        if ((rc = launch_nbody_nodes(a, variant, grid, st))) return rc;
+        double lo, hi;
+        nodes_window(variant, a.n_force, lo, hi);
+        if ((rc = launch_span_order(n, a.pos, a.vel, a.jd0, a.jd1, lo, hi, (int*)q, st))) return rc;
+        // refill: a persistent grid taking the next object from the queue
+        if ((rc = launch_nodes_ordered(a, variant, nodes_variant_for(7, a.n_force),
+                                       g_launch.nodes_refill != 0, (int*)q, st)))
+            return rc;
     } else {
         return set_error(KETE_B200_E_ARGUMENT, "unknown propagation mode");
     }
@@ -1543,7 +1558,10 @@ int kete_b200_fov_check_visible(int64_t n_obj, const double* pos, const double* 
         nb.out_vel = (double*)ov;
         nb.status = (int32_t*)os;
         nb.max_loops = g_launch.max_loops;
-        if ((rc = launch_nbody_nodes(nb, nodes_variant_for(g_launch.nodes_variant, nb.n_force), 0, st)))
+        // one group per candidate, with a variant that carries the general ephemeris evaluation
+        // (the warp-pooled kernels take only the objects inside the fast window)
+        const int v = nodes_variant_for(g_launch.nodes_variant, nb.n_force);
+        if ((rc = launch_nbody_nodes(nb, v >= 9 ? nodes_variant_for(7, nb.n_force) : v, 0, st)))
             return rc;
         if ((rc = launch_fov_finish(a, m, (double*)op, (double*)ov, (int32_t*)os, st))) return rc;
     }

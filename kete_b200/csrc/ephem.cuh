@@ -20,8 +20,15 @@ constexpr int MAX_SEG = 96;
 constexpr int MAX_SLOT = 32;
 constexpr int MAX_FORCE = 16;
 constexpr int MAX_CHAIN = 3;
-// span ordering of the persistent N-body grid: buckets and scratch header size (ints)
+// span ordering of the persistent N-body grid: work buckets, and the scratch header (ints):
+// [0] object queue, [1 ..] bucket histogram, then the bucket cursors (ORDER_BUCKETS work
+// buckets and one last bucket for the objects whose span leaves the fast plan's window),
+// ORDER_RANGE: {0, objects inside the window, n}, ORDER_QUEUE2: the queue of the objects
+// outside it; the processing order follows the header
 constexpr int ORDER_BUCKETS = 120;
+constexpr int ORDER_ALL_BUCKETS = ORDER_BUCKETS + 1;
+constexpr int ORDER_RANGE = 1 + 2 * ORDER_ALL_BUCKETS;
+constexpr int ORDER_QUEUE2 = ORDER_RANGE + 3;
 constexpr int EPH_CACHE = 38;  // body-position cache, doubles per lane (the planets need 36)
 
 constexpr int ORDER_SCRATCH_HEADER = 256;
@@ -93,7 +100,8 @@ struct FastItem {
 struct FastPlan {
     double lo, hi;
     int32_t n_items, ok;
-    int32_t n_vel, pad_;
+    int32_t n_vel;
+    int32_t sun_vel;  // index of the Sun among the first n_vel items (-1: no Sun)
     FastItem item[MAX_ITEMS];
 };
 

@@ -85,9 +85,11 @@ struct NonGrav {
     __device__ __forceinline__ double p(int k) const { return __ldg(base + (int64_t)k * stride); }
 };
 
-// Returns the non-gravitational acceleration (added by the caller), so that no array of the
-// caller has its address taken by this out-of-line function.
-static __device__ __noinline__ double3 nongrav_accel(const NonGrav ng, const double3 rp, const double3 rv) {
+// The non-gravitational acceleration (NonGravModel::add_acceleration, nongrav.rs:114-157)
+// at the Sun-relative position rp and velocity rv, returned for the caller to add.  DT =
+// false: the JPL comet model's delay dt is known to be 0 (no two-body back-propagation).
+template <bool DT>
+__device__ __forceinline__ double3 nongrav_terms(const NonGrav ng, const double3 rp, const double3 rv) {
     const double pos_in[3] = {rp.x, rp.y, rp.z};
     const double vel[3] = {rv.x, rv.y, rv.z};
     double acc[3] = {0.0, 0.0, 0.0};
@@ -118,7 +120,7 @@ static __device__ __noinline__ double3 nongrav_accel(const NonGrav ng, const dou
                     t_vec[0] * pn[1] - t_vec[1] * pn[0]};
     const double nnrm = norm3(nv[0], nv[1], nv[2]);
     const double n_vec[3] = {nv[0] / nnrm, nv[1] / nnrm, nv[2] / nnrm};
-    if (dt != 0.0) {
+    if (DT && dt != 0.0) {
         double p2[3] = {pos[0], pos[1], pos[2]}, v2[3] = {vel[0], vel[1], vel[2]};
         if (analytic_2_body(-dt, p2, v2) == ST_OK) {
             pos[0] = p2[0];
@@ -135,6 +137,12 @@ static __device__ __noinline__ double3 nongrav_accel(const NonGrav ng, const dou
 #pragma unroll
     for (int i = 0; i < 3; ++i) acc[i] += n_vec[i] * (scale * a3);
     return make_double3(acc[0], acc[1], acc[2]);
+}
+
+// nongrav_terms out of line: its arrays are its own, and the force loops that call it do not
+// carry its registers.
+static __device__ __noinline__ double3 nongrav_accel(const NonGrav ng, const double3 rp, const double3 rv) {
+    return nongrav_terms<true>(ng, rp, rv);
 }
 
 // -------------------------------------------------------------------------------------------
@@ -216,10 +224,10 @@ struct SpkForceT {
     // non-gravitational term relative to the Sun, acceleration.rs:161-165), given the relative
     // position rp and velocity rv, r2 = |rp|^2 and ir = rsqrt(r2).  VEL = false serves the
     // bodies whose velocity does not enter the force (no relativistic or non-gravitational
-    // term): rv is then not read.  Callers that evaluate several bodies compute their
-    // reciprocal square roots together (independent chains) before summing the terms in the
-    // reference's order.
-    template <bool VEL = true>
+    // term): rv is then not read.  NG = false leaves the non-gravitational term to the caller.
+    // Callers that evaluate several bodies compute their reciprocal square roots together
+    // (independent chains) before summing the terms in the reference's order.
+    template <bool VEL = true, bool NG = true>
     __device__ __forceinline__ int body_terms(const ForceEntry& fe, bool exact, const double rp[3],
                                               const double rv[3], double r2, double ir,
                                               double& acc0, double& acc1, double& acc2) {
@@ -263,7 +271,7 @@ struct SpkForceT {
             acc0 += jx;
             acc1 += rc * jy - rs * jz;
             acc2 += rs * jy + rc * jz;
-            if (fe.kind == FK_SUN && ng.kind != 0) {
+            if (NG && fe.kind == FK_SUN && ng.kind != 0) {
                 const double3 na = nongrav_accel(ng, make_double3(rp[0], rp[1], rp[2]),
                                                  make_double3(rv[0], rv[1], rv[2]));
                 acc0 += na.x;
@@ -285,7 +293,7 @@ struct SpkForceT {
     // body_terms for the body at bp (velocity bv) seen from (x, v).  Distances use one
     // reciprocal square root per body: r = r2 * rsqrt(r2) and r^-3 = rsqrt(r2)^3 replace the
     // reference's sqrt and 1/(r*r*r) (a few ulp apart).
-    template <bool VEL = true>
+    template <bool VEL = true, bool NG = true>
     __device__ __forceinline__ int body(const ForceEntry& fe, bool exact, const double x[3],
                                         const double v[3], const double bp[3], const double bv[3],
                                         double& acc0, double& acc1, double& acc2) {
@@ -297,7 +305,7 @@ struct SpkForceT {
             rv[2] = v[2] - bv[2];
         }
         const double r2 = rp[0] * rp[0] + rp[1] * rp[1] + rp[2] * rp[2];
-        return body_terms<VEL>(fe, exact, rp, rv, r2, rsqrt(r2), acc0, acc1, acc2);
+        return body_terms<VEL, NG>(fe, exact, rp, rv, r2, rsqrt(r2), acc0, acc1, acc2);
     }
 
     // Fast path: the host-verified window where every body's first segment covers t and all

@@ -63,6 +63,8 @@ struct NBodyArgs {
     int max_loops;        // step-loop bound per object (ST_TIMEOUT beyond)
     int* queue;           // refill counter for the node kernel (null: one object per group)
     const int32_t* order; // processing order (permutation of 0..n-1) or null
+    const int* range;     // device {first, end}: the node kernel takes order[first .. end)
+                          // (null: order[0 .. n))
 };
 
 int launch_two_body(int64_t n, const double* pos, const double* vel, const double* jd0,
@@ -84,8 +86,15 @@ int preload_order_kernels();
 // resolve the allocation-free entry point's scratch address on the current device
 int noalloc_prepare();
 int launch_span_order(int64_t n, const double* pos, const double* vel, const double* jd0,
-                      const double* jd1, int* scratch,
+                      const double* jd1, double lo, double hi, int* scratch,
                       cudaStream_t stream);
+// The node kernels over the processing order that launch_span_order wrote into scratch
+// (variant as launch_nbody_nodes; refill: persistent grid with the object queue).  A
+// warp-pooled variant integrates the objects inside the fast plan's window and
+// general_variant (a form with the general ephemeris evaluation) the others, in a second
+// launch; every other variant takes the whole order in one launch.
+int launch_nodes_ordered(NBodyArgs a, int variant, int general_variant, bool refill,
+                         int* scratch, cudaStream_t stream);
 
 // launch configuration chosen by the tuner (kete_b200_set_launch_config)
 struct LaunchConfig {
@@ -103,7 +112,14 @@ struct LaunchConfig {
 // scratch bound of the adjoint's up-front replay (every block's attempt records)
 constexpr size_t ADJOINT_REPLAY_BYTES = size_t(8) << 30;
 LaunchConfig& launch_config();
-int noalloc_snapshot(int include_asteroids, int64_t center, NBodyArgs& a, LaunchConfig& cfg);
+// What the allocation-free entry point launches: the node variant in cfg.nodes_variant, the
+// variant with the general ephemeris evaluation, and the window of launch_span_order.
+struct NodesPlan {
+    int general_variant;
+    double lo, hi;
+};
+int noalloc_snapshot(int include_asteroids, int64_t center, NBodyArgs& a, LaunchConfig& cfg,
+                     NodesPlan& plan);
 int launch_radau_central(int64_t n, const double* pos, const double* vel, const double* t0,
                          const double* t1, double* out_pos, double* out_vel, int32_t* status,
                          cudaStream_t stream);

@@ -21,7 +21,7 @@
 // (different streams, or different host threads) race on it and must be serialized by the
 // caller, as must a concurrent SPK load or kete_b200_set_launch_config on another thread
 // (the call reads the ephemeris table and launch configuration, then enqueues).  The header
-// that must start at zero (queue, histogram, cursors) is cleared by every call.
+// that must start at zero (queues, histogram, cursors) is cleared by every call.
 #include <cstring>
 #include <mutex>
 
@@ -87,7 +87,8 @@ extern "C" int kete_b200_propagate_n_body_noalloc(
     NBodyArgs a;
     std::memset(&a, 0, sizeof a);
     LaunchConfig cfg;
-    int rc = noalloc_snapshot(include_asteroids, center, a, cfg);
+    NodesPlan plan;
+    int rc = noalloc_snapshot(include_asteroids, center, a, cfg, plan);
     if (rc) return rc;
     int* scratch = nullptr;
     if ((rc = noalloc_scratch(&scratch))) return rc;
@@ -108,12 +109,6 @@ extern "C" int kete_b200_propagate_n_body_noalloc(
     a.min_dist = min_dist;
     a.counters = counters;
     a.max_loops = cfg.max_loops;
-    if ((rc = launch_span_order(n, pos, vel, jd0, jd1, scratch, st))) return rc;
-    a.queue = scratch;
-    a.order = (const int32_t*)(scratch + ORDER_SCRATCH_HEADER);
-    int grid = 0;
-    if ((rc = nodes_grid_size(cfg.nodes_variant, &grid))) return rc;
-    const int64_t need = (n * 8 + 127) / 128;
-    if (grid > need) grid = (int)need;
-    return launch_nbody_nodes(a, cfg.nodes_variant, grid, st);
+    if ((rc = launch_span_order(n, pos, vel, jd0, jd1, plan.lo, plan.hi, scratch, st))) return rc;
+    return launch_nodes_ordered(a, cfg.nodes_variant, plan.general_variant, true, scratch, st);
 }

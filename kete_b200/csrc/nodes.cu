@@ -4,6 +4,8 @@
 // instantiations compile in parallel with the other kernels.
 #include <atomic>
 
+#include "../../include/kete_b200.h"
+
 #include "common.cuh"
 #include "forces.cuh"
 #include "internal.h"
@@ -62,6 +64,10 @@ static int allow_dyn_smem(int variant) {
 
 int launch_nbody_nodes(const NBodyArgs& a, int variant, int grid, cudaStream_t stream) {
     if (a.n <= 0) return 0;
+    if (variant >= 9 && !a.range)
+        return set_error(KETE_B200_E_ARGUMENT,
+                         "the warp-pooled node kernels take the window split of the processing "
+                         "order (launch_nodes_ordered)");
     const int block = NODES_BLOCK;
     if (grid <= 0) grid = (int)((a.n * NODE_G + block - 1) / block);
     int rc = allow_dyn_smem(variant);
@@ -80,6 +86,38 @@ int launch_nbody_nodes(const NBodyArgs& a, int variant, int grid, cudaStream_t s
         default: nbody_nodes_kernel<1, false><<<grid, block, 0, stream>>>(a); break;
     }
     return launched(1, "nbody_nodes_kernel launch");
+}
+
+// Persistent grid of a variant, capped at one lane group per object.
+static int refill_grid(int variant, int64_t n, int* grid) {
+    int rc = nodes_grid_size(variant, grid);
+    if (rc) return rc;
+    const int64_t need = (n * NODE_G + NODES_BLOCK - 1) / NODES_BLOCK;
+    if (*grid > need) *grid = (int)need;
+    return 0;
+}
+
+int launch_nodes_ordered(NBodyArgs a, int variant, int general_variant, bool refill,
+                         int* scratch, cudaStream_t stream) {
+    a.order = (const int32_t*)(scratch + ORDER_SCRATCH_HEADER);
+    int grid = 0, rc = 0;
+    if (variant < 9) {  // one launch over the whole order
+        a.range = nullptr;
+        a.queue = refill ? scratch : nullptr;
+        if (refill && (rc = refill_grid(variant, a.n, &grid))) return rc;
+        return launch_nbody_nodes(a, variant, grid, stream);
+    }
+    // objects inside the window: the pooled kernel; the others: the general form.  The counts
+    // are on the device, so both grids cover every object (groups past their part exit).
+    a.range = scratch + ORDER_RANGE;
+    a.queue = refill ? scratch : nullptr;
+    if (refill && (rc = refill_grid(variant, a.n, &grid))) return rc;
+    if ((rc = launch_nbody_nodes(a, variant, grid, stream))) return rc;
+    a.range = scratch + ORDER_RANGE + 1;
+    a.queue = refill ? scratch + ORDER_QUEUE2 : nullptr;
+    grid = 0;
+    if (refill && (rc = refill_grid(general_variant, a.n, &grid))) return rc;
+    return launch_nbody_nodes(a, general_variant, grid, stream);
 }
 
 int preload_nodes_kernels() {

@@ -148,7 +148,12 @@ __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_nodes_kernel(NBodyArg
         } else {
             k = (obj < 0) ? group : a.n;  // one object per group
         }
-        if (k >= a.n) return false;
+        if (a.range) {  // a part of the order (launch_nodes_ordered)
+            k += a.range[0];
+            if (k >= a.range[1]) return false;
+        } else if (k >= a.n) {
+            return false;
+        }
         obj = a.order ? a.order[k] : k;
         const int64_t n = a.n;
         t = a.jd0[obj];

@@ -20,8 +20,17 @@
 // (lane 7 evaluates the step end during each corrector iteration and supplies the exact
 // evaluation of the accepted step), the predicted corrector start and the compensated state
 // update; the cached positions are rounded to doubles before the force terms read them, so
-// results agree with the uncached forms to rounding.  Outside the ephemeris window of the fast
-// plan a lane evaluates the force from scratch (SpkForce::eval), as every other form does.
+// results agree with the uncached forms to rounding.
+//
+// The kernel carries no general ephemeris evaluation: the host orders the objects whose span
+// leaves the fast plan's window after the others and integrates those with a form that has
+// it (launch_nodes_ordered).  An out-of-line call makes the caller keep its live registers
+// across it; with the general evaluation, the non-gravitational term (inside the force loop)
+// and the centre changes as calls this kernel spilled about a quarter of a kilobyte per lane
+// at 128 registers.  Now the centre changes at an object's start and end are inlined, and the
+// non-gravitational term (relative to the Sun) is added after the bodies' terms are summed,
+// where few values are live: inline for the JPL comet model without delay, and as the one
+// call for the delayed and dust models.
 #pragma once
 #include "common.cuh"
 #include "forces.cuh"
@@ -160,7 +169,8 @@ __device__ __forceinline__ void pool_records(unsigned M, int warp_lane, int warp
 // The force at (x, v) from a lane's cached body states, summed in the fast plan's order
 // (eval_fast's): the velocity items, then the others, with the chained bodies offset by the
 // centre kept before them.  One body at a time: the kernel is bound by its registers, and
-// forming several bodies' terms together spills more than it hides.
+// forming several bodies' terms together spills more than it hides.  The non-gravitational
+// term is not included (the kernel adds it after this sum).
 __device__ __forceinline__ int pool_forces(const FastPlan& P, SpkForce& F, bool exact,
                                            const double x[3], const double v[3],
                                            const double* cache, double out[3]) {
@@ -175,7 +185,7 @@ __device__ __forceinline__ int pool_forces(const FastPlan& P, SpkForce& F, bool 
         const double bv[3] = {cache[(k + 3) * NODES_BLOCK], cache[(k + 4) * NODES_BLOCK],
                               cache[(k + 5) * NODES_BLOCK]};
         const ForceEntry fe{A.mass, A.radius, 0, A.kind, A.naif_id, 0};
-        const int rc = F.body<true>(fe, exact, x, v, bp, bv, acc0, acc1, acc2);
+        const int rc = F.body<true, false>(fe, exact, x, v, bp, bv, acc0, acc1, acc2);
         if (rc != ST_OK) return rc;
     }
     const double zero[3] = {0.0, 0.0, 0.0};
@@ -205,44 +215,14 @@ __device__ __forceinline__ int pool_forces(const FastPlan& P, SpkForce& F, bool 
     return ST_OK;
 }
 
-// The cold paths of the pooled kernel as out-of-line calls, so that their register needs
-// (the segment search and the record types of SpkForce::eval, the centre chains) do not
-// shape the allocation of the hot loop.  Arguments and results travel by value: no array of
-// the caller has its address taken.
-struct SlowForce {
-    double a0, a1, a2, min_dist;
-    int rc, impact_id, min_id;
-};
-
-static __device__ __noinline__ SlowForce pool_slow_eval(int n_force, NonGrav ng, bool exact,
-                                                       double t, double3 x, double3 v,
-                                                       double min_dist, int min_id) {
-    SpkForce F;
-    F.n_force = n_force;
-    F.ng = ng;
-    F.impact_id = 0;
-    F.min_dist = min_dist;
-    F.min_id = min_id;
-    const double xe[3] = {x.x, x.y, x.z}, ve[3] = {v.x, v.y, v.z};
-    double ev[3] = {0.0, 0.0, 0.0};
-    SlowForce r;
-    r.rc = F.eval(exact, t, xe, ve, ev);
-    r.a0 = ev[0];
-    r.a1 = ev[1];
-    r.a2 = ev[2];
-    r.min_dist = F.min_dist;
-    r.impact_id = F.impact_id;
-    r.min_id = F.min_id;
-    return r;
-}
-
+// to_ssb_equatorial (inward = true) or from_ssb_equatorial on values (lane 0 at an object's
+// start and end).
 struct ChainedState {
     double3 p, v;
     int rc;
 };
 
-// to_ssb_equatorial (inward = true) or from_ssb_equatorial, out of line
-static __device__ __noinline__ ChainedState pool_change_center(bool inward, double t, int frame,
+__device__ __forceinline__ ChainedState pool_change_center(bool inward, double t, int frame,
                                                               CenterChain ch, double3 p,
                                                               double3 v) {
     double pp[3] = {p.x, p.y, p.z}, vv[3] = {v.x, v.y, v.z};
@@ -355,7 +335,8 @@ __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_pool_kernel(NBodyArgs
             k = first ? group : a.n;  // one object per group
         }
         first = false;
-        if (k >= a.n) return false;
+        k += a.range[0];  // the objects inside the fast window (launch_nodes_ordered)
+        if (k >= a.range[1]) return false;
         obj = a.order ? a.order[k] : k;
         int frc = ST_OK;
         if (lane == 0) {
@@ -452,37 +433,11 @@ __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_pool_kernel(NBodyArgs
             finish(ST_TIMEOUT);
             active = false;
         }
-        // ---- evaluation point of this lane ----
+        // ---- evaluation time of this lane (the position and velocity follow the record
+        // pass, so that they are not live across its recurrences) ----
         const bool iter_round = phase == PH_ITER;
-        double te = 0.0, xe[3] = {0.0, 0.0, 0.0}, ve[3] = {0.0, 0.0, 0.0};
-        if (active) {
-            if (!iter_round) {
-                te = st[ST_T];
-#pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    xe[c] = st[ST_X + c];
-                    ve[c] = st[ST_V + c];
-                }
-            } else {
-                const double f = nrow[14], frac2 = nrow[15];
-                const double h = st[ST_H];
-                const double h2 = h * h;
-#pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    double bw = 0.0, bu = 0.0;
-#pragma unroll
-                    for (int k = 0; k < 7; ++k) {
-                        const double bck = sb[7 * c + k];
-                        bw += nrow[k] * bck;
-                        bu += nrow[7 + k] * bck;
-                    }
-                    const double ac = st[ST_A + c];
-                    xe[c] = st[ST_X + c] + f * st[ST_V + c] * h + frac2 * h2 * (ac / 2.0 + bw);
-                    ve[c] = st[ST_V + c] + f * h * (ac + bu);
-                }
-                te = st[ST_T] + f * h;
-            }
-        }
+        double te = 0.0;
+        if (active) te = iter_round ? st[ST_T] + nrow[14] * st[ST_H] : st[ST_T];
         const bool fast = active && use_pool && te >= plan.lo && te <= plan.hi;
         const bool need = fast && te != cache_t;
         // ---- the warp's record evaluations for every lane at a new time ----
@@ -498,25 +453,54 @@ __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_pool_kernel(NBodyArgs
             if (need) cache_t = te;
         }
         if (!active) continue;
+        double xe[3], ve[3];
+        if (!iter_round) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                xe[c] = st[ST_X + c];
+                ve[c] = st[ST_V + c];
+            }
+        } else {
+            const double f = nrow[14], frac2 = nrow[15];
+            const double h = st[ST_H];
+            const double h2 = h * h;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                double bw = 0.0, bu = 0.0;
+#pragma unroll
+                for (int k = 0; k < 7; ++k) {
+                    const double bck = sb[7 * c + k];
+                    bw += nrow[k] * bck;
+                    bu += nrow[7 + k] * bck;
+                }
+                const double ac = st[ST_A + c];
+                xe[c] = st[ST_X + c] + f * st[ST_V + c] * h + frac2 * h2 * (ac / 2.0 + bw);
+                ve[c] = st[ST_V + c] + f * h * (ac + bu);
+            }
+        }
         const bool exact = !iter_round || se_lane;
         const double saved_min = F.min_dist;
         const int32_t saved_min_id = F.min_id;
-        double ev[3];
-        int erc;
+        double ev[3] = {0.0, 0.0, 0.0};
+        int erc = ST_DAF_LIMITS;  // outside the window: unreachable, the host keeps those objects out
         if (fast) {
             erc = pool_forces(plan, F, exact, xe, ve, cache, ev);
-        } else {
-            const SlowForce s = pool_slow_eval(F.n_force, F.ng, exact, te,
-                                               make_double3(xe[0], xe[1], xe[2]),
-                                               make_double3(ve[0], ve[1], ve[2]), F.min_dist,
-                                               F.min_id);
-            erc = s.rc;
-            ev[0] = s.a0;
-            ev[1] = s.a1;
-            ev[2] = s.a2;
-            F.min_dist = s.min_dist;
-            F.min_id = s.min_id;
-            if (erc == ST_IMPACT) F.impact_id = s.impact_id;
+            if (F.ng.kind != 0 && erc == ST_OK && plan.sun_vel >= 0) {
+                // non_grav_accel relative to the Sun (acceleration.rs:161-165)
+                // (inline for the JPL comet model without delay; out of line otherwise)
+                const double* sc = cache + 6 * plan.sun_vel * NODES_BLOCK;
+                const double3 rp = make_double3(xe[0] - sc[0], xe[1] - sc[NODES_BLOCK],
+                                                xe[2] - sc[2 * NODES_BLOCK]);
+                const double3 rv = make_double3(ve[0] - sc[3 * NODES_BLOCK],
+                                                ve[1] - sc[4 * NODES_BLOCK],
+                                                ve[2] - sc[5 * NODES_BLOCK]);
+                const double3 na = (F.ng.kind == 1 && F.ng.p(9) == 0.0)
+                                       ? nongrav_terms<false>(F.ng, rp, rv)
+                                       : nongrav_accel(F.ng, rp, rv);
+                ev[0] += na.x;
+                ev[1] += na.y;
+                ev[2] += na.z;
+            }
         }
         // any lane of the group failing fails the group (only DAF limits / impacts occur);
         // the step-end lane's outcome only counts once the iteration converges

@@ -71,6 +71,50 @@ def test_batched_mix_five_year_spans_vs_oracle(gpu, oracle_spk):
         tune.set_config()
 
 
+def test_pooled_forms_split_at_the_fast_window(gpu, oracle, spk_path, tmp_path):
+    """The warp-pooled kernels (variants 9, 10) evaluate the ephemeris only from the fast
+    plan's records, whose window is the coverage of every body's first segment.  With the
+    ephemeris in two files (two segments per body, meeting at JD 2460000.5), the objects whose
+    span crosses into the other file's coverage are ordered after the others and integrated by
+    the form with the general evaluation in a second launch.  Objects start on both sides of
+    the boundary, so that both launches have work whichever segment comes first; every object
+    agrees with the oracle, which searches the segments for every evaluation."""
+    from kete_b200 import tune
+
+    a, b = str(tmp_path / "early.bsp"), str(tmp_path / "late.bsp")
+    synthetic.write_synthetic_spk(a, jd_start=2459000.5, jd_end=2460000.5)
+    synthetic.write_synthetic_spk(b, jd_start=2460000.5, jd_end=2461000.5)
+    n = 400
+    pos, vel, ng = synthetic.mixed(n, seed=83)
+    rng = np.random.default_rng(84)
+    jd0 = np.where(np.arange(n) % 2 == 0, 2459700.5, 2460300.5)
+    jd1 = jd0 + rng.uniform(-600.0, 600.0, n)
+    crossing = (np.minimum(jd0, jd1) < 2460000.5) & (np.maximum(jd0, jd1) > 2460000.5)
+    assert 0.1 < crossing.mean() < 0.9
+    try:
+        gpu.spice.kernel_reload([a, b])
+        oracle.spk_reset()
+        for f in (a, b):
+            oracle.spk_load_bytes(open(f, "rb").read())
+        op, ov, ost, _, _ = oracle.propagate_n_body(pos, vel, jd0, jd1, ng=ng)
+        assert (ost == 0).all()
+        for cfg in (dict(mode=2, variant=10, refill=1), dict(mode=2, variant=9, refill=0),
+                    dict(mode=2, variant=7, refill=1)):
+            tune.set_config(**cfg)
+            p, v, st, det = gpu.propagate_n_body_arrays(pos, vel, jd0, jd1, nongrav=ng, mode=2,
+                                                        with_details=True)
+            far = det["min_dist"] >= 0.01
+            assert (st == 0).all(), cfg
+            err = np.linalg.norm(p - op, axis=0)
+            assert err[far].max() < 1e-9, (cfg, err[far].max())
+            assert far.mean() > 0.9
+    finally:  # restore the session ephemeris for the tests that follow
+        tune.set_config()
+        gpu.spice.kernel_reload([spk_path])
+        oracle.spk_reset()
+        oracle.spk_load_bytes(open(spk_path, "rb").read())
+
+
 def test_step_limit_returns_timeout(gpu, oracle_spk):
     from kete_b200 import tune
 

@@ -356,4 +356,6 @@ def test_kernel_launch_counter(gpu):
     gpu.propagate_n_body_arrays(pos, vel, jd0, jd1, mode=2)
     c2 = count()
     assert c1 - c0 == 1
-    assert c2 - c1 in (1, 4)  # node kernel, plus the three ordering kernels with refill
+    # the three ordering kernels, then the node kernel (the warp-pooled forms launch two: the
+    # objects inside the fast ephemeris window, then the others)
+    assert c2 - c1 in (4, 5)
