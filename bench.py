@@ -82,11 +82,8 @@ NODE_TRAFFIC = {
     ("nbody_mixed_1m", 7, 1): {"bytes_per_object": (13_601_536 + 882_944) / 100_000,
                                "fp64_pipe": 0.217,
                                "captured": "one launch on a 100,000-object sample of the workload"},
-    ("nbody_mixed_1m", 9, 1): {"bytes_per_object": (13_523_968 + 951_296) / 100_000,
-                               "fp64_pipe": 0.241,
-                               "captured": "one launch on a 100,000-object sample of the workload"},
-    ("nbody_mixed_1m", 10, 1): {"bytes_per_object": (13_684_736 + 806_656) / 100_000,
-                                "fp64_pipe": 0.254,
+    ("nbody_mixed_1m", 10, 1): {"bytes_per_object": (13_445_376 + 390_400) / 100_000,
+                                "fp64_pipe": 0.291,
                                 "captured": "one launch on a 100,000-object sample of the workload"},
 }
 

@@ -358,8 +358,9 @@ int kete_b200_fp64_probe(int64_t iters, double* tflops, float* ms);
  * for the form whose lane groups start their steps together and reuse the bodies' positions
  * across a step's corrector iterations; 9 and 10 (168 / 128 registers) for the form that
  * keeps that cache but lets the four objects of a warp step independently, the whole warp
- * sharing each round's ephemeris-record evaluations; default 7; nodes_refill: 1 = persistent
- * grid whose
+ * sharing each round's ephemeris-record evaluations (objects whose span leaves the window
+ * where every perturber's first segment applies are integrated by form 7 in a second
+ * launch); default 7; nodes_refill: 1 = persistent grid whose
  * lane groups take objects from a queue as they finish; thread_block: block size of the
  * one-object-per-thread kernel. */
 int kete_b200_set_launch_config(int nodes_variant, int nodes_refill, int thread_block);
