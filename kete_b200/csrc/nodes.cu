@@ -2,6 +2,7 @@
 // warp-pooled form of radau_pool.cuh): every register-cap / step-end / warp-synchronous /
 // pooled instantiation the tuner chooses from.  Its own translation unit so the
 // instantiations compile in parallel with the other kernels.
+#include <algorithm>
 #include <atomic>
 
 #include "../../include/kete_b200.h"
@@ -107,12 +108,18 @@ int launch_nodes_ordered(NBodyArgs a, int variant, int general_variant, bool ref
         if (refill && (rc = refill_grid(variant, a.n, &grid))) return rc;
         return launch_nbody_nodes(a, variant, grid, stream);
     }
-    // objects inside the window: the pooled kernel; the others: the general form.  The counts
-    // are on the device, so both grids cover every object (groups past their part exit).
+    // objects inside the window: the pooled kernel between its centre-change kernels; the
+    // others: the general form.  The counts are on the device, so every grid covers every
+    // object (threads and groups past their part exit).
     a.range = scratch + ORDER_RANGE;
     a.queue = refill ? scratch : nullptr;
+    const int64_t cgrid = std::min<int64_t>((a.n + 255) / 256, 1184);
+    pool_prepare_kernel<<<(int)cgrid, 256, 0, stream>>>(a);
+    if ((rc = launched(1, "pool_prepare_kernel launch"))) return rc;
     if (refill && (rc = refill_grid(variant, a.n, &grid))) return rc;
     if ((rc = launch_nbody_nodes(a, variant, grid, stream))) return rc;
+    pool_finish_kernel<<<(int)cgrid, 256, 0, stream>>>(a);
+    if ((rc = launched(1, "pool_finish_kernel launch"))) return rc;
     a.range = scratch + ORDER_RANGE + 1;
     a.queue = refill ? scratch + ORDER_QUEUE2 : nullptr;
     grid = 0;
@@ -128,6 +135,8 @@ int preload_nodes_kernels() {
             return rc;
         if ((rc = allow_dyn_smem(v))) return rc;
     }
+    for (const void* f : {(const void*)pool_prepare_kernel, (const void*)pool_finish_kernel})
+        if ((rc = cuda_check(cudaFuncGetAttributes(&fa, f), "load node kernels"))) return rc;
     return 0;
 }
 

@@ -27,10 +27,13 @@
 // it (launch_nodes_ordered).  An out-of-line call makes the caller keep its live registers
 // across it; with the general evaluation, the non-gravitational term (inside the force loop)
 // and the centre changes as calls this kernel spilled about a quarter of a kilobyte per lane
-// at 128 registers.  Now the centre changes at an object's start and end are inlined, and the
+// at 128 registers.  Now the centre changes at an object's start and end run in kernels of
+// their own before and after (pool_prepare_kernel, pool_finish_kernel), and the
 // non-gravitational term (relative to the Sun) is added after the bodies' terms are summed,
 // where few values are live: inline for the JPL comet model without delay, and as the one
-// call for the delayed and dust models.
+// call for the delayed model and dust.  (Without that call, with the delayed comets sent to
+// the general form instead, the kernel needs 145 registers and spills nothing at 128, but
+// it measured 1.7% slower on the batched workload.)
 #pragma once
 #include "common.cuh"
 #include "forces.cuh"
@@ -215,22 +218,59 @@ __device__ __forceinline__ int pool_forces(const FastPlan& P, SpkForce& F, bool 
     return ST_OK;
 }
 
-// to_ssb_equatorial (inward = true) or from_ssb_equatorial on values (lane 0 at an object's
-// start and end).
-struct ChainedState {
-    double3 p, v;
-    int rc;
-};
+// The centre and frame changes of the pooled kernel's objects, in kernels of their own (one
+// thread per object of the part order[range[0] .. range[1])): their code (a general state
+// query of the centre's chain) runs once per object, and inside the step loop's kernel it
+// cost instruction-cache misses to every warp of the SM.
+//
+// Before the integration: the checks of the inputs and to_ssb_equatorial (mod.rs:79-80) at
+// the epoch; the barycentric equatorial state goes to the output arrays, the outcome to
+// status, where nbody_pool_kernel reads both.
+static __global__ void pool_prepare_kernel(NBodyArgs a) {
+    const int64_t first = a.range[0], end = a.range[1], n = a.n;
+    for (int64_t k = first + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < end;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t obj = a.order[k];
+        const double t0 = a.jd0[obj];
+        double p[3] = {a.pos[obj], a.pos[n + obj], a.pos[2 * n + obj]};
+        double v[3] = {a.vel[obj], a.vel[n + obj], a.vel[2 * n + obj]};
+        const bool finite = isfinite(p[0]) && isfinite(p[1]) && isfinite(p[2]) &&
+                            isfinite(v[0]) && isfinite(v[1]) && isfinite(v[2]) && isfinite(t0);
+        int rc = finite ? ST_OK : ST_VALUE_ERROR;
+        if (rc == ST_OK && (a.chain.len > 0 || a.frame == FRAME_ECLIPTIC))
+            rc = to_ssb_equatorial(t0, a.frame, a.chain, p, v);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            a.out_pos[c * n + obj] = p[c];
+            a.out_vel[c * n + obj] = v[c];
+        }
+        a.status[obj] = rc;
+    }
+}
 
-__device__ __forceinline__ ChainedState pool_change_center(bool inward, double t, int frame,
-                                                              CenterChain ch, double3 p,
-                                                              double3 v) {
-    double pp[3] = {p.x, p.y, p.z}, vv[3] = {v.x, v.y, v.z};
-    ChainedState r;
-    r.rc = inward ? to_ssb_equatorial(t, frame, ch, pp, vv) : from_ssb_equatorial(t, frame, ch, pp, vv);
-    r.p = make_double3(pp[0], pp[1], pp[2]);
-    r.v = make_double3(vv[0], vv[1], vv[2]);
-    return r;
+// After it: from_ssb_equatorial (mod.rs:107-116) at the target epoch for every object that
+// arrived; a failure there gives NaN and its status, as in the other forms.
+static __global__ void pool_finish_kernel(NBodyArgs a) {
+    const int64_t first = a.range[0], end = a.range[1], n = a.n;
+    if (!(a.chain.len > 0 || a.frame == FRAME_ECLIPTIC)) return;
+    for (int64_t k = first + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < end;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t obj = a.order[k];
+        if (a.status[obj] != ST_OK) continue;
+        double p[3] = {a.out_pos[obj], a.out_pos[n + obj], a.out_pos[2 * n + obj]};
+        double v[3] = {a.out_vel[obj], a.out_vel[n + obj], a.out_vel[2 * n + obj]};
+        const int rc = from_ssb_equatorial(a.jd1[obj], a.frame, a.chain, p, v);
+        if (rc != ST_OK) {
+            const double nan = __longlong_as_double(0x7ff8000000000000LL);
+            p[0] = p[1] = p[2] = v[0] = v[1] = v[2] = nan;
+            a.status[obj] = rc;
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            a.out_pos[c * n + obj] = p[c];
+            a.out_vel[c * n + obj] = v[c];
+        }
+    }
 }
 
 // Dynamic shared memory of the pooled kernel: the body cache.
@@ -340,23 +380,16 @@ __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_pool_kernel(NBodyArgs
         obj = a.order ? a.order[k] : k;
         int frc = ST_OK;
         if (lane == 0) {
+            // the state at the epoch as pool_prepare_kernel left it (barycentric equatorial,
+            // in the output arrays) and the outcome of its checks
             const int64_t n = a.n;
-            const double t0 = a.jd0[obj];
-            double3 p = make_double3(a.pos[obj], a.pos[n + obj], a.pos[2 * n + obj]);
-            double3 v = make_double3(a.vel[obj], a.vel[n + obj], a.vel[2 * n + obj]);
-            const bool finite = isfinite(p.x) && isfinite(p.y) && isfinite(p.z) &&
-                                isfinite(v.x) && isfinite(v.y) && isfinite(v.z) && isfinite(t0);
-            if (!finite) frc = ST_VALUE_ERROR;
-            if (frc == ST_OK && (a.chain.len > 0 || a.frame == FRAME_ECLIPTIC)) {
-                const ChainedState s = pool_change_center(true, t0, a.frame, a.chain, p, v);
-                frc = s.rc;
-                p = s.p;
-                v = s.v;
-            }
-            st[ST_T] = t0;
+            frc = a.status[obj];
+            st[ST_T] = a.jd0[obj];
             st[ST_TF] = a.jd1[obj];
-            st[ST_X] = p.x; st[ST_X + 1] = p.y; st[ST_X + 2] = p.z;
-            st[ST_V] = v.x; st[ST_V + 1] = v.y; st[ST_V + 2] = v.z;
+            st[ST_X] = a.out_pos[obj]; st[ST_X + 1] = a.out_pos[n + obj];
+            st[ST_X + 2] = a.out_pos[2 * n + obj];
+            st[ST_V] = a.out_vel[obj]; st[ST_V + 1] = a.out_vel[n + obj];
+            st[ST_V + 2] = a.out_vel[2 * n + obj];
         }
         if (lane < 7) {
             sb[lane] = 0.0;
@@ -402,19 +435,10 @@ __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_pool_kernel(NBodyArgs
     const int max_obj_rounds = a.max_loops * 11;
     for (;;) {
         if (phase == PH_STORE) {  // the finished object's outcome (lane 0 stores)
-            if (lane == 0) {
-                int code = outcome;
-                double3 p = make_double3(st[ST_X], st[ST_X + 1], st[ST_X + 2]);
-                double3 v = make_double3(st[ST_V], st[ST_V + 1], st[ST_V + 2]);
-                if (code == ST_OK && (a.chain.len > 0 || a.frame == FRAME_ECLIPTIC)) {
-                    const ChainedState s = pool_change_center(false, st[ST_TF], a.frame, a.chain,
-                                                              p, v);
-                    code = s.rc;
-                    p = s.p;
-                    v = s.v;
-                }
-                const double xs[3] = {p.x, p.y, p.z}, vs[3] = {v.x, v.y, v.z};
-                nodes_store(a, obj, code, xs, vs, F, st[ST_T], cnt);
+            if (lane == 0) {  // barycentric equatorial; pool_finish_kernel changes it back
+                const double xs[3] = {st[ST_X], st[ST_X + 1], st[ST_X + 2]};
+                const double vs[3] = {st[ST_V], st[ST_V + 1], st[ST_V + 2]};
+                nodes_store(a, obj, outcome, xs, vs, F, st[ST_T], cnt);
             }
             __syncwarp(gmask);  // st is read before the next object overwrites it
             phase = PH_DONE;
@@ -487,7 +511,8 @@ __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_pool_kernel(NBodyArgs
             erc = pool_forces(plan, F, exact, xe, ve, cache, ev);
             if (F.ng.kind != 0 && erc == ST_OK && plan.sun_vel >= 0) {
                 // non_grav_accel relative to the Sun (acceleration.rs:161-165)
-                // (inline for the JPL comet model without delay; out of line otherwise)
+                // (inline for the JPL comet model without delay; a call for the delayed model
+                // and dust)
                 const double* sc = cache + 6 * plan.sun_vel * NODES_BLOCK;
                 const double3 rp = make_double3(xe[0] - sc[0], xe[1] - sc[NODES_BLOCK],
                                                 xe[2] - sc[2 * NODES_BLOCK]);

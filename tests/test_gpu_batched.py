@@ -77,7 +77,9 @@ def test_pooled_forms_split_at_the_fast_window(gpu, oracle, spk_path, tmp_path):
     ephemeris in two files (two segments per body, meeting at JD 2460000.5), the objects whose
     span crosses into the other file's coverage are ordered after the others and integrated by
     the form with the general evaluation in a second launch.  Objects start on both sides of
-    the boundary, so that both launches have work whichever segment comes first; every object
+    the boundary, so that both launches have work whichever segment comes first; half the
+    comets have a delayed non-gravitational model (dt != 0, a two-body back-propagation per
+    evaluation, which the pooled kernel makes as its one out-of-line call).  Every object
     agrees with the oracle, which searches the segments for every evaluation."""
     from kete_b200 import tune
 
@@ -85,7 +87,10 @@ def test_pooled_forms_split_at_the_fast_window(gpu, oracle, spk_path, tmp_path):
     synthetic.write_synthetic_spk(a, jd_start=2459000.5, jd_end=2460000.5)
     synthetic.write_synthetic_spk(b, jd_start=2460000.5, jd_end=2461000.5)
     n = 400
-    pos, vel, ng = synthetic.mixed(n, seed=83)
+    pos, vel, ng = synthetic.mixed(n, seed=83, nongrav_frac=0.1)
+    comets = np.flatnonzero(ng[0] == 1.0)
+    ng[9, comets[::2]] = 4.0  # a delayed model for every other comet
+    assert len(comets) >= 20
     rng = np.random.default_rng(84)
     jd0 = np.where(np.arange(n) % 2 == 0, 2459700.5, 2460300.5)
     jd1 = jd0 + rng.uniform(-600.0, 600.0, n)
