@@ -82,8 +82,8 @@ NODE_TRAFFIC = {
     ("nbody_mixed_1m", 7, 1): {"bytes_per_object": (13_601_536 + 882_944) / 100_000,
                                "fp64_pipe": 0.217,
                                "captured": "one launch on a 100,000-object sample of the workload"},
-    ("nbody_mixed_1m", 10, 1): {"bytes_per_object": (13_445_376 + 390_400) / 100_000,
-                                "fp64_pipe": 0.291,
+    ("nbody_mixed_1m", 10, 1): {"bytes_per_object": (13_198_592 + 125_696) / 100_000,
+                                "fp64_pipe": 0.312,
                                 "captured": "one launch on a 100,000-object sample of the workload"},
 }
 
@@ -601,7 +601,13 @@ def run_gpu(args, world, rank, local):
         steps_total, iters_total, exact_total = (int(x) for x in cnt)
         flops, flops_ref = flop_models(steps_total, iters_total, exact_total)
         min_dist = det["min_dist"].cpu().numpy()
-    launches_per_step = (3 if (nbody and best.get("mode") == 2) else 0) + 1
+    # the library's own launch counter over one step (the graph replays the same launches)
+    count = _lib.lib().kete_b200_kernel_launches
+    count.restype = ctypes.c_int64
+    c0 = count()
+    step(d)
+    torch.cuda.synchronize()
+    launches_per_step = int(count() - c0)
 
     for _ in range(args.warmup):
         step(d)
