@@ -958,7 +958,9 @@ int kete_b200_propagate_n_body(int64_t n, const double* pos, const double* vel, 
         const int variant = nodes_variant_for(g_launch.nodes_variant, a.n_force);
         double lo, hi;
         nodes_window(variant, a.n_force, lo, hi);
-        if ((rc = launch_span_order(n, a.pos, a.vel, a.jd0, a.jd1, lo, hi, (int*)q, st))) return rc;
+        if ((rc = launch_span_order(n, a.pos, a.vel, a.jd0, a.jd1, lo, hi,
+                                    variant >= 9 ? a.nongrav : nullptr, (int*)q, st)))
+            return rc;
         // refill: a persistent grid taking the next object from the queue
         if ((rc = launch_nodes_ordered(a, variant, nodes_variant_for(7, a.n_force),
                                        g_launch.nodes_refill != 0, (int*)q, st)))

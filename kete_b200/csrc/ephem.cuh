@@ -22,13 +22,19 @@ constexpr int MAX_FORCE = 16;
 constexpr int MAX_CHAIN = 3;
 // span ordering of the persistent N-body grid: work buckets, and the scratch header (ints):
 // [0] object queue, [1 ..] bucket histogram, then the bucket cursors (ORDER_BUCKETS work
-// buckets and one last bucket for the objects whose span leaves the fast plan's window),
-// ORDER_RANGE: {0, objects inside the window, n}, ORDER_QUEUE2: the queue of the objects
-// outside it; the processing order follows the header
+// buckets, then one bucket for the objects with a non-gravitational model and one for the
+// objects whose span leaves the fast plan's window; the first two kinds only when the caller
+// asks for the split), ORDER_RANGE: {0, start of the non-gravitational bucket, start of the
+// outside bucket, n}, ORDER_QUEUE2: the queue of the objects outside the window,
+// ORDER_QUEUE3: the queue of the non-gravitational bucket; the processing order follows the
+// header
 constexpr int ORDER_BUCKETS = 120;
-constexpr int ORDER_ALL_BUCKETS = ORDER_BUCKETS + 1;
+constexpr int ORDER_NG_BUCKET = ORDER_BUCKETS;
+constexpr int ORDER_OUT_BUCKET = ORDER_BUCKETS + 1;
+constexpr int ORDER_ALL_BUCKETS = ORDER_BUCKETS + 2;
 constexpr int ORDER_RANGE = 1 + 2 * ORDER_ALL_BUCKETS;
-constexpr int ORDER_QUEUE2 = ORDER_RANGE + 3;
+constexpr int ORDER_QUEUE2 = ORDER_RANGE + 4;
+constexpr int ORDER_QUEUE3 = ORDER_RANGE + 5;
 constexpr int EPH_CACHE = 38;  // body-position cache, doubles per lane (the planets need 36)
 
 constexpr int ORDER_SCRATCH_HEADER = 256;

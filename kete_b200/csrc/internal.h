@@ -64,7 +64,9 @@ struct NBodyArgs {
     int* queue;           // refill counter for the node kernel (null: one object per group)
     const int32_t* order; // processing order (permutation of 0..n-1) or null
     const int* range;     // device {first, end}: the node kernel takes order[first .. end)
-                          // (null: order[0 .. n))
+                          // (null: order[0 .. n)); the pooled kernel: {first, start of the
+                          // non-gravitational part, end}
+    int* queue_ng;        // pooled kernel with refill: the queue of the non-gravitational part
 };
 
 int launch_two_body(int64_t n, const double* pos, const double* vel, const double* jd0,
@@ -86,13 +88,14 @@ int preload_order_kernels();
 // resolve the allocation-free entry point's scratch address on the current device
 int noalloc_prepare();
 int launch_span_order(int64_t n, const double* pos, const double* vel, const double* jd0,
-                      const double* jd1, double lo, double hi, int* scratch,
+                      const double* jd1, double lo, double hi, const double* ng, int* scratch,
                       cudaStream_t stream);
 // The node kernels over the processing order that launch_span_order wrote into scratch
 // (variant as launch_nbody_nodes; refill: persistent grid with the object queue).  A
-// warp-pooled variant integrates the objects inside the fast plan's window and
-// general_variant (a form with the general ephemeris evaluation) the others, in a second
-// launch; every other variant takes the whole order in one launch.
+// warp-pooled variant integrates the objects inside the fast plan's window (those with a
+// non-gravitational model from a queue of their own, first on a few SMs) and general_variant
+// (a form with the general ephemeris evaluation) the others, in a second launch; every other
+// variant takes the whole order in one launch.
 int launch_nodes_ordered(NBodyArgs a, int variant, int general_variant, bool refill,
                          int* scratch, cudaStream_t stream);
 

@@ -291,14 +291,17 @@ namespace kb {
 // The warp-pooled node kernel evaluates the ephemeris from the fast plan's records alone, so
 // the objects whose span [jd0, jd1] does not lie inside the plan's window (with a margin of
 // 1e-6 day: every evaluation time of a Radau integration lies between jd0 and jd1 up to
-// rounding) go to one last bucket; the header's range {0, inside, n} splits the order there.
-// Callers without a window pass [-inf, inf].
+// rounding) go to one last bucket.  Before it, one bucket holds the objects with a
+// non-gravitational model (given ng), which the pooled kernel integrates on a few SMs of
+// their own: the model's code, fetched by any warp of an SM, evicts the step loop from the
+// SM's instruction cache.  The header's range {0, ng start, outside start, n} splits the
+// order.  Callers without a window pass [-inf, inf] and ng = null.
 //
 // Scratch layout (ints): [0] object queue, [1..ORDER_ALL_BUCKETS] bucket histogram, then the
-// bucket cursors, the range at ORDER_RANGE, a second queue at ORDER_QUEUE2, then order[n]
-// from int offset ORDER_SCRATCH_HEADER.
+// bucket cursors, the range at ORDER_RANGE, further queues at ORDER_QUEUE2 and ORDER_QUEUE3,
+// then order[n] from int offset ORDER_SCRATCH_HEADER.
 // -------------------------------------------------------------------------------------------
-static_assert(ORDER_QUEUE2 + 1 <= ORDER_SCRATCH_HEADER, "order header too small");
+static_assert(ORDER_QUEUE3 + 1 <= ORDER_SCRATCH_HEADER, "order header too small");
 
 __device__ __forceinline__ bool in_window(double jd0, double jd1, double lo, double hi) {
     constexpr double MARGIN = 1e-6;  // NaN epochs compare false: outside
@@ -327,20 +330,22 @@ __device__ __forceinline__ int work_bucket(int64_t i, int64_t n, const double* _
 
 __device__ __forceinline__ int order_bucket(int64_t i, int64_t n, const double* __restrict__ pos,
                                             const double* __restrict__ vel, double t0, double t1,
-                                            double lo, double hi) {
-    return in_window(t0, t1, lo, hi) ? work_bucket(i, n, pos, vel, t0, t1) : ORDER_BUCKETS;
+                                            double lo, double hi, const double* __restrict__ ng) {
+    if (!in_window(t0, t1, lo, hi)) return ORDER_OUT_BUCKET;
+    if (ng && ng[i] != 0.0) return ORDER_NG_BUCKET;
+    return work_bucket(i, n, pos, vel, t0, t1);
 }
 
 __global__ void order_hist_kernel(int64_t n, const double* __restrict__ pos,
                                   const double* __restrict__ vel, const double* __restrict__ jd0,
                                   const double* __restrict__ jd1, double lo, double hi,
-                                  int* __restrict__ scratch) {
+                                  const double* __restrict__ ng, int* __restrict__ scratch) {
     __shared__ int h[ORDER_ALL_BUCKETS];
     for (int i = threadIdx.x; i < ORDER_ALL_BUCKETS; i += blockDim.x) h[i] = 0;
     __syncthreads();
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x)
-        atomicAdd(&h[order_bucket(i, n, pos, vel, jd0[i], jd1[i], lo, hi)], 1);
+        atomicAdd(&h[order_bucket(i, n, pos, vel, jd0[i], jd1[i], lo, hi, ng)], 1);
     __syncthreads();
     for (int i = threadIdx.x; i < ORDER_ALL_BUCKETS; i += blockDim.x)
         if (h[i]) atomicAdd(&scratch[1 + i], h[i]);
@@ -350,22 +355,24 @@ __global__ void order_scan_kernel(int* __restrict__ scratch) {
     if (threadIdx.x == 0 && blockIdx.x == 0) {
         int run = 0;
         for (int b = 0; b < ORDER_ALL_BUCKETS; ++b) {
-            if (b == ORDER_BUCKETS) scratch[ORDER_RANGE + 1] = run;  // objects inside the window
+            if (b == ORDER_NG_BUCKET) scratch[ORDER_RANGE + 1] = run;
+            if (b == ORDER_OUT_BUCKET) scratch[ORDER_RANGE + 2] = run;  // objects inside the window
             scratch[1 + ORDER_ALL_BUCKETS + b] = run;
             run += scratch[1 + b];
         }
         scratch[ORDER_RANGE] = 0;
-        scratch[ORDER_RANGE + 2] = run;
+        scratch[ORDER_RANGE + 3] = run;
     }
 }
 
 __global__ void order_scatter_kernel(int64_t n, const double* __restrict__ pos,
                                      const double* __restrict__ vel, const double* __restrict__ jd0,
                                      const double* __restrict__ jd1, double lo, double hi,
-                                     int* __restrict__ scratch, int32_t* __restrict__ order) {
+                                     const double* __restrict__ ng, int* __restrict__ scratch,
+                                     int32_t* __restrict__ order) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
-        const int b = order_bucket(i, n, pos, vel, jd0[i], jd1[i], lo, hi);
+        const int b = order_bucket(i, n, pos, vel, jd0[i], jd1[i], lo, hi, ng);
         const int p = atomicAdd(&scratch[1 + ORDER_ALL_BUCKETS + b], 1);
         if (p >= 0 && p < n) order[p] = (int32_t)i;
     }
@@ -382,9 +389,10 @@ int preload_order_kernels() {
 
 // Zero the header, histogram the work, scan, scatter.  scratch must hold
 // ORDER_SCRATCH_HEADER + n ints; order = scratch + ORDER_SCRATCH_HEADER.  [lo, hi]: the fast
-// plan's window whose outsiders are ordered last ([-inf, inf]: no split).
+// plan's window whose outsiders are ordered last, ng: the non-gravitational rows whose
+// objects are ordered just before them ([-inf, inf] and null: no split).
 int launch_span_order(int64_t n, const double* pos, const double* vel, const double* jd0,
-                      const double* jd1, double lo, double hi, int* scratch,
+                      const double* jd1, double lo, double hi, const double* ng, int* scratch,
                       cudaStream_t stream) {
     int rc = cuda_check(cudaMemsetAsync(scratch, 0, ORDER_SCRATCH_HEADER * sizeof(int), stream),
                         "clear order header");
@@ -392,9 +400,9 @@ int launch_span_order(int64_t n, const double* pos, const double* vel, const dou
     const int block = 256;
     int64_t g = (n + block - 1) / block;
     const int grid = (int)(g > 1184 ? 1184 : g);
-    order_hist_kernel<<<grid, block, 0, stream>>>(n, pos, vel, jd0, jd1, lo, hi, scratch);
+    order_hist_kernel<<<grid, block, 0, stream>>>(n, pos, vel, jd0, jd1, lo, hi, ng, scratch);
     order_scan_kernel<<<1, 32, 0, stream>>>(scratch);
-    order_scatter_kernel<<<grid, block, 0, stream>>>(n, pos, vel, jd0, jd1, lo, hi, scratch,
+    order_scatter_kernel<<<grid, block, 0, stream>>>(n, pos, vel, jd0, jd1, lo, hi, ng, scratch,
                                                      (int32_t*)(scratch + ORDER_SCRATCH_HEADER));
     return launched(3, "span order launch");
 }

@@ -109,6 +109,8 @@ extern "C" int kete_b200_propagate_n_body_noalloc(
     a.min_dist = min_dist;
     a.counters = counters;
     a.max_loops = cfg.max_loops;
-    if ((rc = launch_span_order(n, pos, vel, jd0, jd1, plan.lo, plan.hi, scratch, st))) return rc;
+    if ((rc = launch_span_order(n, pos, vel, jd0, jd1, plan.lo, plan.hi,
+                                cfg.nodes_variant >= 9 ? nongrav : nullptr, scratch, st)))
+        return rc;
     return launch_nodes_ordered(a, cfg.nodes_variant, plan.general_variant, true, scratch, st);
 }

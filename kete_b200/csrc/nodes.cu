@@ -113,6 +113,7 @@ int launch_nodes_ordered(NBodyArgs a, int variant, int general_variant, bool ref
     // object (threads and groups past their part exit).
     a.range = scratch + ORDER_RANGE;
     a.queue = refill ? scratch : nullptr;
+    a.queue_ng = refill ? scratch + ORDER_QUEUE3 : nullptr;
     const int64_t cgrid = std::min<int64_t>((a.n + 255) / 256, 1184);
     pool_prepare_kernel<<<(int)cgrid, 256, 0, stream>>>(a);
     if ((rc = launched(1, "pool_prepare_kernel launch"))) return rc;
@@ -120,8 +121,9 @@ int launch_nodes_ordered(NBodyArgs a, int variant, int general_variant, bool ref
     if ((rc = launch_nbody_nodes(a, variant, grid, stream))) return rc;
     pool_finish_kernel<<<(int)cgrid, 256, 0, stream>>>(a);
     if ((rc = launched(1, "pool_finish_kernel launch"))) return rc;
-    a.range = scratch + ORDER_RANGE + 1;
+    a.range = scratch + ORDER_RANGE + 2;
     a.queue = refill ? scratch + ORDER_QUEUE2 : nullptr;
+    a.queue_ng = nullptr;
     grid = 0;
     if (refill && (rc = refill_grid(general_variant, a.n, &grid))) return rc;
     return launch_nbody_nodes(a, general_variant, grid, stream);

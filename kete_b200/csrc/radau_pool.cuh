@@ -219,7 +219,7 @@ __device__ __forceinline__ int pool_forces(const FastPlan& P, SpkForce& F, bool 
 }
 
 // The centre and frame changes of the pooled kernel's objects, in kernels of their own (one
-// thread per object of the part order[range[0] .. range[1])): their code (a general state
+// thread per object of the part order[range[0] .. range[2])): their code (a general state
 // query of the centre's chain) runs once per object, and inside the step loop's kernel it
 // cost instruction-cache misses to every warp of the SM.
 //
@@ -227,7 +227,7 @@ __device__ __forceinline__ int pool_forces(const FastPlan& P, SpkForce& F, bool 
 // the epoch; the barycentric equatorial state goes to the output arrays, the outcome to
 // status, where nbody_pool_kernel reads both.
 static __global__ void pool_prepare_kernel(NBodyArgs a) {
-    const int64_t first = a.range[0], end = a.range[1], n = a.n;
+    const int64_t first = a.range[0], end = a.range[2], n = a.n;
     for (int64_t k = first + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < end;
          k += (int64_t)gridDim.x * blockDim.x) {
         const int64_t obj = a.order[k];
@@ -251,7 +251,7 @@ static __global__ void pool_prepare_kernel(NBodyArgs a) {
 // After it: from_ssb_equatorial (mod.rs:107-116) at the target epoch for every object that
 // arrived; a failure there gives NaN and its status, as in the other forms.
 static __global__ void pool_finish_kernel(NBodyArgs a) {
-    const int64_t first = a.range[0], end = a.range[1], n = a.n;
+    const int64_t first = a.range[0], end = a.range[2], n = a.n;
     if (!(a.chain.len > 0 || a.frame == FRAME_ECLIPTIC)) return;
     for (int64_t k = first + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < end;
          k += (int64_t)gridDim.x * blockDim.x) {
@@ -366,17 +366,41 @@ __global__ void __launch_bounds__(NODES_BLOCK, MINB) nbody_pool_kernel(NBodyArgs
     int outcome = ST_OK;  // outcome of a finished object, stored at the top of the next round
 
     auto fetch = [&]() -> bool {
+        // the objects inside the fast window: order[range[0] .. range[2]), those with a
+        // non-gravitational model from range[1] on (launch_nodes_ordered)
         int64_t k;
         if (a.queue) {
+            // groups on the first SMs take the non-gravitational part first, the others the
+            // rest; each turns to the other part when its own is used up.  Only a few SMs then
+            // fetch the non-gravitational model's code, which evicts the step loop from an
+            // SM's instruction cache.
             int q = 0;
-            if (lane == 0) q = atomicAdd(a.queue, 1);
+            if (lane == 0) {
+                const int r0 = a.range[0], r1 = a.range[1], r2 = a.range[2];
+                unsigned smid, nsm;
+                asm("mov.u32 %0, %%smid;" : "=r"(smid));
+                asm("mov.u32 %0, %%nsmid;" : "=r"(nsm));
+                const bool ng_first =
+                    r2 > r1 && (int64_t)smid * (r2 - r0) < (int64_t)nsm * (r2 - r1) + (r2 - r0);
+                q = r2;  // nothing left
+                for (int pass = 0; pass < 2; ++pass) {
+                    const bool ng_part = (pass == 0) == ng_first;
+                    const int lo = ng_part ? r1 : r0, hi = ng_part ? r2 : r1;
+                    if (hi > lo) {
+                        const int t = atomicAdd(ng_part ? a.queue_ng : a.queue, 1);
+                        if (t < hi - lo) {
+                            q = lo + t;
+                            break;
+                        }
+                    }
+                }
+            }
             k = __shfl_sync(gmask, q, 0, NODE_G);
         } else {
-            k = first ? group : a.n;  // one object per group
+            k = first ? group + a.range[0] : a.n;  // one object per group
         }
         first = false;
-        k += a.range[0];  // the objects inside the fast window (launch_nodes_ordered)
-        if (k >= a.range[1]) return false;
+        if (k >= a.range[2]) return false;
         obj = a.order ? a.order[k] : k;
         int frc = ST_OK;
         if (lane == 0) {
