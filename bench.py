@@ -82,8 +82,8 @@ NODE_TRAFFIC = {
     ("nbody_mixed_1m", 7, 1): {"bytes_per_object": (13_601_536 + 882_944) / 100_000,
                                "fp64_pipe": 0.217,
                                "captured": "one launch on a 100,000-object sample of the workload"},
-    ("nbody_mixed_1m", 10, 1): {"bytes_per_object": (13_198_592 + 125_696) / 100_000,
-                                "fp64_pipe": 0.312,
+    ("nbody_mixed_1m", 10, 1): {"bytes_per_object": (12_881_920 + 127_488) / 100_000,
+                                "fp64_pipe": 0.326,
                                 "captured": "one launch on a 100,000-object sample of the workload"},
 }
 
