@@ -1,5 +1,7 @@
 // adjoint.cu -- reverse-mode gradients: the checkpointed forward pass and the discrete
 // adjoint pass (adjoint.cuh) with their host launchers.
+// every object of the differentiation workloads carries the comet model: inline it
+#define KB_FORCE_NG_INLINE 1
 #include "common.cuh"
 #include "forces.cuh"
 #include "internal.h"

@@ -211,7 +211,12 @@ struct EphCache {
 
 // Acceleration from the SPK perturbers (spk_accel, acceleration.rs:121-168).  KU: the
 // Chebyshev loops' unrolling (cheb_pair); SpkForce is the lane-parallel kernels' compact form.
-template <int KU>
+// NGI: the JPL comet model without delay inline in the Sun's term (the other models stay a
+// call).  The inline code pays where every object carries the model (the differentiation
+// kernels on 4,096 comets: checkpointed forward 12.7 -> 12.0 ms, adjoint 15.0 -> 14.8 ms,
+// sensitivities 61.7 -> 59.8 ms) and costs where few do (the node and thread kernels on the
+// 1M mix with 5% comets: 5% slower).
+template <int KU, bool NGI = false>
 struct SpkForceT {
     int n_force;
     NonGrav ng;
@@ -272,8 +277,11 @@ struct SpkForceT {
             acc1 += rc * jy - rs * jz;
             acc2 += rs * jy + rc * jz;
             if (NG && fe.kind == FK_SUN && ng.kind != 0) {
-                const double3 na = nongrav_accel(ng, make_double3(rp[0], rp[1], rp[2]),
-                                                 make_double3(rv[0], rv[1], rv[2]));
+                const double3 prel = make_double3(rp[0], rp[1], rp[2]);
+                const double3 vrel = make_double3(rv[0], rv[1], rv[2]);
+                const double3 na = (NGI && ng.kind == 1 && ng.p(9) == 0.0)
+                                       ? nongrav_terms<false>(ng, prel, vrel)
+                                       : nongrav_accel(ng, prel, vrel);
                 acc0 += na.x;
                 acc1 += na.y;
                 acc2 += na.z;
@@ -509,7 +517,13 @@ struct SpkForceT {
     }
 };
 
-using SpkForce = SpkForceT<1>;         // lane-parallel kernels: compact loops
+// lane-parallel kernels: compact loops; a translation unit that defines KB_FORCE_NG_INLINE
+// before including this header (the differentiation kernels) gets the inline comet model
+#ifdef KB_FORCE_NG_INLINE
+using SpkForce = SpkForceT<1, true>;
+#else
+using SpkForce = SpkForceT<1>;
+#endif
 using SpkForceUnrolled = SpkForceT<FAST_NC>;  // one object per thread
 
 // central_accel (acceleration.rs:66-80): the Sun at the origin only.

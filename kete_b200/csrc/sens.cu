@@ -2,6 +2,8 @@
 // stm_nodes.cuh) and the one-object-per-thread form (nbody_stm_kernel, every force term in
 // dual numbers from tangent.cuh, the Jacobian of every corrector iteration at its own
 // points), with their host launcher.
+// every object of the differentiation workloads carries the comet model: inline it
+#define KB_FORCE_NG_INLINE 1
 #include "common.cuh"
 #include "forces.cuh"
 #include "internal.h"
